@@ -1,0 +1,211 @@
+/*
+ * ket_sv.h -- C ABI of the B200 dense statevector engine for ket.
+ *
+ * The engine replaces the statevector path of the ket TypeScript library
+ * (dmvjs/ket): the sparse Map<bigint,Complex> kernels of src/statevector.ts
+ * driven by simulatePure (src/circuit.ts:143-161) and the read-outs that
+ * consume its result (run / exactProbs / statevector / amplitude /
+ * probability / marginals / expectation, and vqe / gradient / minimize in
+ * src/algorithms.ts).  Each entry point below names the reference interface
+ * it replaces.
+ *
+ * Conventions (identical to the reference):
+ *   - basis index bit q is qubit q (q0 = LSB, src/statevector.ts:4-5);
+ *   - in every multi-qubit matrix the FIRST listed qubit is the MOST
+ *     significant bit of the local index (src/statevector.ts:32,107-108,237);
+ *   - bitstrings are parsed/printed by the host (q0 leftmost); this ABI only
+ *     sees integer indices.
+ *
+ * Threading: calls on one ket_ctx are serialised by the caller (the JS
+ * caller is single threaded, like the reference).  Every call that returns
+ * data blocks until the data is on the host.  Distinct contexts are
+ * independent.  No entry point keeps a caller pointer after it returns.
+ *
+ * Errors: every function returns a ket_status; ket_last_error() returns a
+ * thread-local message for the last failure on the calling thread.
+ */
+#ifndef KET_SV_H
+#define KET_SV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define KET_API __attribute__((visibility("default")))
+#else
+#define KET_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KET_SV_ABI_VERSION 1
+
+typedef enum ket_status {
+  KET_OK = 0,
+  KET_ERR_RANGE = 1,       /* qubit index out of range: the reference throws RangeError (circuit.ts:1114-1117) */
+  KET_ERR_TYPE = 2,        /* control == target, bad matrix shape, bad argument: TypeError (circuit.ts:1118-1145) */
+  KET_ERR_OOM = 3,         /* device allocation failed */
+  KET_ERR_CUDA = 4,        /* a CUDA runtime call failed */
+  KET_ERR_TIMEOUT = 5,     /* a bounded device wait ran out (status word set by the kernel) */
+  KET_ERR_UNSUPPORTED = 6  /* a valid request the engine does not implement */
+} ket_status;
+
+typedef enum ket_precision { KET_C128 = 0, KET_C64 = 1 } ket_precision;
+
+/* Op kinds: the FlatOp union of src/circuit.ts:20-47 (measure/reset/if are
+ * rejected: the pure path never sees them, src/circuit.ts:1432-1438). */
+typedef enum ket_op_kind {
+  KET_OP_SINGLE = 0,      /* q[0];            2x2 matrix   (applySingle, statevector.ts:47)      */
+  KET_OP_CNOT = 1,        /* q = {c, t}                    (applyCNOT, :70)                      */
+  KET_OP_SWAP = 2,        /* q = {a, b}                    (applySWAP, :85)                      */
+  KET_OP_TWO = 3,         /* q = {a, b};      4x4, a = MSB (applyTwo, :110)                      */
+  KET_OP_CONTROLLED = 4,  /* q = {c, t};      2x2          (applyControlled, :212)               */
+  KET_OP_TOFFOLI = 5,     /* q = {c1, c2, t}               (applyToffoli, :138)                  */
+  KET_OP_CSWAP = 6,       /* q = {c, a, b}                 (applyCSwap, :153)                    */
+  KET_OP_CSRSWAP = 7,     /* q = {c, a, b}                 (applyCsrSwap, :177)                  */
+  KET_OP_UNITARY = 8,     /* q[0..nq-1], q[0] = MSB; 2^nq x 2^nq (applyUnitary, :240)           */
+  KET_OP_BARRIER = 9      /* no effect on the state                                               */
+} ket_op_kind;
+
+#define KET_MAX_OP_QUBITS 10
+#define KET_MAX_QUBITS 40
+
+typedef struct ket_op {
+  int32_t kind;                    /* ket_op_kind */
+  int32_t nq;                      /* number of valid entries in q[] */
+  int32_t q[KET_MAX_OP_QUBITS];
+  int64_t mat;                     /* SINGLE/CONTROLLED/TWO/UNITARY: offset, in complex entries,
+                                      of the row-major matrix in the caller's matrix buffer
+                                      (interleaved re,im doubles); ignored otherwise */
+} ket_op;
+
+typedef struct ket_exec_opts {
+  int32_t fusion;      /* -1 = automatic (default), 0 = one pass per gate, k > 0 = tile width cap (qubits) */
+  int32_t prune;       /* 1 = reference accumulate() semantics: every computed amplitude with
+                          |a|^2 < 1e-14 is flushed to zero (statevector.ts:19-27); 0 = plain dense */
+  int32_t reserved[6];
+} ket_exec_opts;
+
+typedef struct ket_ctx ket_ctx;
+typedef struct ket_state ket_state;
+
+/* ---------------------------------------------------------------- context, memory */
+KET_API const char* ket_last_error(void);
+KET_API int ket_abi_version(void);
+KET_API void ket_exec_opts_default(ket_exec_opts* opts);
+
+/* One context per device; owns one CUDA stream and the scratch buffers. */
+KET_API int ket_ctx_create(int device, ket_ctx** out);
+KET_API int ket_ctx_destroy(ket_ctx* ctx);
+/* Device memory currently held by the context's scratch pool (bytes). */
+KET_API int ket_ctx_scratch_bytes(const ket_ctx* ctx, uint64_t* out);
+/* Host-side fault injection for tests: the after-th device allocation from now
+ * on (0 = the next one) fails with KET_ERR_OOM; a negative value disables it.
+ * No counterpart in the reference (which has no allocator). */
+KET_API int ket_debug_fail_alloc(int after);
+
+/* Dense state of 2^nqubits amplitudes, resident in device memory, set to |0..0>
+ * (zero(n), statevector.ts:16).  precision: KET_C128 or KET_C64. */
+KET_API int ket_state_alloc(ket_ctx* ctx, int nqubits, int precision, ket_state** out);
+KET_API int ket_state_free(ket_state* st);
+KET_API int ket_state_qubits(const ket_state* st, int* nqubits, int* precision);
+/* |idx> (svFromBitstring, circuit.ts:136-140; the host reverses the q0-leftmost string). */
+KET_API int ket_state_set_basis(ket_state* st, uint64_t idx);
+/* Upload / download amplitudes [offset, offset+count) as interleaved FP64 (re, im). */
+KET_API int ket_state_set_amplitudes(ket_state* st, uint64_t offset, uint64_t count, const double* re_im);
+KET_API int ket_state_get_amplitudes(const ket_state* st, uint64_t offset, uint64_t count, double* re_im);
+/* Copy src into dst (same size and precision). */
+KET_API int ket_state_copy(ket_state* dst, const ket_state* src);
+
+/* ---------------------------------------------------------------- running circuits */
+/* simulatePure (circuit.ts:143-161): apply ops in order.  mats holds nmat complex
+ * entries (2*nmat doubles).  Validation mirrors #checkOp (circuit.ts:1113-1146)
+ * and happens before any launch: on error the state is unchanged. */
+KET_API int ket_apply_ops(ket_state* st, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
+                  const ket_exec_opts* opts);
+
+/* Planner statistics for an op list on an n-qubit state without launching
+ * anything (no GPU needed): passes[0] = fused tile passes, passes[1] = single-
+ * gate passes, passes[2] = gates absorbed.  Used by host-side tests. */
+KET_API int ket_plan_stats(int nqubits, int precision, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
+                   const ket_exec_opts* opts, int64_t passes[3]);
+
+/* ---------------------------------------------------------------- read-outs */
+/* amplitude(): out[2i], out[2i+1] = re, im of amplitude idx[i] (circuit.ts:1491-1495). */
+KET_API int ket_amplitudes(const ket_state* st, const uint64_t* idx, size_t k, double* out_re_im);
+/* probabilities() as a dense array: out[i] = |a_i|^2 if > threshold else 0
+ * (statevector.ts:273-280 with threshold 1e-14). */
+KET_API int ket_probs_dense(const ket_state* st, double threshold, double* out);
+/* exactProbs() (circuit.ts:3700-3711): entries with p > threshold in ascending index
+ * order.  Writes min(count, cap) entries; *count = total number of such entries. */
+KET_API int ket_probs_sparse(const ket_state* st, double threshold, uint64_t* idx, double* p, uint64_t cap,
+                     uint64_t* count);
+/* marginals() (circuit.ts:1508-1518): out[q] = P(qubit q = 1), q = 0..n-1. */
+KET_API int ket_marginals(const ket_state* st, double* out);
+/* Joint distribution of m qubits: out[j] = P(bit k of j = qubit qubits[k], for all k), 2^m bins (1 <= m <= 12). */
+KET_API int ket_marginal_dist(const ket_state* st, const int* qubits, int m, double* out);
+/* Sum of |a|^2 (FP64 accumulation). */
+KET_API int ket_norm2(const ket_state* st, double* out);
+/* run() pure fast path sampler (circuit.ts:3424-3453): r[s] are the caller's
+ * uniform draws (makePrng, circuit.ts:813-819); out_idx[s] = the first index, in
+ * ascending order over entries with p > threshold, whose running FP64 sum is >= r[s]
+ * (the last such entry's running sum is taken as 1.0).  For 2^n <= 2^22 the running
+ * sum is accumulated in ascending index order, exactly as the reference does. */
+KET_API int ket_sample(const ket_state* st, const double* r, size_t shots, double threshold, uint64_t* out_idx);
+/* Circuit.expectation(pauli) (circuit.ts:3728-3753): pauli[q] in "IXYZ" acts on qubit q. */
+KET_API int ket_expect_pauli(const ket_state* st, const char* pauli, double* out);
+/* vqe() energy (algorithms.ts:301-336): sum_t coeffs[t] <P_t>.  ops holds nterms
+ * strings of n characters back to back; ops[t*n + 0] acts on qubit n-1 (the
+ * PauliTerm convention, algorithms.ts:283-285).  Terms with |coeff| < 1e-15 are
+ * skipped and all-identity terms add coeff, as the reference does. */
+KET_API int ket_expect_pauli_sum(const ket_state* st, int nterms, const double* coeffs, const char* ops, double* out);
+
+/* ---------------------------------------------------------------- differentiation */
+/* Parametric gates of a circuit template (the 'parametric' ops of circuit.ts:39-43
+ * after bind(), resolveParametric circuit.ts:1047-1073).  The angle fed to the gate
+ * is scale * params[param] + shift. */
+typedef enum ket_param_gate {
+  KET_PG_RX = 0, KET_PG_RY = 1, KET_PG_RZ = 2, KET_PG_U1 = 3,     /* single-qubit (rz also vz; u1 also p) */
+  KET_PG_GPI = 4, KET_PG_GPI2 = 5,
+  KET_PG_CRX = 6, KET_PG_CRY = 7, KET_PG_CRZ = 8, KET_PG_CU1 = 9, /* controlled: q = {c, t} */
+  KET_PG_XX = 10, KET_PG_YY = 11, KET_PG_ZZ = 12, KET_PG_XY = 13  /* two-qubit: q = {a, b} */
+} ket_param_gate;
+
+typedef struct ket_param_binding {
+  int32_t op;        /* index into the template's op list; that op's matrix is replaced */
+  int32_t gate;      /* ket_param_gate */
+  int32_t param;     /* parameter index */
+  int32_t reserved;
+  double scale;      /* angle = scale * params[param] + shift */
+  double shift;
+} ket_param_binding;
+
+/* Adjoint gradient of E(theta) = <psi(theta)|H|psi(theta)>, psi(theta) = U(theta)|init>,
+ * for `batch` parameter vectors (params[b*nparams + k]).  Replaces gradient() by parameter
+ * shift (algorithms.ts:536-547), which costs 2*nparams energy evaluations.  The template
+ * ops carry placeholder matrices for bound ops; H is a PauliTerm list (see
+ * ket_expect_pauli_sum).  energy[b] and grad[b*nparams + k] are written.
+ * checkpoint_every: 0 = automatic (about sqrt(#ops)), -1 = none; the forward state is
+ * stored every that many ops and restored during the reverse sweep. */
+KET_API int ket_adjoint_gradient(ket_ctx* ctx, int nqubits, uint64_t init, const ket_op* ops, size_t nops,
+                         const double* mats, size_t nmat, const ket_param_binding* binds, size_t nbinds,
+                         const double* params, int nparams, int batch, int nterms, const double* coeffs,
+                         const char* pauli_ops, int checkpoint_every, double* energy, double* grad);
+
+/* ---------------------------------------------------------------- batching */
+/* QAOA MaxCut batch: instance i has n[i] qubits, ne[i] edges at edges[2*eoff[i] ...],
+ * p layers with gamma[i*p + l], beta[i*p + l].  Circuit: H on all qubits, then per layer
+ * exp(-i gamma Z_u Z_v) on every edge and Rx(2 beta) on every qubit.  out[i] = <C> =
+ * sum_edges (1 - <Z_u Z_v>)/2 in FP64.  This equals vqe(qaoa(n, E, -2*gamma, beta),
+ * maxCutHamiltonian(n, E)) of algorithms.ts:231-276.  All instances run in one
+ * persistent launch (captured in a CUDA graph and replayed when use_graph = 1). */
+KET_API int ket_batch_qaoa(ket_ctx* ctx, int ninst, const int* n, const int* ne, const int64_t* eoff, const int* edges,
+                   int p, const double* gamma, const double* beta, int use_graph, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KET_SV_H */

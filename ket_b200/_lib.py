@@ -1,0 +1,136 @@
+"""ctypes binding of the engine's C ABI (include/ket_sv.h).
+
+This is the Python twin of the Node N-API addon (napi/ket_addon.c): it maps
+status codes to the exceptions the reference throws (RangeError / TypeError)
+and owns the process-wide default context.  There is no fallback: if the
+CUDA library is missing or no GPU is present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libket_sv.so")
+
+KET_OK, KET_ERR_RANGE, KET_ERR_TYPE, KET_ERR_OOM, KET_ERR_CUDA, KET_ERR_TIMEOUT, KET_ERR_UNSUPPORTED = range(7)
+KET_C128, KET_C64 = 0, 1
+
+OP_SINGLE, OP_CNOT, OP_SWAP, OP_TWO, OP_CONTROLLED, OP_TOFFOLI, OP_CSWAP, OP_CSRSWAP, OP_UNITARY, OP_BARRIER = range(10)
+MAX_OP_QUBITS = 10
+
+PG = {"rx": 0, "ry": 1, "rz": 2, "vz": 2, "u1": 3, "p": 3, "gpi": 4, "gpi2": 5, "crx": 6, "cry": 7, "crz": 8,
+      "cu1": 9, "xx": 10, "yy": 11, "zz": 12, "xy": 13}
+
+
+class RangeError(ValueError):
+    """The reference's RangeError (e.g. a qubit index out of range)."""
+
+
+class KetError(RuntimeError):
+    """An engine failure with no reference counterpart (device, memory, timeout)."""
+
+
+class ket_op(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("nq", C.c_int32), ("q", C.c_int32 * MAX_OP_QUBITS), ("mat", C.c_int64)]
+
+
+class ket_exec_opts(C.Structure):
+    _fields_ = [("fusion", C.c_int32), ("prune", C.c_int32), ("reserved", C.c_int32 * 6)]
+
+
+class ket_param_binding(C.Structure):
+    _fields_ = [("op", C.c_int32), ("gate", C.c_int32), ("param", C.c_int32), ("reserved", C.c_int32),
+                ("scale", C.c_double), ("shift", C.c_double)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"ket_b200 CUDA library not built: {LIB_PATH} is missing (run ket_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, u64, dbl, sz = C.c_void_p, C.c_int, C.c_uint64, C.c_double, C.c_size_t
+        P = C.POINTER
+        sigs = {
+            "ket_last_error": (C.c_char_p, []),
+            "ket_abi_version": (i32, []),
+            "ket_exec_opts_default": (None, [P(ket_exec_opts)]),
+            "ket_debug_fail_alloc": (i32, [i32]),
+            "ket_ctx_create": (i32, [i32, P(vp)]),
+            "ket_ctx_destroy": (i32, [vp]),
+            "ket_ctx_scratch_bytes": (i32, [vp, P(u64)]),
+            "ket_state_alloc": (i32, [vp, i32, i32, P(vp)]),
+            "ket_state_free": (i32, [vp]),
+            "ket_state_qubits": (i32, [vp, P(i32), P(i32)]),
+            "ket_state_set_basis": (i32, [vp, u64]),
+            "ket_state_set_amplitudes": (i32, [vp, u64, u64, P(dbl)]),
+            "ket_state_get_amplitudes": (i32, [vp, u64, u64, P(dbl)]),
+            "ket_state_copy": (i32, [vp, vp]),
+            "ket_apply_ops": (i32, [vp, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts)]),
+            "ket_plan_stats": (i32, [i32, i32, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts), P(C.c_int64)]),
+            "ket_amplitudes": (i32, [vp, P(u64), sz, P(dbl)]),
+            "ket_probs_dense": (i32, [vp, dbl, P(dbl)]),
+            "ket_probs_sparse": (i32, [vp, dbl, P(u64), P(dbl), u64, P(u64)]),
+            "ket_marginals": (i32, [vp, P(dbl)]),
+            "ket_marginal_dist": (i32, [vp, P(i32), i32, P(dbl)]),
+            "ket_norm2": (i32, [vp, P(dbl)]),
+            "ket_sample": (i32, [vp, P(dbl), sz, dbl, P(u64)]),
+            "ket_expect_pauli": (i32, [vp, C.c_char_p, P(dbl)]),
+            "ket_expect_pauli_sum": (i32, [vp, i32, P(dbl), C.c_char_p, P(dbl)]),
+            "ket_adjoint_gradient": (i32, [vp, i32, u64, P(ket_op), sz, P(dbl), sz, P(ket_param_binding), sz,
+                                           P(dbl), i32, i32, i32, P(dbl), C.c_char_p, i32, P(dbl), P(dbl)]),
+            "ket_batch_qaoa": (i32, [vp, i32, P(i32), P(i32), P(C.c_int64), P(i32), i32, P(dbl), P(dbl), i32,
+                                     P(dbl)]),
+        }
+        for name, (res, args) in sigs.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+        return L
+
+
+def check(rc: int):
+    if rc == KET_OK:
+        return
+    msg = lib().ket_last_error().decode(errors="replace")
+    if rc == KET_ERR_RANGE:
+        raise RangeError(msg)
+    if rc == KET_ERR_TYPE:
+        raise TypeError(msg)
+    raise KetError(f"ket engine error {rc}: {msg}")
+
+
+_ctx = None
+_ctx_lock = threading.Lock()
+
+
+def default_ctx():
+    """Process-wide engine context on CUDA device 0 (created on first use)."""
+    global _ctx
+    if _ctx is None:
+        with _ctx_lock:
+            if _ctx is None:
+                h = C.c_void_p()
+                dev = int(os.environ.get("KET_DEVICE", "0"))
+                check(lib().ket_ctx_create(dev, C.byref(h)))
+                _ctx = h
+    return _ctx
+
+
+def exec_opts(fusion: int = -1, prune: bool = True) -> ket_exec_opts:
+    o = ket_exec_opts()
+    lib().ket_exec_opts_default(C.byref(o))
+    o.fusion = fusion
+    o.prune = 1 if prune else 0
+    return o

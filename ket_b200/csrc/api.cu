@@ -1,0 +1,381 @@
+// api.cu -- the C ABI of the statevector engine (include/ket_sv.h).
+//
+// Control flow per call: validate on the host (mirroring the reference's
+// synchronous throws), launch on the context's stream, then wait with a
+// deadline by polling an event (never an unbounded synchronize), and report
+// CUDA failures as status codes with a thread-local message.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+#include "ctx.h"
+#include "launch.h"
+#include "read.h"
+
+namespace ket {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  g_err = std::string(where) + ": " + cudaGetErrorString(e);
+  return KET_ERR_CUDA;
+}
+
+// Allocation fault injection (host side): the N-th device allocation from now
+// fails with KET_ERR_OOM.  Set by ket_debug_fail_alloc() or KET_FAIL_ALLOC_AFTER.
+static long long g_fail_after = -2;
+
+static bool alloc_should_fail() {
+  if (g_fail_after == -2) {
+    const char* e = getenv("KET_FAIL_ALLOC_AFTER");
+    g_fail_after = e ? atoll(e) : -1;
+  }
+  if (g_fail_after < 0) return false;
+  if (g_fail_after == 0) { g_fail_after = -1; return true; }
+  g_fail_after--;
+  return false;
+}
+
+int dev_alloc(void** p, size_t bytes) {
+  *p = nullptr;
+  if (alloc_should_fail()) return fail(KET_ERR_OOM, "device allocation failed (injected)");
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(KET_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+  }
+  return KET_OK;
+}
+
+int ctx_scratch(ket_ctx* ctx, size_t bytes, void** out) {
+  bytes = std::max<size_t>(bytes, 256);
+  if (ctx->scratch_bytes < bytes) {
+    int rc = ctx_wait(ctx);
+    if (rc) return rc;
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    size_t want = std::max(bytes, size_t(1) << 20);
+    rc = dev_alloc(&ctx->scratch, want);
+    if (rc) return rc;
+    ctx->scratch_bytes = want;
+  }
+  *out = ctx->scratch;
+  return KET_OK;
+}
+
+double wait_deadline_s() {
+  const char* e = getenv("KET_WAIT_TIMEOUT_S");
+  return e ? atof(e) : 1800.0;
+}
+
+int ctx_wait(ket_ctx* ctx) {
+  cudaError_t e = cudaEventRecord(ctx->done, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+  auto t0 = std::chrono::steady_clock::now();
+  const double limit = wait_deadline_s();
+  int spins = 0;
+  for (;;) {
+    e = cudaEventQuery(ctx->done);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) return cuda_fail(e, "device execution");
+    if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el > limit) return fail(KET_ERR_TIMEOUT, "device work did not finish within the wait deadline");
+  }
+  return KET_OK;
+}
+
+static size_t amp_bytes(int precision) { return precision == KET_C64 ? 8 : 16; }
+
+}  // namespace ket
+
+using namespace ket;
+
+extern "C" {
+
+const char* ket_last_error(void) { return g_err.c_str(); }
+int ket_abi_version(void) { return KET_SV_ABI_VERSION; }
+
+void ket_exec_opts_default(ket_exec_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->fusion = -1;
+  o->prune = 1;
+}
+
+int ket_debug_fail_alloc(int after) {
+  g_fail_after = after;
+  return KET_OK;
+}
+
+int ket_ctx_create(int device, ket_ctx** out) {
+  if (!out) return fail(KET_ERR_TYPE, "null output pointer");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(KET_ERR_CUDA, std::string("no CUDA device available: ") + cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= count) return fail(KET_ERR_RANGE, "device index out of range");
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  ket_ctx* c = new ket_ctx();
+  c->device = device;
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaStreamCreate"); }
+  e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
+  if (e != cudaSuccess) { cudaStreamDestroy(c->stream); delete c; return cuda_fail(e, "cudaEventCreate"); }
+  *out = c;
+  return KET_OK;
+}
+
+int ket_ctx_destroy(ket_ctx* c) {
+  if (!c) return KET_OK;
+  cudaSetDevice(c->device);
+  ctx_wait(c);
+  if (c->scratch) cudaFree(c->scratch);
+  if (c->scratch2) cudaFree(c->scratch2);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  cudaEventDestroy(c->done);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return KET_OK;
+}
+
+int ket_ctx_scratch_bytes(const ket_ctx* c, uint64_t* out) {
+  if (!c || !out) return fail(KET_ERR_TYPE, "null argument");
+  *out = c->scratch_bytes + c->scratch2_bytes;
+  return KET_OK;
+}
+
+int ket_state_alloc(ket_ctx* c, int n, int precision, ket_state** out) {
+  if (!c || !out) return fail(KET_ERR_TYPE, "null argument");
+  *out = nullptr;
+  if (n < 1 || n > KET_MAX_QUBITS) return fail(KET_ERR_RANGE, "qubit count out of range: " + std::to_string(n));
+  if (precision != KET_C128 && precision != KET_C64) return fail(KET_ERR_TYPE, "precision must be KET_C128 or KET_C64");
+  cudaSetDevice(c->device);
+  size_t bytes = amp_bytes(precision) << n;
+  void* p = nullptr;
+  int rc = dev_alloc(&p, bytes);
+  if (rc) return rc;
+  ket_state* s = new ket_state();
+  s->ctx = c;
+  s->n = n;
+  s->precision = precision;
+  s->amp = p;
+  s->bytes = bytes;
+  rc = ket_state_set_basis(s, 0);
+  if (rc) { cudaFree(p); delete s; return rc; }
+  *out = s;
+  return KET_OK;
+}
+
+int ket_state_free(ket_state* s) {
+  if (!s) return KET_OK;
+  cudaSetDevice(s->ctx->device);
+  ctx_wait(s->ctx);
+  cudaFree(s->amp);
+  delete s;
+  return KET_OK;
+}
+
+int ket_state_qubits(const ket_state* s, int* n, int* precision) {
+  if (!s) return fail(KET_ERR_TYPE, "null state");
+  if (n) *n = s->n;
+  if (precision) *precision = s->precision;
+  return KET_OK;
+}
+
+int ket_state_set_basis(ket_state* s, uint64_t idx) {
+  if (!s) return fail(KET_ERR_TYPE, "null state");
+  if (s->n < 64 && (idx >> s->n) != 0) return fail(KET_ERR_RANGE, "basis index out of range");
+  cudaSetDevice(s->ctx->device);
+  cudaError_t e = cudaMemsetAsync(s->amp, 0, s->bytes, s->ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  if (s->precision == KET_C64) {
+    float one[2] = {1.0f, 0.0f};
+    e = cudaMemcpyAsync((char*)s->amp + 8 * idx, one, 8, cudaMemcpyHostToDevice, s->ctx->stream);
+  } else {
+    double one[2] = {1.0, 0.0};
+    e = cudaMemcpyAsync((char*)s->amp + 16 * idx, one, 16, cudaMemcpyHostToDevice, s->ctx->stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+  return ctx_wait(s->ctx);
+}
+
+int ket_state_set_amplitudes(ket_state* s, uint64_t off, uint64_t cnt, const double* re_im) {
+  if (!s || (!re_im && cnt)) return fail(KET_ERR_TYPE, "null argument");
+  uint64_t N = uint64_t(1) << s->n;
+  if (off > N || cnt > N - off) return fail(KET_ERR_RANGE, "amplitude range out of bounds");
+  if (cnt == 0) return KET_OK;
+  cudaSetDevice(s->ctx->device);
+  if (s->precision == KET_C128) {
+    cudaError_t e = cudaMemcpyAsync((char*)s->amp + 16 * off, re_im, 16 * cnt, cudaMemcpyHostToDevice, s->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+    return ctx_wait(s->ctx);
+  }
+  std::vector<float> tmp(2 * cnt);
+  for (uint64_t i = 0; i < 2 * cnt; i++) tmp[i] = (float)re_im[i];
+  cudaError_t e = cudaMemcpyAsync((char*)s->amp + 8 * off, tmp.data(), 8 * cnt, cudaMemcpyHostToDevice, s->ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+  return ctx_wait(s->ctx);
+}
+
+int ket_state_get_amplitudes(const ket_state* s, uint64_t off, uint64_t cnt, double* re_im) {
+  if (!s || (!re_im && cnt)) return fail(KET_ERR_TYPE, "null argument");
+  uint64_t N = uint64_t(1) << s->n;
+  if (off > N || cnt > N - off) return fail(KET_ERR_RANGE, "amplitude range out of bounds");
+  if (cnt == 0) return KET_OK;
+  cudaSetDevice(s->ctx->device);
+  if (s->precision == KET_C128) {
+    cudaError_t e = cudaMemcpyAsync(re_im, (char*)s->amp + 16 * off, 16 * cnt, cudaMemcpyDeviceToHost, s->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+    return ctx_wait(s->ctx);
+  }
+  std::vector<float> tmp(2 * cnt);
+  cudaError_t e = cudaMemcpyAsync(tmp.data(), (char*)s->amp + 8 * off, 8 * cnt, cudaMemcpyDeviceToHost, s->ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+  int rc = ctx_wait(s->ctx);
+  if (rc) return rc;
+  for (uint64_t i = 0; i < 2 * cnt; i++) re_im[i] = tmp[i];
+  return KET_OK;
+}
+
+int ket_state_copy(ket_state* dst, const ket_state* src) {
+  if (!dst || !src) return fail(KET_ERR_TYPE, "null state");
+  if (dst->n != src->n || dst->precision != src->precision) return fail(KET_ERR_TYPE, "state shape mismatch");
+  cudaSetDevice(dst->ctx->device);
+  cudaError_t e = cudaMemcpyAsync(dst->amp, src->amp, src->bytes, cudaMemcpyDeviceToDevice, dst->ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+  return ctx_wait(dst->ctx);
+}
+
+int ket_plan_stats(int n, int precision, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
+                   const ket_exec_opts* opts, int64_t passes[3]) {
+  ket_exec_opts o;
+  if (opts) o = *opts; else ket_exec_opts_default(&o);
+  if (n < 1 || n > KET_MAX_QUBITS) return fail(KET_ERR_RANGE, "qubit count out of range");
+  Plan plan;
+  std::string err;
+  int rc = lower_ops(n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
+  if (rc) return fail(rc, err);
+  plan_passes(n, precision, o.fusion, plan);
+  passes[0] = passes[1] = passes[2] = 0;
+  for (auto& p : plan.passes) {
+    if (p.fused) passes[0]++; else passes[1]++;
+    passes[2] += (int64_t)p.gates.size();
+  }
+  return KET_OK;
+}
+
+int ket_apply_ops(ket_state* s, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
+                  const ket_exec_opts* opts) {
+  if (!s) return fail(KET_ERR_TYPE, "null state");
+  if (nops && !ops) return fail(KET_ERR_TYPE, "null op list");
+  ket_exec_opts o;
+  if (opts) o = *opts; else ket_exec_opts_default(&o);
+  Plan plan;
+  std::string err;
+  int rc = lower_ops(s->n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
+  if (rc) return fail(rc, err);
+  if (plan.gates.empty()) return KET_OK;
+  plan_passes(s->n, s->precision, o.fusion, plan);
+  return run_plan(s, plan, o);
+}
+
+}  // extern "C"
+
+namespace ket {
+
+int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
+  ket_ctx* c = s->ctx;
+  cudaSetDevice(c->device);
+  // Device image: all DevOps of fused passes, then MATK descriptors.
+  std::vector<DevOp> devops;
+  std::vector<size_t> pass_off(plan.passes.size(), 0);
+  std::vector<size_t> matk_off(plan.passes.size(), 0);
+  size_t matk_bytes = 0;
+  for (size_t i = 0; i < plan.passes.size(); i++) {
+    const Pass& p = plan.passes[i];
+    if (p.fused) {
+      pass_off[i] = devops.size();
+      for (int gi : p.gates) devops.push_back(encode_devop(plan.gates[gi], p, o.prune != 0));
+    } else {
+      const Gate& g = plan.gates[p.gates[0]];
+      if (g.type == G_MATK) {
+        matk_off[i] = matk_bytes;
+        matk_bytes += 64 + 16 * g.mk.size();
+        matk_bytes = (matk_bytes + 255) & ~size_t(255);
+      }
+    }
+  }
+  size_t ops_bytes = ((sizeof(DevOp) * devops.size()) + 255) & ~size_t(255);
+  size_t total = ops_bytes + matk_bytes;
+  void* dev = nullptr;
+  if (total) {
+    int rc = ctx_scratch(c, total, &dev);
+    if (rc) return rc;
+    std::vector<unsigned char> host(total, 0);
+    if (!devops.empty()) memcpy(host.data(), devops.data(), sizeof(DevOp) * devops.size());
+    for (size_t i = 0; i < plan.passes.size(); i++) {
+      const Pass& p = plan.passes[i];
+      if (p.fused) continue;
+      const Gate& g = plan.gates[p.gates[0]];
+      if (g.type != G_MATK) continue;
+      unsigned char* dst = host.data() + ops_bytes + matk_off[i];
+      int* q = reinterpret_cast<int*>(dst);
+      for (size_t j = 0; j < g.tk.size(); j++) q[j] = g.tk[j];
+      memcpy(dst + 64, g.mk.data(), 16 * g.mk.size());
+    }
+    cudaError_t e = cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(ops)");
+  }
+  const DevOp* dops = reinterpret_cast<const DevOp*>(dev);
+  for (size_t i = 0; i < plan.passes.size(); i++) {
+    const Pass& p = plan.passes[i];
+    cudaError_t e;
+    if (p.fused) {
+      PassArgs a;
+      memset(&a, 0, sizeof(a));
+      a.amp = s->amp;
+      a.ops = dops + pass_off[i];
+      a.nops = (int)p.gates.size();
+      a.n = s->n;
+      a.m = p.m;
+      a.L = p.L;
+      a.nh = (int)p.hbits.size();
+      for (int j = 0; j < a.nh; j++) a.hbits[j] = p.hbits[j];
+      uint64_t S = (p.L >= 64) ? ~uint64_t(0) : ((uint64_t(1) << p.L) - 1);
+      for (int q : p.hbits) S |= uint64_t(1) << q;
+      a.nctx = 0;
+      for (int q = 0; q < s->n; q++)
+        if (!((S >> q) & 1)) a.ctxbits[a.nctx++] = q;
+      a.thr = 1e-14;
+      a.qthr = 1e-7;
+      e = launch_fused(a, s->precision, c->stream);
+    } else {
+      const Gate& g = plan.gates[p.gates[0]];
+      const void* mk = g.type == G_MATK ? (const void*)((const char*)dev + ops_bytes + matk_off[i]) : nullptr;
+      e = launch_gate(g, s->precision, s->amp, s->n, mk, c->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  }
+  return ctx_wait(c);
+}
+
+}  // namespace ket

@@ -1,0 +1,61 @@
+// engine.h -- host-side structures of the statevector engine.
+#pragma once
+
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/ket_sv.h"
+
+namespace ket {
+
+struct cd {
+  double re, im;
+};
+
+// Internal gate after lowering a ket_op (controls folded into a mask).
+enum GType : int32_t {
+  G_MAT1 = 0,   // 2x2 on t0, controls cmask
+  G_DIAG1 = 1,  // diag(d0, d1) on t0, controls cmask
+  G_X1 = 2,     // X on t0 (CNOT / Toffoli), controls cmask
+  G_SWAP = 3,   // swap t0, t1, controls cmask
+  G_MAT2 = 4,   // 4x4 on (t0 = MSB, t1), controls cmask
+  G_MATK = 5,   // dense 2^k x 2^k on tk (tk[0] = MSB)
+  G_DIAG2 = 6   // diag(m0..m3) on (t0 = MSB, t1), controls cmask
+};
+
+struct Gate {
+  GType type;
+  int t0 = -1, t1 = -1;
+  uint64_t cmask = 0;
+  bool prune = false;         // computed outputs are flushed when |a|^2 < 1e-14
+  cd m[16];                   // MAT1: m[0..3]; DIAG1: m[0], m[1]; DIAG2: m[0..3]; MAT2: m[0..15]
+  std::vector<int> tk;        // MATK targets
+  std::vector<cd> mk;         // MATK matrix
+  int src_op = -1;            // index of the ket_op it came from
+};
+
+// Tile pass: the tile holds qubits {0..L-1} U hbits; gates are applied in order.
+struct Pass {
+  bool fused = false;
+  int m = 0;                  // tile qubits
+  int L = 0;                  // low contiguous qubits in the tile
+  std::vector<int> hbits;     // global positions of tile bits L..m-1
+  std::vector<int> gates;     // indices into the gate list
+};
+
+struct Plan {
+  std::vector<Gate> gates;
+  std::vector<Pass> passes;
+};
+
+// Lower and validate an op list (mirrors #checkOp, circuit.ts:1113-1146).
+int lower_ops(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, bool prune,
+              std::vector<Gate>& out, std::string& err);
+// Greedy fusion planner.
+void plan_passes(int n, int precision, int fusion, Plan& plan);
+
+// Tile width used for fused passes at a given precision.
+int tile_qubits(int precision, int fusion);
+
+}  // namespace ket

@@ -1,0 +1,279 @@
+// planner.cpp -- op validation, lowering and the greedy fusion planner.
+//
+// lower_ops() turns the reference's FlatOp list (circuit.ts:20-47, carried
+// as ket_op) into internal gates: control qubits become a mask, diagonal and
+// X-type matrices are recognised (they then need no amplitude pairing), and
+// identity gates and barriers are dropped.  Validation mirrors #checkOp
+// (circuit.ts:1113-1146): RangeError for an out-of-range qubit, TypeError for
+// control == target or a malformed unitary.
+//
+// plan_passes() groups gates into tile passes.  A pass streams the state
+// through tiles of 2^m amplitudes: the tile holds the L lowest qubits
+// (contiguous in memory, so loads coalesce) plus m-L chosen high qubits.  A
+// gate joins the pass when every qubit it mixes lies in the tile; control
+// qubits and diagonal gates may sit anywhere, since their bit values are
+// known from each amplitude's global index.  Gate order is preserved: a gate
+// deferred to a later pass blocks every later gate that shares a qubit.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "engine.h"
+
+namespace ket {
+
+namespace {
+
+inline bool is0(cd a) { return a.re == 0.0 && a.im == 0.0; }
+inline bool is1(cd a) { return a.re == 1.0 && a.im == 0.0; }
+
+int range_err(std::string& err, int q, int n) {
+  err = "qubit index " + std::to_string(q) + " is out of range for a " + std::to_string(n) + "-qubit circuit";
+  return KET_ERR_RANGE;
+}
+
+uint64_t bit(int q) { return uint64_t(1) << q; }
+
+// Qubits a gate touches (targets and controls).
+uint64_t gate_qubits(const Gate& g) {
+  uint64_t m = g.cmask;
+  if (g.t0 >= 0) m |= bit(g.t0);
+  if (g.t1 >= 0) m |= bit(g.t1);
+  for (int q : g.tk) m |= bit(q);
+  return m;
+}
+
+// Qubits whose amplitudes a gate mixes (must lie in the tile).
+uint64_t gate_mix(const Gate& g) {
+  switch (g.type) {
+    case G_DIAG1: case G_DIAG2: return 0;
+    case G_MAT1: case G_X1: return bit(g.t0);
+    case G_SWAP: case G_MAT2: return bit(g.t0) | bit(g.t1);
+    case G_MATK: { uint64_t m = 0; for (int q : g.tk) m |= bit(q); return m; }
+  }
+  return 0;
+}
+
+// A 4x4 with every off-diagonal entry zero becomes a diagonal phase gate.
+void lower_diag2(Gate& g) {
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++)
+      if (r != c && !is0(g.m[r * 4 + c])) return;
+  cd d[4] = {g.m[0], g.m[5], g.m[10], g.m[15]};
+  g.type = G_DIAG2;
+  for (int k = 0; k < 4; k++) g.m[k] = d[k];
+}
+
+bool fusable(const Gate& g) { return g.type != G_MATK || g.tk.size() <= 2; }
+
+}  // namespace
+
+int lower_ops(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, bool prune,
+              std::vector<Gate>& out, std::string& err) {
+  out.clear();
+  out.reserve(nops);
+  auto getm = [&](const ket_op& op, int k, cd* dst, std::vector<cd>* vdst) -> int {
+    size_t cnt = size_t(1) << (2 * k);
+    if (op.mat < 0 || (size_t)op.mat + cnt > nmat || mats == nullptr) {
+      err = "matrix offset out of bounds for op";
+      return KET_ERR_TYPE;
+    }
+    for (size_t i = 0; i < cnt; i++) {
+      cd v{mats[2 * (op.mat + i)], mats[2 * (op.mat + i) + 1]};
+      if (dst) dst[i] = v;
+      if (vdst) vdst->push_back(v);
+    }
+    return KET_OK;
+  };
+  for (size_t i = 0; i < nops; i++) {
+    const ket_op& op = ops[i];
+    int need = -1;
+    switch (op.kind) {
+      case KET_OP_SINGLE: need = 1; break;
+      case KET_OP_CNOT: case KET_OP_SWAP: case KET_OP_TWO: case KET_OP_CONTROLLED: need = 2; break;
+      case KET_OP_TOFFOLI: case KET_OP_CSWAP: case KET_OP_CSRSWAP: need = 3; break;
+      case KET_OP_UNITARY: case KET_OP_BARRIER: break;
+      default: err = "unknown op kind " + std::to_string(op.kind); return KET_ERR_TYPE;
+    }
+    if (need >= 0 && op.nq != need) {
+      err = "op " + std::to_string(i) + ": expected " + std::to_string(need) + " qubits";
+      return KET_ERR_TYPE;
+    }
+    if (op.nq < 0 || op.nq > KET_MAX_OP_QUBITS) { err = "op qubit count out of bounds"; return KET_ERR_TYPE; }
+    if (op.kind == KET_OP_UNITARY && op.nq == 0) { err = "unitary: qubits must be non-empty"; return KET_ERR_TYPE; }
+    for (int j = 0; j < op.nq; j++)
+      if (op.q[j] < 0 || op.q[j] >= n) return range_err(err, op.q[j], n);
+    const int* q = op.q;
+    Gate g;
+    g.src_op = (int)i;
+    switch (op.kind) {
+      case KET_OP_BARRIER: continue;
+      case KET_OP_CNOT:
+        if (q[0] == q[1]) { err = "control and target qubits must differ (got " + std::to_string(q[0]) + ")"; return KET_ERR_TYPE; }
+        g.type = G_X1; g.t0 = q[1]; g.cmask = bit(q[0]);
+        break;
+      case KET_OP_TOFFOLI:
+        if (q[2] == q[0] || q[2] == q[1]) { err = "toffoli: target repeats a control qubit"; return KET_ERR_TYPE; }
+        g.type = G_X1; g.t0 = q[2]; g.cmask = bit(q[0]) | bit(q[1]);
+        break;
+      case KET_OP_SWAP:
+        if (q[0] == q[1]) continue;  // applySWAP with a == b is the identity
+        g.type = G_SWAP; g.t0 = q[0]; g.t1 = q[1];
+        break;
+      case KET_OP_CSWAP:
+        if (q[1] == q[2]) continue;
+        if (q[0] == q[1] || q[0] == q[2]) { err = "cswap: control repeats a target qubit"; return KET_ERR_TYPE; }
+        g.type = G_SWAP; g.t0 = q[1]; g.t1 = q[2]; g.cmask = bit(q[0]);
+        break;
+      case KET_OP_CSRSWAP: {
+        if (q[1] == q[2] || q[0] == q[1] || q[0] == q[2]) { err = "csrswap: qubits must be distinct"; return KET_ERR_TYPE; }
+        const double s = 1.0 / std::sqrt(2.0);
+        g.type = G_MAT2; g.t0 = q[1]; g.t1 = q[2]; g.cmask = bit(q[0]); g.prune = prune;
+        for (int k = 0; k < 16; k++) g.m[k] = cd{0, 0};
+        g.m[0] = cd{1, 0}; g.m[5] = cd{s, 0}; g.m[6] = cd{0, s}; g.m[9] = cd{0, s}; g.m[10] = cd{s, 0}; g.m[15] = cd{1, 0};
+        break;
+      }
+      case KET_OP_SINGLE: case KET_OP_CONTROLLED: {
+        int t = op.kind == KET_OP_SINGLE ? q[0] : q[1];
+        if (op.kind == KET_OP_CONTROLLED) {
+          if (q[0] == q[1]) { err = "control and target qubits must differ (got " + std::to_string(q[0]) + ")"; return KET_ERR_TYPE; }
+          g.cmask = bit(q[0]);
+        }
+        cd m[4];
+        int rc = getm(op, 1, m, nullptr);
+        if (rc) return rc;
+        g.t0 = t;
+        g.prune = prune;
+        if (is0(m[1]) && is0(m[2])) {
+          if (is1(m[0]) && is1(m[3])) continue;  // identity: outputs equal inputs bit for bit
+          g.type = G_DIAG1; g.m[0] = m[0]; g.m[1] = m[3];
+        } else if (is0(m[0]) && is0(m[3]) && is1(m[1]) && is1(m[2])) {
+          g.type = G_X1; g.prune = false;  // 0*x0 + 1*x1 == x1 exactly: a permutation
+        } else {
+          g.type = G_MAT1;
+          for (int k = 0; k < 4; k++) g.m[k] = m[k];
+        }
+        break;
+      }
+      case KET_OP_TWO: {
+        if (q[0] == q[1]) { err = "two-qubit gate on a repeated qubit"; return KET_ERR_TYPE; }
+        int rc = getm(op, 2, g.m, nullptr);
+        if (rc) return rc;
+        g.type = G_MAT2; g.t0 = q[0]; g.t1 = q[1]; g.prune = prune;
+        lower_diag2(g);
+        break;
+      }
+      case KET_OP_UNITARY: {
+        int k = op.nq;
+        for (int a = 0; a < k; a++)
+          for (int b = a + 1; b < k; b++)
+            if (q[a] == q[b]) { err = "unitary: repeated qubit"; return KET_ERR_TYPE; }
+        g.prune = prune;
+        if (k == 1) {
+          cd m[4];
+          int rc = getm(op, 1, m, nullptr);
+          if (rc) return rc;
+          g.t0 = q[0];
+          if (is0(m[1]) && is0(m[2])) {
+            if (is1(m[0]) && is1(m[3])) continue;
+            g.type = G_DIAG1; g.m[0] = m[0]; g.m[1] = m[3];
+          } else {
+            g.type = G_MAT1;
+            for (int j = 0; j < 4; j++) g.m[j] = m[j];
+          }
+        } else if (k == 2) {
+          int rc = getm(op, 2, g.m, nullptr);
+          if (rc) return rc;
+          g.type = G_MAT2; g.t0 = q[0]; g.t1 = q[1];
+          lower_diag2(g);
+        } else {
+          int rc = getm(op, k, nullptr, &g.mk);
+          if (rc) return rc;
+          g.type = G_MATK;
+          g.tk.assign(q, q + k);
+        }
+        break;
+      }
+    }
+    out.push_back(std::move(g));
+  }
+  return KET_OK;
+}
+
+int tile_qubits(int precision, int fusion) {
+  int mx = precision == KET_C64 ? 13 : 12;
+  if (fusion > 0) return std::max(6, std::min(fusion, mx));
+  return mx;
+}
+
+void plan_passes(int n, int precision, int fusion, Plan& plan) {
+  plan.passes.clear();
+  const std::vector<Gate>& G = plan.gates;
+  const int M = std::min(n, tile_qubits(precision, fusion));
+  const int L = std::min(n, 5);
+  const uint64_t low = (L >= 64) ? ~uint64_t(0) : bit(L) - 1;
+  std::vector<int> pending(G.size());
+  for (size_t i = 0; i < G.size(); i++) pending[i] = (int)i;
+
+  auto single_pass = [&](int gi) {
+    Pass p;
+    p.fused = false;
+    p.gates.push_back(gi);
+    plan.passes.push_back(std::move(p));
+  };
+
+  if (fusion == 0) {
+    for (int gi : pending) single_pass(gi);
+    return;
+  }
+
+  while (!pending.empty()) {
+    // Choose the tile's qubit set along the frontier of pending gates.
+    uint64_t S = (M >= n) ? (n >= 64 ? ~uint64_t(0) : bit(n) - 1) : low;
+    for (;;) {
+      bool grew = false;
+      uint64_t B = 0;
+      for (int gi : pending) {
+        const Gate& g = G[gi];
+        uint64_t qs = gate_qubits(g);
+        if (qs & B) { B |= qs; continue; }
+        if (!fusable(g)) { B |= qs; continue; }
+        uint64_t mix = gate_mix(g);
+        if ((mix & ~S) == 0) continue;
+        uint64_t miss = mix & ~S;
+        if (__builtin_popcountll(S | miss) <= M) { S |= miss; grew = true; break; }
+        B |= qs;
+      }
+      if (!grew) break;
+    }
+    // Sweep: take every gate applicable in tile S, preserving order.
+    Pass p;
+    p.fused = true;
+    p.m = M;
+    p.L = L;
+    uint64_t B = 0;
+    std::vector<int> rest;
+    for (int gi : pending) {
+      const Gate& g = G[gi];
+      uint64_t qs = gate_qubits(g);
+      if ((qs & B) || !fusable(g) || (gate_mix(g) & ~S)) { B |= qs; rest.push_back(gi); continue; }
+      p.gates.push_back(gi);
+    }
+    if (p.gates.empty()) {
+      // Front gate cannot be fused (wide unitary): run it alone.
+      single_pass(pending[0]);
+      pending.erase(pending.begin());
+      continue;
+    }
+    for (int q = 0; q < n; q++)
+      if (((S >> q) & 1) && !((low >> q) & 1)) p.hbits.push_back(q);
+    // Pad the tile to M qubits with unused high qubits (keeps tile count fixed).
+    for (int q = n - 1; (int)p.hbits.size() + L < M && q >= L; q--)
+      if (!((S >> q) & 1)) { p.hbits.push_back(q); S |= bit(q); }
+    std::sort(p.hbits.begin(), p.hbits.end());
+    plan.passes.push_back(std::move(p));
+    pending.swap(rest);
+  }
+}
+
+}  // namespace ket

@@ -1,0 +1,130 @@
+"""The oracle pinned against the reference's own known answers.
+
+Every case in tests/golden/reference_kats.json restates a test of the
+reference suite (dmvjs/ket src/circuit.test.ts) with its expected value and
+digit count; the oracle must reproduce all of them in its sparse mode (the
+reference's own data structure and pruning) and in its dense modes.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from harness import bit_index, init_index, load_kats, oracle_circuit, tol
+from oracle import oracle as O
+
+CASES = load_kats()
+
+
+def eval_oracle(case, mode):
+    c = oracle_circuit(case)
+    st = c.simulate(init=init_index(case), mode=mode)
+    idx, p = st.exact_probs()
+    probs = {format(int(i), "b").zfill(case["n"])[::-1]: float(v) for i, v in zip(idx, p)}
+    for chk in case["checks"]:
+        kind = chk[0]
+        if kind == "amp":
+            a = st.amplitude(bit_index(chk[1]))
+            assert abs(a.real - chk[2]) < tol(chk[4]), (case["id"], chk, a)
+            assert abs(a.imag - chk[3]) < tol(chk[4]), (case["id"], chk, a)
+        elif kind == "prob":
+            assert abs(probs.get(chk[1], 0.0) - chk[2]) < tol(chk[3]), (case["id"], chk, probs)
+        elif kind == "nkeys":
+            assert len(probs) == chk[1], (case["id"], probs)
+        elif kind == "uniform":
+            assert all(abs(v - chk[1]) < tol(chk[2]) for v in probs.values())
+        elif kind == "marg":
+            m = st.marginals()
+            assert abs(m[chk[1]] - chk[2]) < tol(chk[3])
+        elif kind == "norm":
+            assert abs(sum(probs.values()) - 1.0) < tol(chk[1])
+        elif kind == "vqe":
+            e = c.vqe([(t[0], t[1]) for t in chk[1]], mode=mode)
+            assert abs(e - chk[2]) < tol(chk[3]), (case["id"], e)
+        elif kind == "expect":
+            # the reference's expectation() starts from |0..0>
+            e = c.expectation(chk[1], mode=mode)
+            assert abs(e - chk[2]) < tol(chk[3]), (case["id"], e)
+        else:
+            raise AssertionError(kind)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["id"] for c in CASES])
+def test_kat_sparse(case):
+    eval_oracle(case, O.SPARSE)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["id"] for c in CASES])
+def test_kat_dense(case):
+    eval_oracle(case, O.DENSE)
+
+
+def test_gradient_kats():
+    """gradient() parameter-shift KATs (circuit.test.ts:4168-4219)."""
+    Z = [(1.0, "Z")]
+    # realAmplitudes(1, 0) is exactly ry(p0, 0)
+    for theta, want in [(0.0, 0.0), (math.pi / 4, -math.sin(math.pi / 4)), (math.pi, 0.0)]:
+        g = O.gradient(O.ANS_REAL_AMPLITUDES, 1, 0, [theta], Z)
+        assert abs(g[0] - want) < tol(10)
+    p0, p1 = math.pi / 3, math.pi / 6
+    g = O.gradient(O.ANS_REAL_AMPLITUDES, 2, 0, [p0, p1], [(1.0, "ZI"), (1.0, "IZ")])
+    assert abs(g[0] + math.sin(p0)) < tol(10) and abs(g[1] + math.sin(p1)) < tol(10)
+    g1 = O.gradient(O.ANS_REAL_AMPLITUDES, 1, 0, [math.pi / 5], [(1.0, "Z")])
+    g2 = O.gradient(O.ANS_REAL_AMPLITUDES, 1, 0, [math.pi / 5], [(2.0, "Z")])
+    assert abs(g2[0] - 2 * g1[0]) < tol(10)
+
+
+def test_minimize_kats():
+    """minimize() KATs (circuit.test.ts:4239-4262)."""
+    r = O.minimize(O.ANS_REAL_AMPLITUDES, 1, 0, [0.1], [(1.0, "Z")])
+    assert abs(r["energy"] + 1) < tol(4) and r["converged"]
+    r = O.minimize(O.ANS_REAL_AMPLITUDES, 2, 0, [0.1, 0.1], [(1.0, "ZZ"), (0.5, "ZI")], lr=0.2, steps=500)
+    assert abs(r["energy"] + 1.5) < tol(3) and r["converged"]
+    r = O.minimize(O.ANS_REAL_AMPLITUDES, 1, 0, [0.1], [(1.0, "Z")], steps=1)
+    assert not r["converged"] and r["steps"] == 1
+    r = O.minimize(O.ANS_REAL_AMPLITUDES, 1, 0, [math.pi], [(1.0, "Z")])
+    assert r["converged"] and r["steps"] == 0
+
+
+def test_qaoa_4cycle():
+    """qaoa + maxCutHamiltonian on the 4-cycle (circuit.test.ts:6373-6421)."""
+    edges = [(0, 1), (1, 2), (2, 3), (3, 0)]
+    H = O.maxcut_hamiltonian(4, edges)
+    assert H[0] == (2.0, "IIII") and len(H) == 5
+    idx, p = O.qaoa(4, edges, [], []).simulate().exact_probs()
+    assert len(idx) == 16 and all(abs(v - 1 / 16) < tol(10) for v in p)
+    st = O.qaoa(4, edges, [math.pi / 4], [0.15 * math.pi]).simulate()
+    probs = dict(zip([int(i) for i in st.exact_probs()[0]], st.exact_probs()[1]))
+    assert probs.get(0b0101, 0) > 0.20 and probs.get(0b1010, 0) > 0.20   # '1010' and '0101'
+    assert O.qaoa(4, edges, [math.pi / 4], [0.15 * math.pi]).vqe(H) > 2.5
+    assert abs(O.OCircuit(4).vqe(H)) < tol(10)
+    assert O.maxcut_hamiltonian(3, []) == []
+
+
+def test_bigint_indices_sparse():
+    """Qubits 30, 31 and 40 (circuit.test.ts:482-505) on the sparse oracle."""
+    c = O.OCircuit(31).add("h", [0]).add("cnot", [0, 30])
+    idx, p = c.simulate().exact_probs()
+    assert list(idx) == [0, (1 << 30) | 1]
+    c = O.OCircuit(32).add("h", [0]).add("cnot", [0, 31])
+    idx, _ = c.simulate().exact_probs()
+    assert list(idx) == [0, (1 << 31) | 1]
+    c = O.OCircuit(41).add("x", [40])
+    idx, p = c.simulate().exact_probs()
+    assert list(idx) == [1 << 40] and p[0] == 1.0
+
+
+def test_bounds_errors():
+    """#checkOp errors (circuit.test.ts:507-552)."""
+    with pytest.raises(O.OracleRangeError):
+        O.OCircuit(2).add("h", [-1])
+    with pytest.raises(O.OracleRangeError):
+        O.OCircuit(2).add("x", [2])
+    with pytest.raises(O.OracleRangeError):
+        O.OCircuit(2).add("cnot", [5, 1])
+    with pytest.raises(O.OracleRangeError):
+        O.OCircuit(3).add("ccx", [0, 1, 3])
+    with pytest.raises(O.OracleTypeError):
+        O.OCircuit(2).add("cnot", [1, 1])
+    with pytest.raises(O.OracleTypeError):
+        O.OCircuit(2).add("crx", [0, 0], [0.5])
