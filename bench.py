@@ -1,0 +1,361 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 statevector engine on its headline workload.
+
+Workload (one step): the 30-qubit dense complex128 state (16 GiB in HBM) is
+reset to |0...0>, then the seeded 40-layer brickwork circuit followed by
+qft(30) -- 2260 gates -- is applied, and the outputs are read back: 1024
+amplitudes at seeded basis indices and the joint distribution of q0..q9.
+Inputs are synthetic (xorshift32 seed 42, see ket_b200/workloads.py); the
+16 GiB state exceeds the 126 MB L2, so no flush is needed between steps.
+
+  value   gates/s from device busy time (sum of the engine's kernel times,
+          CUDA events on the engine's stream), inputs already resident
+  e2e     gates/s by wall clock through the public API from host buffers
+          (op list + matrices in, amplitudes and marginals out)
+
+The roofline entry is for the dominant kernel, the register-tiled fused pass:
+algorithmic bytes per launch = 2 * 16 * 2^30 (one read and one write of the
+state), divided by its mean event-timed duration.
+
+--impl reference times the reference algorithm on the host cores instead:
+the sparse-map restatement of src/statevector.ts (oracle/, the reference
+itself is TypeScript and no JavaScript runtime exists on these machines) on
+bounded samples of the same circuit family at 20 qubits, all host cores
+running copies in parallel, converted to the same unit.
+
+Multi-GPU (torchrun): the engine runs on one GPU; each rank runs an
+independent replica of the workload (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ket", choices=["ket", "reference"])
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--layers", type=int, default=40)
+    ap.add_argument("--prune", type=int, default=1, help="1: reference pruning semantics (default), 0: plain dense")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Dist:
+    """torch.distributed plumbing for replicas: barrier and max over ranks."""
+
+    def __init__(self, world, rank, local):
+        self.world, self.rank, self.local = world, rank, local
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+            self.dist = dist
+            self.torch = torch
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            self.dist.barrier()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        t = self.torch.tensor([float(v)], device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.dist.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        busy = [s for s, p in zip(sm, power) if p > 200] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def ncu_traffic(n):
+    """DRAM bytes per fused-pass launch from the committed ncu summary, scaled
+    from the profiled state size to 2^n amplitudes."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "fused_pass_traffic.json")) as f:
+            d = json.load(f)
+        return d["dram_bytes_per_launch"] * 2.0 ** (n - d["qubits"])
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------- CPU baseline
+SAMPLE_N, SAMPLE_FIRST, SAMPLE_OPS = 20, 70, 12
+
+
+def cpu_sample(_=None):
+    """Time the reference algorithm (sparse map with pruning, 1 thread) on
+    ops [100, 112) of the 20-qubit brickwork(40)+qft(20) circuit (seed 42),
+    after simulating ops [0, 100) untimed.  Returns (seconds, amplitude updates)."""
+    from oracle import oracle as O
+    c, _ = O.brickwork(SAMPLE_N, 40, 42, with_qft=True)
+    return c.time_ops(SAMPLE_FIRST, SAMPLE_OPS, mode=O.SPARSE)
+
+
+def cpu_rate(nproc):
+    """30-qubit-equivalent gates/s of nproc parallel copies of the sample."""
+    if nproc <= 1:
+        sec, upd = cpu_sample()
+        return upd / sec / 2.0 ** 30, sec
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    t0 = time.time()
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(cpu_sample, range(nproc))
+    wall = time.time() - t0
+    upd = sum(r[1] for r in res)
+    slowest = max(r[0] for r in res)
+    return upd / slowest / 2.0 ** 30, wall
+
+
+def sample_desc(cores):
+    return (f"reference algorithm (sparse Map + 1e-14 pruning, restated in C++: oracle/ket_oracle.cpp) on ops "
+            f"[{SAMPLE_FIRST},{SAMPLE_FIRST + SAMPLE_OPS}) of the {SAMPLE_N}-qubit brickwork(40)+qft({SAMPLE_N}) "
+            f"circuit, seed 42, {cores} process(es); rate = amplitude updates/s / 2^30")
+
+
+def run_reference(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    O.build()
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_rate(cores)
+    vals = []
+    t0 = time.time()
+    for _ in range(args.steps):
+        v, _w = cpu_rate(cores)
+        vals.append(v)
+    wall = time.time() - t0
+    value = statistics.mean(vals)
+    line = {
+        "impl": "reference",
+        "metric": "30q gates/s",
+        "value": value,
+        "unit": "gates/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "30-qubit brickwork(40 layers)+qft(30), seed 42, complex128; reference sampled at "
+                               f"{SAMPLE_N} qubits", "qubits": args.qubits},
+        "cpu_baseline": {"value": value, "unit": "gates/s", "cores": cores, "kind": "port",
+                         "sample": sample_desc(cores)},
+        "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ket(args):
+    world, rank, local = dist_env()
+    os.environ["KET_DEVICE"] = str(local)
+    dist = Dist(world, rank, local)
+    import ctypes as C
+
+    import numpy as np
+
+    from ket_b200 import _lib, workloads as W
+    from ket_b200.circuit import DeviceState, flatten_ops, ops_to_abi
+
+    n = args.qubits
+    circ, idx = W.brickwork_qft(n, args.layers, 42)
+    arr, mats, k = ops_to_abi(flatten_ops(circ.ops))
+    L = _lib.lib()
+    ctx = _lib.default_ctx()
+    st = DeviceState(n)
+    prune = bool(args.prune)
+    marg_q = list(range(10))
+    idx_arr = np.array(idx, dtype=np.uint64)
+
+    def step():
+        st.set_basis(0)
+        st.apply_abi(arr, mats, k, prune=prune)
+        a = st.amplitudes(idx_arr)
+        md = st.marginal_dist(marg_q)
+        return a, md
+
+    for _ in range(args.warmup):
+        step()
+
+    def counters():
+        lc = C.c_uint64()
+        h2d, d2h = C.c_uint64(), C.c_uint64()
+        L.ket_ctx_launch_count(ctx, C.byref(lc))
+        L.ket_ctx_io_bytes(ctx, C.byref(h2d), C.byref(d2h))
+        return lc.value, h2d.value, d2h.value
+
+    L.ket_ctx_profile(ctx, 1)
+    clocks = ClockSampler(local)
+    dist.barrier()
+    clocks.start()
+    c0 = counters()
+    t0 = time.perf_counter()
+    kinds_all, ms_all = [], []
+    for _ in range(args.steps):
+        a, md = step()
+        cnt = C.c_size_t()
+        kinds = (C.c_int * 65536)()
+        ms = (C.c_float * 65536)()
+        _lib.check(L.ket_ctx_profile_read(ctx, kinds, ms, 65536, C.byref(cnt)))
+        kinds_all += list(kinds[: cnt.value])
+        ms_all += list(ms[: cnt.value])
+    wall = time.perf_counter() - t0
+    c1 = counters()
+    clk = clocks.stop()
+    L.ket_ctx_profile(ctx, 0)
+
+    busy_s = sum(ms_all) / 1e3
+    busy_max = dist.max(busy_s)
+    wall_max = dist.max(wall)
+    gates_total = k * args.steps * world
+    value = gates_total / busy_max
+    e2e = gates_total / wall_max
+    fused = [t for kd, t in zip(kinds_all, ms_all) if kd == 0]
+    peak, peak_kind = hbm_peak()
+    bytes_per_launch = 2 * 16 * 2.0 ** n
+    achieved = bytes_per_launch / (statistics.mean(fused) / 1e3) / 1e9 if fused else None
+    passes_per_step = len(fused) / args.steps if fused else 0
+    line = {
+        "metric": "30q gates/s",
+        "value": value,
+        "unit": "gates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": busy_max / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "c128 (f64)",
+        "data": "synthetic",
+        "config": {"workload": f"{n}-qubit brickwork({args.layers} layers)+qft({n}), seed 42, complex128, "
+                               "outputs 1024 amplitudes + q0-q9 marginals",
+                   "qubits": n, "gates_per_step": k, "fused_passes_per_step": passes_per_step,
+                   "pruning": "reference (|a|^2<1e-14 flushed per gate)" if prune else "off (plain dense)",
+                   "l2_flush": "not needed: 16 GiB state > 126 MB L2",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": "gates/s", "h2d_bytes_per_step": (c1[1] - c0[1]) // args.steps,
+                "d2h_bytes_per_step": (c1[2] - c0[2]) // args.steps},
+        "gpu_launches": c1[0] - c0[0],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                     "traffic": ncu_traffic(n), "kernel": "k_fused2 (register-tiled fused pass)",
+                     "bytes_per_launch": bytes_per_launch},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, _ = cpu_rate(1)
+        line["cpu_baseline"] = {"value": v, "unit": "gates/s", "cores": 1, "kind": "port", "sample": sample_desc(1)}
+    dist.close()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ket(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -101,6 +101,18 @@ KET_API int ket_ctx_create(int device, ket_ctx** out);
 KET_API int ket_ctx_destroy(ket_ctx* ctx);
 /* Device memory currently held by the context's scratch pool (bytes). */
 KET_API int ket_ctx_scratch_bytes(const ket_ctx* ctx, uint64_t* out);
+/* Per-launch timing: with profiling on, every kernel the context launches is
+ * bracketed by CUDA events on its stream; ket_ctx_profile_read waits for the
+ * stream, returns (kind, milliseconds) per launch since the last read and
+ * clears the list.  Kinds: 0 register-tiled fused pass, 1 small-state fused
+ * pass, 2 single-gate pass, 3 read-out, 4 adjoint sweep, 5 batch.  No
+ * counterpart in the reference (which only times whole calls, benchmark/run.mjs:16-35). */
+KET_API int ket_ctx_profile(ket_ctx* ctx, int enable);
+KET_API int ket_ctx_profile_read(ket_ctx* ctx, int* kinds, float* ms, size_t cap, size_t* count);
+/* Kernel launches made by the context so far. */
+KET_API int ket_ctx_launch_count(const ket_ctx* ctx, uint64_t* count);
+/* Bytes the context has copied host->device and device->host so far. */
+KET_API int ket_ctx_io_bytes(const ket_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
 /* Host-side fault injection for tests: the after-th device allocation from now
  * on (0 = the next one) fails with KET_ERR_OOM; a negative value disables it.
  * No counterpart in the reference (which has no allocator). */
@@ -131,6 +143,13 @@ KET_API int ket_apply_ops(ket_state* st, const ket_op* ops, size_t nops, const d
  * gate passes, passes[2] = gates absorbed.  Used by host-side tests. */
 KET_API int ket_plan_stats(int nqubits, int precision, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
                    const ket_exec_opts* opts, int64_t passes[3]);
+
+/* Same, for the register-tiled passes: counts[t] = number of program ops of type t
+ * (0 layout exchange, 1/2 2x2 on a register/lane bit, 3/4 X on a register/lane
+ * bit, 5 register swap, 6 4x4, 7-10 diagonal forms), counts[14] = tiled passes,
+ * counts[15] = other passes.  No counterpart in the reference. */
+KET_API int ket_plan_program_stats(int nqubits, int precision, const ket_op* ops, size_t nops, const double* mats,
+                                   size_t nmat, const ket_exec_opts* opts, int64_t counts[16]);
 
 /* ---------------------------------------------------------------- read-outs */
 /* amplitude(): out[2i], out[2i+1] = re, im of amplitude idx[i] (circuit.ts:1491-1495). */

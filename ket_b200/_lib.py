@@ -69,6 +69,10 @@ def lib():
             "ket_ctx_create": (i32, [i32, P(vp)]),
             "ket_ctx_destroy": (i32, [vp]),
             "ket_ctx_scratch_bytes": (i32, [vp, P(u64)]),
+            "ket_ctx_profile": (i32, [vp, i32]),
+            "ket_ctx_profile_read": (i32, [vp, P(i32), P(C.c_float), sz, P(sz)]),
+            "ket_ctx_launch_count": (i32, [vp, P(u64)]),
+            "ket_ctx_io_bytes": (i32, [vp, P(u64), P(u64)]),
             "ket_state_alloc": (i32, [vp, i32, i32, P(vp)]),
             "ket_state_free": (i32, [vp]),
             "ket_state_qubits": (i32, [vp, P(i32), P(i32)]),
@@ -78,6 +82,8 @@ def lib():
             "ket_state_copy": (i32, [vp, vp]),
             "ket_apply_ops": (i32, [vp, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts)]),
             "ket_plan_stats": (i32, [i32, i32, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts), P(C.c_int64)]),
+            "ket_plan_program_stats": (i32, [i32, i32, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts),
+                                             P(C.c_int64)]),
             "ket_amplitudes": (i32, [vp, P(u64), sz, P(dbl)]),
             "ket_probs_dense": (i32, [vp, dbl, P(dbl)]),
             "ket_probs_sparse": (i32, [vp, dbl, P(u64), P(dbl), u64, P(u64)]),

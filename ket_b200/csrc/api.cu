@@ -101,6 +101,26 @@ int ctx_wait(ket_ctx* ctx) {
 
 static size_t amp_bytes(int precision) { return precision == KET_C64 ? 8 : 16; }
 
+void prof_begin(ket_ctx* c) {
+  if (!c->prof) return;
+  if (c->prof_next + 2 > c->ev_pool.size()) {
+    for (int i = 0; i < 64; i++) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) { c->prof = false; return; }
+      c->ev_pool.push_back(e);
+    }
+  }
+  cudaEventRecord(c->ev_pool[c->prof_next], c->stream);
+}
+
+void prof_end(ket_ctx* c, int kind) {
+  c->launches++;
+  if (!c->prof || c->prof_next + 2 > c->ev_pool.size()) return;
+  cudaEventRecord(c->ev_pool[c->prof_next + 1], c->stream);
+  c->prof_kind.push_back(kind);
+  c->prof_next += 2;
+}
+
 }  // namespace ket
 
 using namespace ket;
@@ -140,6 +160,11 @@ int ket_ctx_create(int device, ket_ctx** out) {
   if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaStreamCreate"); }
   e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
   if (e != cudaSuccess) { cudaStreamDestroy(c->stream); delete c; return cuda_fail(e, "cudaEventCreate"); }
+  void* st = nullptr;
+  int rc = dev_alloc(&st, 256);
+  if (rc) { cudaEventDestroy(c->done); cudaStreamDestroy(c->stream); delete c; return rc; }
+  c->d_status = (int*)st;
+  cudaMemsetAsync(c->d_status, 0, 256, c->stream);
   *out = c;
   return KET_OK;
 }
@@ -150,7 +175,9 @@ int ket_ctx_destroy(ket_ctx* c) {
   ctx_wait(c);
   if (c->scratch) cudaFree(c->scratch);
   if (c->scratch2) cudaFree(c->scratch2);
+  if (c->d_status) cudaFree(c->d_status);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   cudaEventDestroy(c->done);
   cudaStreamDestroy(c->stream);
   delete c;
@@ -160,6 +187,44 @@ int ket_ctx_destroy(ket_ctx* c) {
 int ket_ctx_scratch_bytes(const ket_ctx* c, uint64_t* out) {
   if (!c || !out) return fail(KET_ERR_TYPE, "null argument");
   *out = c->scratch_bytes + c->scratch2_bytes;
+  return KET_OK;
+}
+
+int ket_ctx_profile(ket_ctx* c, int enable) {
+  if (!c) return fail(KET_ERR_TYPE, "null context");
+  c->prof = enable != 0;
+  c->prof_kind.clear();
+  c->prof_next = 0;
+  return KET_OK;
+}
+
+int ket_ctx_profile_read(ket_ctx* c, int* kinds, float* ms, size_t cap, size_t* count) {
+  if (!c || !count) return fail(KET_ERR_TYPE, "null argument");
+  int rc = ctx_wait(c);
+  if (rc) return rc;
+  size_t n = c->prof_kind.size();
+  *count = n;
+  for (size_t i = 0; i < n && i < cap; i++) {
+    if (kinds) kinds[i] = c->prof_kind[i];
+    float t = 0.f;
+    cudaEventElapsedTime(&t, c->ev_pool[2 * i], c->ev_pool[2 * i + 1]);
+    if (ms) ms[i] = t;
+  }
+  c->prof_kind.clear();
+  c->prof_next = 0;
+  return KET_OK;
+}
+
+int ket_ctx_io_bytes(const ket_ctx* c, uint64_t* h2d, uint64_t* d2h) {
+  if (!c) return fail(KET_ERR_TYPE, "null context");
+  if (h2d) *h2d = c->h2d_bytes;
+  if (d2h) *d2h = c->d2h_bytes;
+  return KET_OK;
+}
+
+int ket_ctx_launch_count(const ket_ctx* c, uint64_t* out) {
+  if (!c || !out) return fail(KET_ERR_TYPE, "null argument");
+  *out = c->launches;
   return KET_OK;
 }
 
@@ -207,6 +272,7 @@ int ket_state_set_basis(ket_state* s, uint64_t idx) {
   cudaSetDevice(s->ctx->device);
   cudaError_t e = cudaMemsetAsync(s->amp, 0, s->bytes, s->ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  s->ctx->h2d_bytes += s->precision == KET_C64 ? 8 : 16;
   if (s->precision == KET_C64) {
     float one[2] = {1.0f, 0.0f};
     e = cudaMemcpyAsync((char*)s->amp + 8 * idx, one, 8, cudaMemcpyHostToDevice, s->ctx->stream);
@@ -274,11 +340,33 @@ int ket_plan_stats(int n, int precision, const ket_op* ops, size_t nops, const d
   std::string err;
   int rc = lower_ops(n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
   if (rc) return fail(rc, err);
-  plan_passes(n, precision, o.fusion, plan);
+  plan_passes(n, precision, o.fusion, o.prune != 0, plan);
   passes[0] = passes[1] = passes[2] = 0;
   for (auto& p : plan.passes) {
     if (p.fused) passes[0]++; else passes[1]++;
     passes[2] += (int64_t)p.gates.size();
+  }
+  return KET_OK;
+}
+
+int ket_plan_program_stats(int n, int precision, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
+                           const ket_exec_opts* opts, int64_t counts[16]) {
+  ket_exec_opts o;
+  if (opts) o = *opts; else ket_exec_opts_default(&o);
+  if (n < 1 || n > KET_MAX_QUBITS) return fail(KET_ERR_RANGE, "qubit count out of range");
+  Plan plan;
+  std::string err;
+  int rc = lower_ops(n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
+  if (rc) return fail(rc, err);
+  plan_passes(n, precision, o.fusion, o.prune != 0, plan);
+  for (int i = 0; i < 16; i++) counts[i] = 0;
+  for (auto& p : plan.passes) {
+    if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) { counts[15]++; continue; }
+    std::vector<FOp> prog;
+    uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
+    plan_program(plan, p, precision, o.prune != 0, prog, lp, sp);
+    for (auto& f : prog) counts[f.type]++;
+    counts[14]++;
   }
   return KET_OK;
 }
@@ -294,7 +382,7 @@ int ket_apply_ops(ket_state* s, const ket_op* ops, size_t nops, const double* ma
   int rc = lower_ops(s->n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
   if (rc) return fail(rc, err);
   if (plan.gates.empty()) return KET_OK;
-  plan_passes(s->n, s->precision, o.fusion, plan);
+  plan_passes(s->n, s->precision, o.fusion, o.prune != 0, plan);
   return run_plan(s, plan, o);
 }
 
@@ -305,16 +393,42 @@ namespace ket {
 int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
   ket_ctx* c = s->ctx;
   cudaSetDevice(c->device);
-  // Device image: all DevOps of fused passes, then MATK descriptors.
+  const bool prune = o.prune != 0;
+  // Device image: v2 programs (FOp), v1 programs (DevOp), then MATK descriptors.
+  const size_t np = plan.passes.size();
+  std::vector<FOp> fops;
   std::vector<DevOp> devops;
-  std::vector<size_t> pass_off(plan.passes.size(), 0);
-  std::vector<size_t> matk_off(plan.passes.size(), 0);
+  std::vector<size_t> off(np, 0), matk_off(np, 0);
+  std::vector<Pass2Args> p2(np);
+  std::vector<bool> use2(np, false);
   size_t matk_bytes = 0;
-  for (size_t i = 0; i < plan.passes.size(); i++) {
+  for (size_t i = 0; i < np; i++) {
     const Pass& p = plan.passes[i];
-    if (p.fused) {
-      pass_off[i] = devops.size();
-      for (int gi : p.gates) devops.push_back(encode_devop(plan.gates[gi], p, o.prune != 0));
+    if (p.fused && p.m == KET_T2_BITS && s->n >= KET_T2_BITS) {
+      use2[i] = true;
+      std::vector<FOp> prog;
+      Pass2Args& a = p2[i];
+      memset(&a, 0, sizeof(a));
+      plan_program(plan, p, s->precision, prune, prog, a.load_pos, a.store_pos);
+      off[i] = fops.size();
+      fops.insert(fops.end(), prog.begin(), prog.end());
+      a.amp = s->amp;
+      a.nops = (int)prog.size();
+      a.n = s->n;
+      a.L = p.L;
+      a.nh = (int)p.hbits.size();
+      for (int j = 0; j < a.nh; j++) a.hbits[j] = p.hbits[j];
+      uint64_t S = (uint64_t(1) << p.L) - 1;
+      for (int q : p.hbits) S |= uint64_t(1) << q;
+      a.nctx = 0;
+      for (int q = 0; q < s->n; q++)
+        if (!((S >> q) & 1)) a.ctxbits[a.nctx++] = q;
+      a.thr = 1e-14;
+      a.qthr = 1e-7;
+      a.status = c->d_status;
+    } else if (p.fused) {
+      off[i] = devops.size();
+      for (int gi : p.gates) devops.push_back(encode_devop(plan.gates[gi], p, prune));
     } else {
       const Gate& g = plan.gates[p.gates[0]];
       if (g.type == G_MATK) {
@@ -324,36 +438,45 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
       }
     }
   }
-  size_t ops_bytes = ((sizeof(DevOp) * devops.size()) + 255) & ~size_t(255);
-  size_t total = ops_bytes + matk_bytes;
+  const size_t f_bytes = ((sizeof(FOp) * fops.size()) + 255) & ~size_t(255);
+  const size_t d_bytes = ((sizeof(DevOp) * devops.size()) + 255) & ~size_t(255);
+  const size_t total = f_bytes + d_bytes + matk_bytes;
   void* dev = nullptr;
   if (total) {
     int rc = ctx_scratch(c, total, &dev);
     if (rc) return rc;
     std::vector<unsigned char> host(total, 0);
-    if (!devops.empty()) memcpy(host.data(), devops.data(), sizeof(DevOp) * devops.size());
-    for (size_t i = 0; i < plan.passes.size(); i++) {
+    if (!fops.empty()) memcpy(host.data(), fops.data(), sizeof(FOp) * fops.size());
+    if (!devops.empty()) memcpy(host.data() + f_bytes, devops.data(), sizeof(DevOp) * devops.size());
+    for (size_t i = 0; i < np; i++) {
       const Pass& p = plan.passes[i];
       if (p.fused) continue;
       const Gate& g = plan.gates[p.gates[0]];
       if (g.type != G_MATK) continue;
-      unsigned char* dst = host.data() + ops_bytes + matk_off[i];
+      unsigned char* dst = host.data() + f_bytes + d_bytes + matk_off[i];
       int* q = reinterpret_cast<int*>(dst);
       for (size_t j = 0; j < g.tk.size(); j++) q[j] = g.tk[j];
       memcpy(dst + 64, g.mk.data(), 16 * g.mk.size());
     }
+    c->h2d_bytes += total;
     cudaError_t e = cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(ops)");
   }
-  const DevOp* dops = reinterpret_cast<const DevOp*>(dev);
-  for (size_t i = 0; i < plan.passes.size(); i++) {
+  const FOp* dfops = reinterpret_cast<const FOp*>(dev);
+  const DevOp* dops = reinterpret_cast<const DevOp*>((const char*)dev + f_bytes);
+  for (size_t i = 0; i < np; i++) {
     const Pass& p = plan.passes[i];
     cudaError_t e;
-    if (p.fused) {
+    int kind = use2[i] ? PK_FUSED2 : (p.fused ? PK_FUSED1 : PK_GATE);
+    prof_begin(c);
+    if (use2[i]) {
+      p2[i].ops = dfops + off[i];
+      e = launch_fused2(p2[i], s->precision, c->stream);
+    } else if (p.fused) {
       PassArgs a;
       memset(&a, 0, sizeof(a));
       a.amp = s->amp;
-      a.ops = dops + pass_off[i];
+      a.ops = dops + off[i];
       a.nops = (int)p.gates.size();
       a.n = s->n;
       a.m = p.m;
@@ -370,12 +493,28 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
       e = launch_fused(a, s->precision, c->stream);
     } else {
       const Gate& g = plan.gates[p.gates[0]];
-      const void* mk = g.type == G_MATK ? (const void*)((const char*)dev + ops_bytes + matk_off[i]) : nullptr;
+      const void* mk =
+          g.type == G_MATK ? (const void*)((const char*)dev + f_bytes + d_bytes + matk_off[i]) : nullptr;
       e = launch_gate(g, s->precision, s->amp, s->n, mk, c->stream);
     }
+    prof_end(c, kind);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   }
-  return ctx_wait(c);
+  int rc = ctx_wait(c);
+  if (rc) return rc;
+  return check_status(c);
+}
+
+// Read and clear the device status word (set by kernels whose bounded waits ran out).
+int check_status(ket_ctx* c) {
+  int st = 0;
+  cudaError_t e = cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "status read");
+  if (st != 0) {
+    cudaMemset(c->d_status, 0, sizeof(int));
+    return fail(st, "a device-side bounded wait ran out (status " + std::to_string(st) + ")");
+  }
+  return KET_OK;
 }
 
 }  // namespace ket

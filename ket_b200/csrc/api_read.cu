@@ -21,15 +21,24 @@ int check_state(const ket_state* s) {
 
 int h2d(ket_ctx* c, void* dst, const void* src, size_t bytes) {
   if (!bytes) return KET_OK;
+  c->h2d_bytes += bytes;
   cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
   return e == cudaSuccess ? KET_OK : cuda_fail(e, "cudaMemcpyAsync(H2D)");
 }
 int d2h(ket_ctx* c, void* dst, const void* src, size_t bytes) {
   if (!bytes) return KET_OK;
+  c->d2h_bytes += bytes;
   cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
   return e == cudaSuccess ? KET_OK : cuda_fail(e, "cudaMemcpyAsync(D2H)");
 }
 int launched(cudaError_t e) { return e == cudaSuccess ? KET_OK : cuda_fail(e, "kernel launch"); }
+
+// Launch a read-out kernel bracketed for accounting/profiling.
+#define LAUNCH_READ(c, expr) (prof_begin(c), prof_end_ret((c), (expr)))
+int prof_end_ret(ket_ctx* c, cudaError_t e) {
+  prof_end(c, PK_READ);
+  return launched(e);
+}
 
 #define TRY(x) do { int _rc = (x); if (_rc) return _rc; } while (0)
 
@@ -51,7 +60,7 @@ int ket_amplitudes(const ket_state* s, const uint64_t* idx, size_t k, double* ou
   uint64_t* di = (uint64_t*)scr;
   double* dout = (double*)align_up((char*)(di + k), 256);
   TRY(h2d(s->ctx, di, idx, 8 * k));
-  TRY(launched(launch_gather(s->amp, s->precision, di, k, dout, s->ctx->stream)));
+  TRY(LAUNCH_READ(s->ctx, launch_gather(s->amp, s->precision, di, k, dout, s->ctx->stream)));
   TRY(d2h(s->ctx, out, dout, 16 * k));
   return ctx_wait(s->ctx);
 }
@@ -62,7 +71,7 @@ int ket_norm2(const ket_state* s, double* out) {
   void* scr;
   TRY(ctx_scratch(s->ctx, norm2_scratch(s->n) + 64, &scr));
   double* res = (double*)scr;
-  TRY(launched(launch_norm2(s->amp, s->n, s->precision, res + 8, res, s->ctx->stream)));
+  TRY(LAUNCH_READ(s->ctx, launch_norm2(s->amp, s->n, s->precision, res + 8, res, s->ctx->stream)));
   TRY(d2h(s->ctx, out, res, 8));
   return ctx_wait(s->ctx);
 }
@@ -75,7 +84,7 @@ int ket_probs_dense(const ket_state* s, double thr, double* out) {
   void* scr;
   TRY(ctx_scratch(s->ctx, 8 * chunk, &scr));
   for (uint64_t off = 0; off < N; off += chunk) {
-    TRY(launched(launch_probs_dense(s->amp, s->precision, off, chunk, thr, (double*)scr, s->ctx->stream)));
+    TRY(LAUNCH_READ(s->ctx, launch_probs_dense(s->amp, s->precision, off, chunk, thr, (double*)scr, s->ctx->stream)));
     TRY(d2h(s->ctx, out + off, scr, 8 * chunk));
     TRY(ctx_wait(s->ctx));
   }
@@ -90,7 +99,7 @@ int ket_probs_sparse(const ket_state* s, double thr, uint64_t* idx, double* p, u
   void* scr;
   TRY(ctx_scratch(s->ctx, 16 * nb + 512, &scr));
   uint64_t* dcounts = (uint64_t*)scr;
-  TRY(launched(launch_count_kept(s->amp, s->n, s->precision, thr, dcounts, s->ctx->stream)));
+  TRY(LAUNCH_READ(s->ctx, launch_count_kept(s->amp, s->n, s->precision, thr, dcounts, s->ctx->stream)));
   std::vector<uint64_t> counts(nb), offs(nb);
   TRY(d2h(s->ctx, counts.data(), dcounts, 8 * nb));
   TRY(ctx_wait(s->ctx));
@@ -104,7 +113,7 @@ int ket_probs_sparse(const ket_state* s, double thr, uint64_t* idx, double* p, u
   uint64_t* didx = (uint64_t*)align_up((char*)(doffs + nb), 256);
   double* dp = (double*)align_up((char*)(didx + ncopy), 256);
   TRY(h2d(s->ctx, doffs, offs.data(), 8 * nb));
-  TRY(launched(launch_compact_kept(s->amp, s->n, s->precision, thr, doffs, ncopy, didx, dp, s->ctx->stream)));
+  TRY(LAUNCH_READ(s->ctx, launch_compact_kept(s->amp, s->n, s->precision, thr, doffs, ncopy, didx, dp, s->ctx->stream)));
   TRY(d2h(s->ctx, idx, didx, 8 * ncopy));
   TRY(d2h(s->ctx, p, dp, 8 * ncopy));
   return ctx_wait(s->ctx);
@@ -119,7 +128,7 @@ int ket_marginals(const ket_state* s, double* out) {
   TRY(ctx_scratch(s->ctx, 8 * (nb * s->n + s->n) + 512, &scr));
   double* res = (double*)scr;
   double* partial = (double*)align_up((char*)(res + s->n), 256);
-  TRY(launched(launch_marginals(s->amp, s->n, s->precision, partial, res, s->ctx->stream)));
+  TRY(LAUNCH_READ(s->ctx, launch_marginals(s->amp, s->n, s->precision, partial, res, s->ctx->stream)));
   TRY(d2h(s->ctx, out, res, 8 * s->n));
   return ctx_wait(s->ctx);
 }
@@ -144,7 +153,7 @@ int ket_marginal_dist(const ket_state* s, const int* qubits, int m, double* out)
   TRY(ctx_scratch(s->ctx, 8 * (nb * width + width) + 512, &scr));
   double* res = (double*)scr;
   double* partial = (double*)align_up((char*)(res + width), 256);
-  TRY(launched(launch_marginal_dist(s->amp, s->n, s->precision, spec, partial, res, s->ctx->stream)));
+  TRY(LAUNCH_READ(s->ctx, launch_marginal_dist(s->amp, s->n, s->precision, spec, partial, res, s->ctx->stream)));
   TRY(d2h(s->ctx, out, res, 8 * width));
   return ctx_wait(s->ctx);
 }
@@ -160,7 +169,7 @@ int ket_sample(const ket_state* s, const double* r, size_t shots, double thr, ui
   uint64_t* dout = (uint64_t*)align_up((char*)(dr + shots), 256);
   void* work = align_up((char*)(dout + shots), 256);
   TRY(h2d(s->ctx, dr, r, 8 * shots));
-  TRY(launched(launch_sample(s->amp, s->n, s->precision, thr, dr, shots, work, dout, s->ctx->stream)));
+  TRY(LAUNCH_READ(s->ctx, launch_sample(s->amp, s->n, s->precision, thr, dr, shots, work, dout, s->ctx->stream)));
   TRY(d2h(s->ctx, out, dout, 8 * shots));
   return ctx_wait(s->ctx);
 }
@@ -198,7 +207,7 @@ int pauli_terms_expect(const ket_state* s, const std::vector<Term>& terms, doubl
   double* res = (double*)scr;
   double* partial = (double*)align_up((char*)(res + gl.size()), 256);
   for (size_t i = 0; i < gl.size(); i++)
-    TRY(launched(launch_pauli_group(s->amp, s->n, s->precision, gl[i], partial, res + i, s->ctx->stream)));
+    TRY(LAUNCH_READ(s->ctx, launch_pauli_group(s->amp, s->n, s->precision, gl[i], partial, res + i, s->ctx->stream)));
   std::vector<double> h(gl.size());
   TRY(d2h(s->ctx, h.data(), res, 8 * gl.size()));
   TRY(ctx_wait(s->ctx));

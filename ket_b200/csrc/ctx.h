@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/ket_sv.h"
 #include "engine.h"
@@ -20,6 +21,14 @@ struct ket_ctx {
   size_t scratch2_bytes = 0;
   cudaGraphExec_t graph_exec = nullptr;  // last captured batch launch
   uint64_t graph_key = 0;
+  // launch accounting and optional per-launch CUDA-event timing
+  int* d_status = nullptr;        // device status word written by kernels (bounded waits)
+  uint64_t launches = 0;
+  uint64_t h2d_bytes = 0, d2h_bytes = 0;  // host<->device copies made by the context
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> prof_kind;     // kind of each timed launch
+  size_t prof_next = 0;           // next free event pair
 };
 
 struct ket_state {
@@ -39,5 +48,12 @@ int dev_alloc(void** p, size_t bytes);
 int ctx_scratch(ket_ctx* ctx, size_t bytes, void** out);
 int ctx_wait(ket_ctx* ctx);
 int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o);
+int check_status(ket_ctx* c);
+
+// Launch kinds reported by ket_ctx_profile_read.
+enum { PK_FUSED2 = 0, PK_FUSED1 = 1, PK_GATE = 2, PK_READ = 3, PK_ADJOINT = 4, PK_BATCH = 5 };
+// Bracket one kernel launch on ctx->stream (counts it; times it when profiling).
+void prof_begin(ket_ctx* c);
+void prof_end(ket_ctx* c, int kind);
 
 }  // namespace ket

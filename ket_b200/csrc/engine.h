@@ -53,7 +53,7 @@ struct Plan {
 int lower_ops(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, bool prune,
               std::vector<Gate>& out, std::string& err);
 // Greedy fusion planner.
-void plan_passes(int n, int precision, int fusion, Plan& plan);
+void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& plan);
 
 // Tile width used for fused passes at a given precision.
 int tile_qubits(int precision, int fusion);

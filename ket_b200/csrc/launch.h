@@ -34,6 +34,64 @@ struct PassArgs {
   double thr, qthr;  // pruning threshold and its square root
 };
 
+// ---------------------------------------------------------------- register-tiled pass
+// The tile's 12 bits are split into roles: 5 lane bits, 3 warp bits, 4 register
+// bits (each thread holds 16 amplitudes).  A layout lists, for lane bits 0..4,
+// warp bits 0..2 and register bits 0..3, which tile bit plays that role.
+#define KET_T2_BITS 12
+enum FOpType : uint8_t {
+  FO_EXCH = 0,    // re-layout the tile through shared memory
+  FO_MAT1R = 1,   // 2x2 on register bit a
+  FO_MAT1L = 2,   // 2x2 on lane bit a (warp shuffles)
+  FO_X1R = 3,     // X on register bit a
+  FO_X1L = 4,     // X on lane bit a
+  FO_SWAPS = 5,   // swap tile bits a, b (controls allowed) through shared memory
+  FO_MAT2S = 6,   // 4x4 on tile bits a (MSB), b through shared memory
+  FO_RELABEL = 11,// no data movement: the layout's role -> tile-bit map changes (uncontrolled SWAP)
+  FO_DIAG = 7,    // diag phase on tile bits d0 (and d1), anywhere (general form)
+  FO_DIAGR = 8,   // diag(m0, m1) on register bit a
+  FO_DIAGT = 9,   // diag(m0, m1) on thread-id bit a (lane 0-4 / warp 5-7): one phase per thread
+  FO_DIAGX = 10,  // diag(m0, m1) on a qubit outside the tile (mask dg0): one phase per tile
+};
+
+// flags
+#define FOF_PRUNE 1u    // flush computed amplitudes with |a|^2 < 1e-14
+#define FOF_REAL 2u     // MAT1: every matrix entry is real
+#define FOF_D0ONE 4u    // DIAG*: m0 == 1 exactly (only bit-1 amplitudes change)
+#define FOF_RXFORM 8u   // MAT1: m00, m11 real and m01, m10 imaginary (Rx-like)
+#define FOF_LAZY 16u    // DIAGT/DIAGX without register controls: folded into a per-thread phase
+
+struct FOp {
+  uint8_t type, a, b, flags;
+  uint8_t pos[KET_T2_BITS];   // FO_EXCH: new layout
+  uint32_t creg;              // controls on register bits (bit k = register bit k)
+  uint32_t cthr;              // controls on thread-id bits (lane bits 0-4, warp bits 5-7)
+  uint32_t ctile;             // FO_DIAG: controls inside the tile (tile-bit mask)
+  int16_t d0, d1;             // FO_DIAG: tile bit of t0 / t1, -1 = outside the tile, -2 = none
+  uint64_t cctx;              // controls on global bits outside the tile
+  uint64_t dg0, dg1;          // FO_DIAG*: global mask of t0 / t1 when outside the tile
+  uint64_t pad;               // header = 64 bytes
+  double m[32];
+};
+
+struct Pass2Args {
+  void* amp;
+  const FOp* ops;
+  int nops;
+  int n, L, nh, nctx;
+  uint8_t load_pos[KET_T2_BITS];   // layout used for the global load
+  uint8_t store_pos[KET_T2_BITS];  // layout in force at the global store
+  int hbits[KET_MAX_TILE_HBITS];   // global qubit of tile bits L..11
+  int ctxbits[KET_MAX_CTX_BITS];
+  double thr, qthr;
+  int* status;                     // device status word: set to KET_ERR_TIMEOUT if a bounded wait ran out
+};
+
+// Lower one fused pass to a register-tiled program (segments + exchanges).
+void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, std::vector<FOp>& prog,
+                  uint8_t load_pos[KET_T2_BITS], uint8_t store_pos[KET_T2_BITS]);
+cudaError_t launch_fused2(const Pass2Args& a, int precision, cudaStream_t s);
+
 struct Ctx;
 
 // Encode a gate for a fused pass.

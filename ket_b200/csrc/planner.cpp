@@ -16,6 +16,7 @@
 // deferred to a later pass blocks every later gate that shares a qubit.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "engine.h"
@@ -65,6 +66,13 @@ void lower_diag2(Gate& g) {
 }
 
 bool fusable(const Gate& g) { return g.type != G_MATK || g.tk.size() <= 2; }
+
+// Gates that can change amplitude magnitudes.  With the reference's per-gate
+// pruning (accumulate(), statevector.ts:19-27) their relative order must be
+// kept: pruning after G1 then G2 differs from pruning after G2 then G1.
+// Diagonal phases and permutations preserve magnitudes, so they may move past
+// mixing gates on other qubits without changing what gets pruned.
+bool is_mixing(const Gate& g) { return g.type == G_MAT1 || g.type == G_MAT2 || g.type == G_MATK; }
 
 }  // namespace
 
@@ -201,16 +209,19 @@ int lower_ops(int n, const ket_op* ops, size_t nops, const double* mats, size_t 
 }
 
 int tile_qubits(int precision, int fusion) {
-  int mx = precision == KET_C64 ? 13 : 12;
+  int mx = 12;
   if (fusion > 0) return std::max(6, std::min(fusion, mx));
   return mx;
 }
 
-void plan_passes(int n, int precision, int fusion, Plan& plan) {
+void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& plan) {
   plan.passes.clear();
   const std::vector<Gate>& G = plan.gates;
   const int M = std::min(n, tile_qubits(precision, fusion));
-  const int L = std::min(n, 5);
+  // L low qubits are contiguous in every tile: 2^L amplitudes per HBM chunk
+  // (one TMA bulk copy each, >= 32 bytes so both precisions stay 16-byte sized).
+  static int Lenv = getenv("KET_TILE_LOW") ? atoi(getenv("KET_TILE_LOW")) : 5;
+  const int L = std::min(n, std::max(2, std::min(5, Lenv)));
   const uint64_t low = (L >= 64) ? ~uint64_t(0) : bit(L) - 1;
   std::vector<int> pending(G.size());
   for (size_t i = 0; i < G.size(); i++) pending[i] = (int)i;
@@ -227,24 +238,48 @@ void plan_passes(int n, int precision, int fusion, Plan& plan) {
     return;
   }
 
-  while (!pending.empty()) {
-    // Choose the tile's qubit set along the frontier of pending gates.
-    uint64_t S = (M >= n) ? (n >= 64 ? ~uint64_t(0) : bit(n) - 1) : low;
-    for (;;) {
-      bool grew = false;
-      uint64_t B = 0;
-      for (int gi : pending) {
-        const Gate& g = G[gi];
-        uint64_t qs = gate_qubits(g);
-        if (qs & B) { B |= qs; continue; }
-        if (!fusable(g)) { B |= qs; continue; }
-        uint64_t mix = gate_mix(g);
-        if ((mix & ~S) == 0) continue;
-        uint64_t miss = mix & ~S;
-        if (__builtin_popcountll(S | miss) <= M) { S |= miss; grew = true; break; }
+  // Gates a pass over tile set S would absorb (the sweep below, counted).
+  auto absorbed = [&](uint64_t S, std::vector<uint64_t>* cand) -> int {
+    uint64_t B = 0;
+    bool mixblocked = false;
+    int taken = 0;
+    for (int gi : pending) {
+      const Gate& g = G[gi];
+      uint64_t qs = gate_qubits(g);
+      bool mixing = keep_mix_order && is_mixing(g);
+      bool blocked = (qs & B) || (mixing && mixblocked) || !fusable(g);
+      uint64_t miss = gate_mix(g) & ~S;
+      if (blocked || miss) {
+        if (!blocked && miss && cand && cand->size() < 16) {
+          bool dup = false;
+          for (uint64_t c : *cand) dup |= (c == miss);
+          if (!dup) cand->push_back(miss);
+        }
         B |= qs;
+        if (mixing) mixblocked = true;
+        continue;
       }
-      if (!grew) break;
+      taken++;
+    }
+    return taken;
+  };
+
+  while (!pending.empty()) {
+    // Grow the tile's qubit set one step at a time, each time adding the
+    // missing targets of whichever frontier gate lets the pass absorb most.
+    uint64_t S = (M >= n) ? (n >= 64 ? ~uint64_t(0) : bit(n) - 1) : low;
+    while (__builtin_popcountll(S) < M) {
+      std::vector<uint64_t> cand;
+      absorbed(S, &cand);
+      int best = -1;
+      uint64_t bestS = S;
+      for (uint64_t c : cand) {
+        if (__builtin_popcountll(S | c) > M) continue;
+        int v = absorbed(S | c, nullptr);
+        if (v > best) { best = v; bestS = S | c; }
+      }
+      if (best < 0) break;
+      S = bestS;
     }
     // Sweep: take every gate applicable in tile S, preserving order.
     Pass p;
@@ -252,11 +287,18 @@ void plan_passes(int n, int precision, int fusion, Plan& plan) {
     p.m = M;
     p.L = L;
     uint64_t B = 0;
+    bool mixblocked = false;
     std::vector<int> rest;
     for (int gi : pending) {
       const Gate& g = G[gi];
       uint64_t qs = gate_qubits(g);
-      if ((qs & B) || !fusable(g) || (gate_mix(g) & ~S)) { B |= qs; rest.push_back(gi); continue; }
+      bool mixing = keep_mix_order && is_mixing(g);
+      if ((qs & B) || (mixing && mixblocked) || !fusable(g) || (gate_mix(g) & ~S)) {
+        B |= qs;
+        if (mixing) mixblocked = true;
+        rest.push_back(gi);
+        continue;
+      }
       p.gates.push_back(gi);
     }
     if (p.gates.empty()) {

@@ -1,0 +1,247 @@
+// program.cpp -- lowers one fused pass to the register-tiled program run by
+// k_fused2: a sequence of gate ops, each addressed by the role (register bit,
+// lane bit, anywhere-diagonal) its target plays in the current tile layout,
+// with a layout exchange inserted whenever the next gate's target sits on a
+// warp bit (or a two-qubit gate needs both targets in registers).
+//
+// Layout choice looks ahead: the tile bits needed soonest become register
+// and lane bits, the ones needed latest become warp bits.  The first and last
+// layouts keep lane bit l on tile bit l (l < 5) so the global load and store
+// of each warp touch contiguous 128-byte lines.
+#include <algorithm>
+#include <cstring>
+
+#include "launch.h"
+
+namespace ket {
+
+namespace {
+
+const int NB = KET_T2_BITS;
+
+struct Lay {
+  int pos[NB];   // role -> tile bit: 0..4 lanes, 5..7 warps, 8..11 registers
+  int role[NB];  // tile bit -> role
+};
+
+void fill_roles(Lay& l) {
+  for (int r = 0; r < NB; r++) l.role[l.pos[r]] = r;
+}
+
+bool a0_compatible(const Lay& l) {
+  for (int i = 0; i < 5; i++)
+    if (l.pos[i] != i) return false;
+  return true;
+}
+
+bool is_reg(const Lay& l, int tb) { return l.role[tb] >= 8; }
+bool is_lane(const Lay& l, int tb) { return l.role[tb] < 5; }
+
+// Tile-local bit of a global qubit, -1 when outside the tile.
+int tpos(const Pass& p, int q) {
+  if (q < 0) return -1;
+  if (q < p.L) return q;
+  for (size_t j = 0; j < p.hbits.size(); j++)
+    if (p.hbits[j] == q) return p.L + (int)j;
+  return -1;
+}
+
+bool needs_two_regs(const Gate&) { return false; }
+
+bool fits(const Gate& g, const Pass& p, const Lay& l) {
+  switch (g.type) {
+    case G_DIAG1: case G_DIAG2: case G_SWAP: case G_MAT2: return true;  // SWAP/MAT2 work in any layout
+    case G_MAT1: case G_X1: {
+      int t = tpos(p, g.t0);
+      return is_reg(l, t) || is_lane(l, t);
+    }
+    default: return false;
+  }
+}
+
+// Choose a layout for the gates from index `from` on.
+Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision) {
+  const int INF = 1 << 30;
+  int next[NB], nreg[NB];
+  for (int b = 0; b < NB; b++) { next[b] = INF; nreg[b] = 0; }
+  for (size_t i = from; i < p.gates.size(); i++) {
+    const Gate& g = plan.gates[p.gates[i]];
+    if (g.type == G_DIAG1 || g.type == G_DIAG2) continue;
+    int ts[2] = {tpos(p, g.t0), g.type == G_SWAP || g.type == G_MAT2 ? tpos(p, g.t1) : -1};
+    for (int t : ts) {
+      if (t < 0) continue;
+      if (next[t] == INF) { next[t] = (int)i; nreg[t] = needs_two_regs(g) ? 1 : 0; }
+    }
+  }
+  // the current gate's two-qubit targets must be registers
+  std::vector<int> must;
+  if (from < p.gates.size()) {
+    const Gate& g = plan.gates[p.gates[from]];
+    if (needs_two_regs(g)) { must.push_back(tpos(p, g.t0)); must.push_back(tpos(p, g.t1)); }
+  }
+  std::vector<int> order(NB);
+  for (int b = 0; b < NB; b++) order[b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    if (next[x] != next[y]) return next[x] < next[y];
+    return nreg[x] > nreg[y];
+  });
+  Lay l;
+  std::vector<bool> used(NB, false);
+  std::vector<int> regs, lanes, warps;
+  auto take_reg = [&](int b) { regs.push_back(b); used[b] = true; };
+  if (a0) {
+    for (int b = 0; b < 5; b++) { lanes.push_back(b); used[b] = true; }
+    for (int b : must) if (!used[b] && (int)regs.size() < 4) take_reg(b);
+    for (int b : order) if (!used[b] && (int)regs.size() < 4 && b >= 5) take_reg(b);
+    for (int b : order) if (!used[b]) { warps.push_back(b); used[b] = true; }
+  } else {
+    for (int b : must) if (!used[b] && (int)regs.size() < 4) take_reg(b);
+    // prefer registers for bits whose first use needs two registers
+    for (int b : order) if (!used[b] && (int)regs.size() < 4 && nreg[b]) take_reg(b);
+    for (int b : order) if (!used[b] && (int)regs.size() < 4) take_reg(b);
+    for (int b : order) if (!used[b] && (int)lanes.size() < 5) { lanes.push_back(b); used[b] = true; }
+    for (int b = 0; b < NB; b++) if (!used[b]) { warps.push_back(b); used[b] = true; }
+    // Shared-memory bank spread: the swizzle folds tile bits mod 3 (c128) or
+    // mod 4 (c64) into the low bits, so lanes 0..2 (0..3) should cover
+    // distinct residues.
+    const int mod = precision == KET_C64 ? 4 : 3;
+    std::vector<int> ln = lanes, out;
+    for (int r = 0; r < mod && !ln.empty(); r++) {
+      for (size_t k = 0; k < ln.size(); k++)
+        if (ln[k] % mod == r) { out.push_back(ln[k]); ln.erase(ln.begin() + k); break; }
+    }
+    for (int b : ln) out.push_back(b);
+    lanes = out;
+  }
+  for (int i = 0; i < 5; i++) l.pos[i] = lanes[i];
+  for (int i = 0; i < 3; i++) l.pos[5 + i] = warps[i];
+  for (int i = 0; i < 4; i++) l.pos[8 + i] = regs[i];
+  fill_roles(l);
+  return l;
+}
+
+FOp make_exch(const Lay& l) {
+  FOp o;
+  memset(&o, 0, sizeof(o));
+  o.type = FO_EXCH;
+  for (int i = 0; i < NB; i++) o.pos[i] = (uint8_t)l.pos[i];
+  return o;
+}
+
+// Split a control mask over the current layout.
+void controls(const Gate& g, const Pass& p, const Lay& l, FOp& o) {
+  for (int q = 0; q < 64; q++) {
+    if (!((g.cmask >> q) & 1)) continue;
+    int t = tpos(p, q);
+    if (t < 0) { o.cctx |= uint64_t(1) << q; continue; }
+    o.ctile |= 1u << t;
+    int r = l.role[t];
+    if (r >= 8) o.creg |= 1u << (r - 8);
+    else o.cthr |= 1u << r;  // lanes 0..4 -> tid bits 0..4, warps 5..7 -> tid bits 5..7
+  }
+}
+
+FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
+  FOp o;
+  memset(&o, 0, sizeof(o));
+  o.flags = (g.prune && prune) ? FOF_PRUNE : 0;
+  o.d0 = o.d1 = -2;
+  controls(g, p, l, o);
+  int t0 = tpos(p, g.t0), t1 = tpos(p, g.t1);
+  switch (g.type) {
+    case G_MAT1: case G_X1: {
+      bool reg = is_reg(l, t0);
+      o.type = g.type == G_MAT1 ? (reg ? FO_MAT1R : FO_MAT1L) : (reg ? FO_X1R : FO_X1L);
+      o.a = (uint8_t)(reg ? l.role[t0] - 8 : l.role[t0]);
+      bool real = true;
+      for (int k = 0; k < 4; k++) {
+        o.m[2 * k] = g.m[k].re;
+        o.m[2 * k + 1] = g.m[k].im;
+        real = real && g.m[k].im == 0.0;
+      }
+      bool rx = g.m[0].im == 0.0 && g.m[3].im == 0.0 && g.m[1].re == 0.0 && g.m[2].re == 0.0;
+      if (g.type == G_MAT1 && real) o.flags |= FOF_REAL;
+      else if (g.type == G_MAT1 && rx) o.flags |= FOF_RXFORM;
+      break;
+    }
+    case G_SWAP:
+      o.type = FO_SWAPS;
+      o.a = (uint8_t)t0;
+      o.b = (uint8_t)t1;
+      break;
+    case G_MAT2:
+      o.type = FO_MAT2S;
+      o.a = (uint8_t)t0;
+      o.b = (uint8_t)t1;
+      for (int k = 0; k < 16; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
+      break;
+    case G_DIAG1: {
+      // A phase keeps |a| (to the last bit), so the reference's pruning after
+      // it can only fire on amplitudes it already pruned: no prune flag.
+      o.flags &= ~FOF_PRUNE;
+      for (int k = 0; k < 2; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
+      if (g.m[0].re == 1.0 && g.m[0].im == 0.0) o.flags |= FOF_D0ONE;
+      if (t0 < 0) {
+        o.type = FO_DIAGX;
+        o.dg0 = uint64_t(1) << g.t0;
+      } else if (is_reg(l, t0)) {
+        o.type = FO_DIAGR;
+        o.a = (uint8_t)(l.role[t0] - 8);
+      } else {
+        o.type = FO_DIAGT;
+        o.a = (uint8_t)l.role[t0];  // lanes 0..4 -> tid bits 0..4, warps 5..7 -> tid bits 5..7
+      }
+      if (o.type != FO_DIAGR && o.creg == 0) o.flags |= FOF_LAZY;
+      break;
+    }
+    case G_DIAG2: {
+      o.flags &= ~FOF_PRUNE;
+      o.type = FO_DIAG;
+      o.d0 = (int16_t)(t0 >= 0 ? t0 : -1);
+      if (t0 < 0) o.dg0 = uint64_t(1) << g.t0;
+      o.d1 = (int16_t)(t1 >= 0 ? t1 : -1);
+      if (t1 < 0) o.dg1 = uint64_t(1) << g.t1;
+      for (int k = 0; k < 4; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
+      o.creg = 0;
+      o.cthr = 0;
+      break;
+    }
+    default: break;
+  }
+  return o;
+}
+
+}  // namespace
+
+void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, std::vector<FOp>& prog,
+                  uint8_t load_pos[KET_T2_BITS], uint8_t store_pos[KET_T2_BITS]) {
+  prog.clear();
+  Lay cur = choose(plan, p, 0, true, precision);
+  for (int i = 0; i < NB; i++) load_pos[i] = (uint8_t)cur.pos[i];
+  for (size_t i = 0; i < p.gates.size(); i++) {
+    const Gate& g = plan.gates[p.gates[i]];
+    if (g.type == G_SWAP && g.cmask == 0) {
+      // An uncontrolled SWAP moves no data: the two tile bits trade roles.
+      int t0 = tpos(p, g.t0), t1 = tpos(p, g.t1);
+      std::swap(cur.pos[cur.role[t0]], cur.pos[cur.role[t1]]);
+      fill_roles(cur);
+      FOp o = make_exch(cur);
+      o.type = FO_RELABEL;
+      prog.push_back(o);
+      continue;
+    }
+    if (!fits(g, p, cur)) {
+      cur = choose(plan, p, i, false, precision);
+      prog.push_back(make_exch(cur));
+    }
+    prog.push_back(make_op(g, p, cur, prune));
+  }
+  if (!a0_compatible(cur)) {
+    Lay last = choose(plan, p, p.gates.size(), true, precision);
+    cur = last;
+    prog.push_back(make_exch(cur));
+  }
+  for (int i = 0; i < NB; i++) store_pos[i] = (uint8_t)cur.pos[i];
+}
+
+}  // namespace ket

@@ -45,6 +45,7 @@
 #include <unordered_map>
 #include <unordered_set>
 #include <algorithm>
+#include <chrono>
 #include <stdexcept>
 #ifdef _OPENMP
 #include <omp.h>
@@ -995,6 +996,47 @@ int orc_regular3(int n, uint32_t* state, int* edges) {
   for (size_t i = 0; i < e.size(); i++) { edges[2 * i] = e[i].first; edges[2 * i + 1] = e[i].second; }
   *state = rng.s;
   return (int)e.size();
+}
+
+// CPU-baseline timing: simulate ops [0, first) untimed, then time ops
+// [first, first+count) in the given mode (sparse = the reference's algorithm).
+// Returns the amplitude updates done in the timed range (sum over timed ops of
+// the entries the op visits: the map size for the sparse path, 2^n dense).
+uint64_t orc_time_ops(void* cp, uint64_t init, int mode, int first, int count, double* seconds) {
+  const Circuit& c = *(Circuit*)cp;
+  Circuit pre{c.n, {}}, timed{c.n, {}};
+  for (int i = 0; i < (int)c.ops.size(); i++) {
+    if (i < first) pre.ops.push_back(c.ops[i]);
+    else if (i < first + count) timed.ops.push_back(c.ops[i]);
+  }
+  State* s = simulate(pre, init, mode);
+  uint64_t updates = 0;
+  auto t0 = std::chrono::steady_clock::now();
+  if (mode == 0) {
+    for (const Op& op : timed.ops) {
+      updates += s->sv.size();
+      switch (op.kind) {
+        case K_SINGLE: s->sv = applySingle(s->sv, op.q[0], op.m, s->ps); break;
+        case K_CNOT: s->sv = applyCNOT(s->sv, op.q[0], op.q[1]); break;
+        case K_CONTROLLED: s->sv = applyControlled(s->sv, op.q[0], op.q[1], op.m, s->ps); break;
+        case K_SWAP: s->sv = applySWAP(s->sv, op.q[0], op.q[1]); break;
+        case K_TOFFOLI: s->sv = applyToffoli(s->sv, op.q[0], op.q[1], op.q[2]); break;
+        case K_CSWAP: s->sv = applyCSwap(s->sv, op.q[0], op.q[1], op.q[2]); break;
+        case K_CSRSWAP: s->sv = applyCsrSwap(s->sv, op.q[0], op.q[1], op.q[2], s->ps); break;
+        case K_TWO: s->sv = applyTwo(s->sv, op.q[0], op.q[1], op.m, s->ps); break;
+        case K_UNITARY: s->sv = applyUnitary(s->sv, op.q, op.m, s->ps); break;
+        case K_BARRIER: break;
+      }
+    }
+  } else {
+    for (const Op& op : timed.ops) {
+      updates += s->d.a.size();
+      dense_apply(s->d, op);
+    }
+  }
+  *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  delete s;
+  return updates;
 }
 
 uint32_t orc_prng_next(uint32_t* state) { Prng r(*state); uint32_t v = r.next_u32(); *state = r.s; return v; }

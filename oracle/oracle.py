@@ -80,6 +80,7 @@ def lib():
         "orc_brickwork": (vp, [i32, i32, u32, i32, P(u32)]),
         "orc_regular3": (i32, [i32, P(u32), P(i32)]),
         "orc_prng_next": (u32, [P(u32)]),
+        "orc_time_ops": (u64, [vp, u64, i32, i32, i32, P(dbl)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -165,6 +166,13 @@ class OCircuit:
 
     def simulate(self, init: int = 0, mode: int = SPARSE) -> "OState":
         return OState(self._L.orc_simulate(self.h_, init, mode), self.qubits)
+
+    def time_ops(self, first: int, count: int, init: int = 0, mode: int = SPARSE):
+        """(seconds, amplitude updates) for ops [first, first+count) after
+        simulating ops [0, first) untimed."""
+        sec = C.c_double()
+        upd = self._L.orc_time_ops(self.h_, init, mode, first, count, C.byref(sec))
+        return sec.value, int(upd)
 
     def expectation(self, pauli: str, init: int = 0, mode: int = SPARSE) -> float:
         return self._L.orc_expectation(self.h_, pauli.encode(), init, mode)

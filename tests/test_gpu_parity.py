@@ -196,7 +196,9 @@ def test_c64_state_close_to_c128():
     kc, _ = W.brickwork_circuit(14, 10, 42)
     a128 = kc._state(None, precision=0).amplitudes_dense()
     a64 = kc._state(None, precision=KET_C64).amplitudes_dense()
-    fid = abs(np.vdot(a128, a64)) ** 2
+    n64 = np.vdot(a64, a64).real
+    fid = abs(np.vdot(a128, a64)) ** 2 / n64           # a128 has unit norm
+    assert abs(n64 - 1) < 1e-5                           # FP32 gate entries drift the norm
     assert fid > 1 - 1e-9 and np.max(np.abs(a128 - a64)) < 1e-5
 
 
