@@ -213,6 +213,16 @@ KET_API int ket_adjoint_gradient(ket_ctx* ctx, int nqubits, uint64_t init, const
                          const double* params, int nparams, int batch, int nterms, const double* coeffs,
                          const char* pauli_ops, int checkpoint_every, double* energy, double* grad);
 
+/* Parameter-shift gradient on the same engine, the reference's algorithm
+ * (gradient(), algorithms.ts:536-547): 2*nparams + 1 full simulations per
+ * parameter vector, grad_k = (E(theta + pi/2 e_k) - E(theta - pi/2 e_k)) / 2.
+ * prune: 1 = the reference's per-gate pruning, 0 = plain dense.  Same arguments
+ * as ket_adjoint_gradient otherwise. */
+KET_API int ket_shift_gradient(ket_ctx* ctx, int nqubits, uint64_t init, const ket_op* ops, size_t nops,
+                               const double* mats, size_t nmat, const ket_param_binding* binds, size_t nbinds,
+                               const double* params, int nparams, int batch, int nterms, const double* coeffs,
+                               const char* pauli_ops, int prune, double* energy, double* grad);
+
 /* ---------------------------------------------------------------- batching */
 /* QAOA MaxCut batch: instance i has n[i] qubits, ne[i] edges at edges[2*eoff[i] ...],
  * p layers with gamma[i*p + l], beta[i*p + l].  Circuit: H on all qubits, then per layer

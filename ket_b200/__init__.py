@@ -9,6 +9,7 @@ from .circuit import Circuit, DeviceState, Distribution, flatten_ops, make_prng
 from .algorithms import (AnsatzFn, MinimizeResult, PauliTerm, efficientSU2, gradient, gradient_shift, iqft,
                          maxCutHamiltonian, minimize, qaoa, qft, realAmplitudes, vqe)
 from . import gates
+from .batch import batch_qaoa
 
 __all__ = ["Circuit", "Distribution", "DeviceState", "flatten_ops", "make_prng", "KET_C128", "KET_C64", "KetError",
            "RangeError", "AnsatzFn", "MinimizeResult", "PauliTerm", "efficientSU2", "gradient", "gradient_shift",

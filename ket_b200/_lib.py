@@ -12,7 +12,7 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libket_sv.so")
+LIB_PATH = os.environ.get("KET_SV_LIB") or os.path.join(_HERE, "libket_sv.so")
 
 KET_OK, KET_ERR_RANGE, KET_ERR_TYPE, KET_ERR_OOM, KET_ERR_CUDA, KET_ERR_TIMEOUT, KET_ERR_UNSUPPORTED = range(7)
 KET_C128, KET_C64 = 0, 1
@@ -95,6 +95,8 @@ def lib():
             "ket_expect_pauli_sum": (i32, [vp, i32, P(dbl), C.c_char_p, P(dbl)]),
             "ket_adjoint_gradient": (i32, [vp, i32, u64, P(ket_op), sz, P(dbl), sz, P(ket_param_binding), sz,
                                            P(dbl), i32, i32, i32, P(dbl), C.c_char_p, i32, P(dbl), P(dbl)]),
+            "ket_shift_gradient": (i32, [vp, i32, u64, P(ket_op), sz, P(dbl), sz, P(ket_param_binding), sz,
+                                         P(dbl), i32, i32, i32, P(dbl), C.c_char_p, i32, P(dbl), P(dbl)]),
             "ket_batch_qaoa": (i32, [vp, i32, P(i32), P(i32), P(C.c_int64), P(i32), i32, P(dbl), P(dbl), i32,
                                      P(dbl)]),
         }

@@ -178,6 +178,8 @@ def gradient(ansatz, hamiltonian, params: Sequence[float], method: str = "auto")
     if method == "shift":
         return gradient_shift(ansatz, hamiltonian, params)
     from .adjoint import adjoint_gradient, TraceError
+    if len(params) == 0:
+        return []
     try:
         _, g = adjoint_gradient(ansatz, hamiltonian, [list(params)])
         return [float(v) for v in g[0]]

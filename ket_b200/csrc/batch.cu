@@ -1,0 +1,377 @@
+// batch.cu -- thousands of QAOA MaxCut circuits of uneven width in one
+// persistent launch (ket_batch_qaoa).
+//
+// Each instance: H on all n qubits, then per layer exp(-i gamma Z_u Z_v) on
+// every edge and Rx(2 beta) on every qubit; output <C> = sum_e (1 - <Z_u Z_v>)/2.
+// The reference builds the same circuit as qaoa(n, E, -2 gamma, beta)
+// (algorithms.ts:260-276: cnot . rz . cnot per edge) and measures it with
+// vqe(., maxCutHamiltonian(n, E)) (algorithms.ts:231-241, 301-336).
+//
+// Work items are pulled from a global queue by a persistent grid:
+//   * an instance of n <= TILE qubits is one item, simulated entirely in
+//     shared memory (all layers and the <C> reduction);
+//   * a wider instance is split into 2p passes of tiles of 2^TILE amplitudes
+//     (pass A of a layer: the cost phase, which is diagonal, plus Rx on qubits
+//     0..TILE-1; pass B: Rx on the remaining qubits).  A tile of pass k waits
+//     (bounded spin, error flag on timeout) until every tile of pass k-1 of
+//     its instance has been written back; the queue hands items out in an
+//     order where everything a tile waits on was handed out earlier, so the
+//     fully resident grid cannot deadlock.
+// The cost phase exp(-i gamma (|E| - 2 cut(x))) takes cut(x) from the edge
+// masks and a per-layer table of |E|+1 phases.  <C> partials are written per
+// (instance, tile) and reduced in a fixed order.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "ctx.h"
+#include "launch.h"
+
+namespace ket {
+
+namespace {
+
+#define KQ_MAX_EDGES 64
+#define KQ_MAX_P 16
+
+struct QInst {
+  int n, ne, p, ntiles;     // ntiles = 2^(n - tile) for split instances, 1 otherwise
+  int64_t state;            // offset (amplitudes) of the instance's state in the workspace (split only)
+  int64_t edge_off;         // first edge in the edge array
+  int64_t part_off;         // first <C> partial of the instance
+};
+
+struct QItem {
+  int inst;
+  int pass;   // -1: whole instance in shared memory; else pass index 0..2p-1
+  int tile;
+};
+
+struct QArgs {
+  const QInst* inst;
+  const QItem* items;
+  const uint64_t* emask;    // edge masks (1<<u | 1<<v)
+  const double* gamma;      // [inst * p + l]
+  const double* beta;
+  double2* work;            // split-instance states
+  double* part;             // <C> partials
+  unsigned int* next;       // queue head
+  unsigned int* done;       // per instance: tiles finished (pass-major)
+  int* status;
+  int nitems;
+  int tile;                 // tile qubits
+};
+
+__device__ __forceinline__ int cut_of(uint64_t x, const uint64_t* em, int ne) {
+  int c = 0;
+  for (int e = 0; e < ne; e++) c += __popcll(x & em[e]) & 1;
+  return c;
+}
+
+template <int NT>
+__device__ void fill_phase(double2* tab, double gamma, int ne) {
+  for (int c = threadIdx.x; c <= ne; c += NT) {
+    double s, co;
+    sincos(-gamma * (double)(ne - 2 * c), &s, &co);
+    tab[c] = make_double2(co, s);
+  }
+}
+
+// Rx(2 beta) on local bit q of a shared-memory array of 2^m amplitudes.
+template <int NT>
+__device__ void rx_smem(double2* s, int m, int q, double cb, double sb) {
+  const uint32_t half = 1u << (m - 1);
+  for (uint32_t p = threadIdx.x; p < half; p += NT) {
+    uint32_t i0 = insert0_32(p, q), i1 = i0 | (1u << q);
+    double2 a = s[i0], b = s[i1];
+    // [[c, -i s], [-i s, c]]
+    s[i0] = make_double2(fma(cb, a.x, sb * b.y), fma(cb, a.y, -sb * b.x));
+    s[i1] = make_double2(fma(cb, b.x, sb * a.y), fma(cb, b.y, -sb * a.x));
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* s = reinterpret_cast<double2*>(smraw);
+  double2* tab = s + (1u << a.tile);                             // phase table (<= 65 entries)
+  uint64_t* em = reinterpret_cast<uint64_t*>(tab + KQ_MAX_EDGES + 1);
+  double* red = reinterpret_cast<double*>(em + KQ_MAX_EDGES);     // 32 doubles
+  __shared__ int item_sh;
+  const int T = a.tile;
+  for (;;) {
+    if (threadIdx.x == 0) item_sh = (int)atomicAdd(a.next, 1u);
+    __syncthreads();
+    const int it = item_sh;
+    __syncthreads();
+    if (it >= a.nitems) break;
+    const QItem w = a.items[it];
+    const QInst I = a.inst[w.inst];
+    for (int e = threadIdx.x; e < I.ne; e += NT) em[e] = a.emask[I.edge_off + e];
+    const int n = I.n;
+    if (w.pass < 0) {
+      // ---- whole instance in shared memory
+      const uint32_t N = 1u << n;
+      const double amp0 = 1.0 / sqrt((double)N);
+      for (uint32_t i = threadIdx.x; i < N; i += NT) s[i] = make_double2(amp0, 0.0);
+      for (int l = 0; l < I.p; l++) {
+        __syncthreads();
+        fill_phase<NT>(tab, a.gamma[w.inst * I.p + l], I.ne);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < N; i += NT) {
+          const double2 ph = tab[cut_of(i, em, I.ne)];
+          const double2 v = s[i];
+          s[i] = make_double2(fma(ph.x, v.x, -ph.y * v.y), fma(ph.x, v.y, ph.y * v.x));
+        }
+        double sb, cb;
+        sincos(a.beta[w.inst * I.p + l], &sb, &cb);
+        for (int q = 0; q < n; q++) {
+          __syncthreads();
+          rx_smem<NT>(s, n, q, cb, sb);
+        }
+      }
+      __syncthreads();
+      double acc = 0.0;
+      for (uint32_t i = threadIdx.x; i < N; i += NT) {
+        const double2 v = s[i];
+        acc += (v.x * v.x + v.y * v.y) * (double)cut_of(i, em, I.ne);
+      }
+      acc = block_sum<NT>(acc, red);
+      if (threadIdx.x == 0) a.part[I.part_off] = acc;
+      __syncthreads();
+      continue;
+    }
+    // ---- one tile of one pass of a wide instance
+    const int layer = w.pass >> 1;
+    const bool passA = (w.pass & 1) == 0;
+    // tile bits: pass A = qubits 0..T-1; pass B = low (T - (n - T)) qubits + qubits T..n-1
+    const int nhigh = n - T;               // qubits >= T
+    const int lowB = T - nhigh;            // low qubits kept in pass-B tiles
+    if (w.pass > 0) {
+      // wait until every tile of the previous pass has been written back
+      const unsigned int need = (unsigned int)w.pass * (unsigned int)I.ntiles;
+      if (threadIdx.x == 0) {
+        volatile unsigned int* d = a.done + w.inst;
+        uint32_t spins = 0;
+        while (*d < need) {
+          if (++spins > (1u << 24)) { atomicExch(a.status, (int)KET_ERR_TIMEOUT); break; }
+          __nanosleep(200);
+        }
+        __threadfence();
+      }
+      __syncthreads();
+    }
+    double2* g = a.work + I.state;
+    // global index of tile element i
+    auto gidx = [&](uint32_t i) -> uint64_t {
+      if (passA) return ((uint64_t)w.tile << T) | i;
+      const uint64_t lo = i & ((1u << lowB) - 1);
+      const uint64_t hi = (uint64_t)(i >> lowB) << T;                 // qubits T..n-1
+      const uint64_t mid = (uint64_t)w.tile << lowB;                  // qubits lowB..T-1 from the tile id
+      return hi | mid | lo;
+    };
+    const uint32_t TN = 1u << T;
+    if (w.pass == 0) {
+      const double amp0 = 1.0 / sqrt((double)(uint64_t(1) << n));
+      for (uint32_t i = threadIdx.x; i < TN; i += NT) s[i] = make_double2(amp0, 0.0);
+    } else {
+      for (uint32_t i = threadIdx.x; i < TN; i += NT) s[i] = g[gidx(i)];
+    }
+    double sb, cb;
+    sincos(a.beta[w.inst * I.p + layer], &sb, &cb);
+    if (passA) {
+      __syncthreads();
+      fill_phase<NT>(tab, a.gamma[w.inst * I.p + layer], I.ne);
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < TN; i += NT) {
+        const double2 ph = tab[cut_of(gidx(i), em, I.ne)];
+        const double2 v = s[i];
+        s[i] = make_double2(fma(ph.x, v.x, -ph.y * v.y), fma(ph.x, v.y, ph.y * v.x));
+      }
+      for (int q = 0; q < T; q++) {
+        __syncthreads();
+        rx_smem<NT>(s, T, q, cb, sb);
+      }
+    } else {
+      for (int q = lowB; q < T; q++) {
+        __syncthreads();
+        rx_smem<NT>(s, T, q, cb, sb);
+      }
+    }
+    __syncthreads();
+    const bool last = w.pass == 2 * I.p - 1;
+    if (last) {
+      double acc = 0.0;
+      for (uint32_t i = threadIdx.x; i < TN; i += NT) {
+        const double2 v = s[i];
+        acc += (v.x * v.x + v.y * v.y) * (double)cut_of(gidx(i), em, I.ne);
+      }
+      acc = block_sum<NT>(acc, red);
+      if (threadIdx.x == 0) a.part[I.part_off + w.tile] = acc;
+    } else {
+      for (uint32_t i = threadIdx.x; i < TN; i += NT) g[gidx(i)] = s[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(a.done + w.inst, 1u);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_qaoa_reduce(const QInst* inst, int ninst, const double* part, double* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ninst) return;
+  const QInst I = inst[i];
+  double acc = 0.0;
+  for (int t = 0; t < I.ntiles; t++) acc += part[I.part_off + t];
+  out[i] = acc;
+}
+
+}  // namespace
+}  // namespace ket
+
+using namespace ket;
+
+extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne, const int64_t* eoff,
+                              const int* edges, int p, const double* gamma, const double* beta, int use_graph,
+                              double* out) {
+  if (!c || (ninst > 0 && (!n || !ne || !eoff || !edges || !gamma || !beta || !out)))
+    return fail(KET_ERR_TYPE, "null argument");
+  if (ninst < 0 || p < 0 || p > KQ_MAX_P) return fail(KET_ERR_TYPE, "bad instance count or layer count");
+  if (ninst == 0) return KET_OK;
+  cudaSetDevice(c->device);
+  const int T = 12, NT = 256;
+  std::vector<QInst> inst(ninst);
+  std::vector<uint64_t> masks;
+  int64_t work = 0, parts = 0, nedges = 0;
+  for (int i = 0; i < ninst; i++) {
+    if (n[i] < 1 || n[i] > 30) return fail(KET_ERR_RANGE, "instance qubit count out of range (1..30)");
+    if (ne[i] < 0 || ne[i] > KQ_MAX_EDGES) return fail(KET_ERR_TYPE, "instance edge count out of range (0..64)");
+    if (n[i] > T && n[i] - T > T) return fail(KET_ERR_UNSUPPORTED, "instances wider than 24 qubits");
+    QInst& I = inst[i];
+    I.n = n[i];
+    I.ne = ne[i];
+    I.p = p;
+    I.edge_off = (int64_t)masks.size();
+    for (int e = 0; e < ne[i]; e++) {
+      int u = edges[2 * (eoff[i] + e)], v = edges[2 * (eoff[i] + e) + 1];
+      if (u < 0 || v < 0 || u >= n[i] || v >= n[i]) return fail(KET_ERR_RANGE, "edge endpoint out of range");
+      if (u == v) return fail(KET_ERR_TYPE, "self-loop edge");
+      masks.push_back((uint64_t(1) << u) | (uint64_t(1) << v));
+    }
+    nedges += ne[i];
+    const bool split = I.n > T && p > 0;
+    I.ntiles = split ? (1 << (I.n - T)) : 1;
+    I.state = split ? work : 0;
+    if (split) work += int64_t(1) << I.n;
+    I.part_off = parts;
+    parts += I.ntiles;
+  }
+  // Work order: wide instances pass by pass (largest first, interleaved so a
+  // tile rarely waits), then the shared-memory instances (largest first).
+  std::vector<int> order(ninst);
+  for (int i = 0; i < ninst; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return inst[x].n > inst[y].n; });
+  std::vector<QItem> items;
+  for (int k = 0; k < 2 * p; k++)
+    for (int i : order) {
+      const QInst& I = inst[i];
+      if (!(I.n > T && p > 0)) continue;
+      for (int t = 0; t < I.ntiles; t++) items.push_back(QItem{i, k, t});
+    }
+  for (int i : order)
+    if (!(inst[i].n > T && p > 0)) items.push_back(QItem{i, -1, 0});
+  // device buffers in the second scratch pool
+  auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+  size_t off_inst = 0, off_items = al(sizeof(QInst) * ninst), off_mask = off_items + al(sizeof(QItem) * items.size());
+  size_t off_g = off_mask + al(8 * std::max<size_t>(masks.size(), 1));
+  size_t off_b = off_g + al(8 * (size_t)ninst * p + 8);
+  size_t off_part = off_b + al(8 * (size_t)ninst * p + 8);
+  size_t off_out = off_part + al(8 * (size_t)parts);
+  size_t off_cnt = off_out + al(8 * (size_t)ninst);
+  size_t off_work = off_cnt + al(4 * ((size_t)ninst + 2));
+  size_t total = off_work + 16 * (size_t)work + 256;
+  if (c->scratch2_bytes < total) {
+    int rc = ctx_wait(c);
+    if (rc) return rc;
+    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+    if (c->scratch2) cudaFree(c->scratch2);
+    c->scratch2 = nullptr;
+    c->scratch2_bytes = 0;
+    rc = dev_alloc(&c->scratch2, total);
+    if (rc) return rc;
+    c->scratch2_bytes = total;
+  }
+  char* base = (char*)c->scratch2;
+  std::vector<double> gv(gamma, gamma + (size_t)ninst * p), bv(beta, beta + (size_t)ninst * p);
+  cudaMemcpyAsync(base + off_inst, inst.data(), sizeof(QInst) * ninst, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(base + off_items, items.data(), sizeof(QItem) * items.size(), cudaMemcpyHostToDevice, c->stream);
+  if (!masks.empty()) cudaMemcpyAsync(base + off_mask, masks.data(), 8 * masks.size(), cudaMemcpyHostToDevice, c->stream);
+  if (p > 0) {
+    cudaMemcpyAsync(base + off_g, gv.data(), 8 * gv.size(), cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(base + off_b, bv.data(), 8 * bv.size(), cudaMemcpyHostToDevice, c->stream);
+  }
+  c->h2d_bytes += sizeof(QInst) * ninst + sizeof(QItem) * items.size() + 8 * masks.size() + 16 * gv.size();
+  QArgs a;
+  a.inst = (const QInst*)(base + off_inst);
+  a.items = (const QItem*)(base + off_items);
+  a.emask = (const uint64_t*)(base + off_mask);
+  a.gamma = (const double*)(base + off_g);
+  a.beta = (const double*)(base + off_b);
+  a.part = (double*)(base + off_part);
+  a.next = (unsigned int*)(base + off_cnt);
+  a.done = a.next + 2;
+  a.status = c->d_status;
+  a.work = (double2*)(base + off_work);
+  a.nitems = (int)items.size();
+  a.tile = T;
+  const size_t smem = (16u << T) + 16 * (KQ_MAX_EDGES + 1) + 8 * KQ_MAX_EDGES + 8 * 32;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_batch_qaoa<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_qaoa<NT>, NT, smem);
+  per_sm = std::max(1, per_sm);
+  const int grid = num_sms() * per_sm;  // persistent: every CTA resident at once
+  double* dout = (double*)(base + off_out);
+  auto record = [&]() -> cudaError_t {
+    cudaMemsetAsync(a.next, 0, 4 * ((size_t)ninst + 2), c->stream);
+    k_batch_qaoa<NT><<<grid, NT, smem, c->stream>>>(a);
+    k_qaoa_reduce<<<(ninst + 127) / 128, 128, 0, c->stream>>>(a.inst, ninst, a.part, dout);
+    return cudaGetLastError();
+  };
+  cudaError_t e;
+  prof_begin(c);
+  if (use_graph) {
+    cudaGraph_t graph;
+    e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+    e = record();
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+    if (e != cudaSuccess) return cuda_fail(e, "batch capture");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+    e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    e = cudaGraphLaunch(c->graph_exec, c->stream);
+  } else {
+    e = record();
+  }
+  prof_end(c, PK_BATCH);
+  c->launches += 2;
+  if (e != cudaSuccess) return cuda_fail(e, "batch launch");
+  e = cudaMemcpyAsync(out, dout, 8 * (size_t)ninst, cudaMemcpyDeviceToHost, c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(out)");
+  c->d2h_bytes += 8 * (size_t)ninst;
+  int rc = ctx_wait(c);
+  if (rc) return rc;
+  return check_status(c);
+}

@@ -8,7 +8,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/ket_sv.h"
+#include "ket_sv.h"
 #include "engine.h"
 
 struct ket_ctx {

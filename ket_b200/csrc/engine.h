@@ -5,7 +5,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/ket_sv.h"
+#include "ket_sv.h"
 
 namespace ket {
 
@@ -21,7 +21,13 @@ enum GType : int32_t {
   G_SWAP = 3,   // swap t0, t1, controls cmask
   G_MAT2 = 4,   // 4x4 on (t0 = MSB, t1), controls cmask
   G_MATK = 5,   // dense 2^k x 2^k on tk (tk[0] = MSB)
-  G_DIAG2 = 6   // diag(m0..m3) on (t0 = MSB, t1), controls cmask
+  G_DIAG2 = 6,  // diag(m0..m3) on (t0 = MSB, t1), controls cmask
+  // Adjoint-sweep probes (read-only): on a state whose top qubit `anc` splits
+  // it into psi (anc = 0) and lambda (anc = 1), accumulate Re<lambda|D|psi>
+  // into gradient slot `slot`.
+  G_GRADM = 7,  // D 2x2 on t0, controls cmask
+  G_GRADD = 8,  // D = diag(m0, m1) on t0, controls cmask
+  G_GRADM2 = 9  // D 4x4 on (t0 = MSB, t1), controls cmask
 };
 
 struct Gate {
@@ -33,6 +39,7 @@ struct Gate {
   std::vector<int> tk;        // MATK targets
   std::vector<cd> mk;         // MATK matrix
   int src_op = -1;            // index of the ket_op it came from
+  int slot = -1;              // G_GRAD*: gradient slot
 };
 
 // Tile pass: the tile holds qubits {0..L-1} U hbits; gates are applied in order.
@@ -47,7 +54,10 @@ struct Pass {
 struct Plan {
   std::vector<Gate> gates;
   std::vector<Pass> passes;
+  int anc = -1;               // adjoint sweep: qubit that selects psi / lambda, kept in every tile
 };
+
+inline bool is_grad(const Gate& g) { return g.type == G_GRADM || g.type == G_GRADD || g.type == G_GRADM2; }
 
 // Lower and validate an op list (mirrors #checkOp, circuit.ts:1113-1146).
 int lower_ops(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, bool prune,

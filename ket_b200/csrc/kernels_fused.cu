@@ -290,11 +290,53 @@ __device__ __forceinline__ void issue_tile(const Pass2Args& a, const typename Ve
   }
 }
 
-template <typename R, int NT>
-__global__ void __launch_bounds__(NT, 2) k_fused2(Pass2Args a) {
+// Adjoint probes.  Register bit 3 selects psi (0) / lambda (1).
+// Re<lambda| D |psi> with D 2x2 on register bit A.
+template <typename R, int A>
+__device__ __forceinline__ double grad_m(const cpx<R>* x, const R* d, uint32_t smask) {
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    if ((j >> A) & 1) continue;
+    if (!((smask >> j) & 1)) continue;
+    const int j1 = j | (1 << A);
+    cpx<R> u0 = mac2<R>(d[0], d[1], x[j], d[2], d[3], x[j1]);
+    cpx<R> u1 = mac2<R>(d[4], d[5], x[j], d[6], d[7], x[j1]);
+    acc += (double)x[j + 8].re * u0.re + (double)x[j + 8].im * u0.im + (double)x[j1 + 8].re * u1.re +
+           (double)x[j1 + 8].im * u1.im;
+  }
+  return acc;
+}
+// Re<lambda| diag(d0, d1) on register bit A |psi>; A = -1: one factor (d0) for all.
+template <typename R, int A>
+__device__ __forceinline__ double grad_d(const cpx<R>* x, R d0r, R d0i, R d1r, R d1i, uint32_t smask) {
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    if (!((smask >> j) & 1)) continue;
+    const bool one = A >= 0 && ((j >> (A < 0 ? 0 : A)) & 1);
+    cpx<R> u = cmul<R>(one ? d1r : d0r, one ? d1i : d0i, x[j]);
+    acc += (double)x[j + 8].re * u.re + (double)x[j + 8].im * u.im;
+  }
+  return acc;
+}
+
+// Warp-sum v and add it to the CTA's gradient accumulator for (slot, warp).
+__device__ __forceinline__ void grad_accum(double* sgrad, int slot, int warp, int lane, double v) {
+  v = warp_sum(v);
+  if (lane == 0) sgrad[slot * 8 + warp] += v;
+}
+
+template <typename R, int NT, bool GRAD>
+__global__ void __launch_bounds__(NT, GRAD ? 1 : 2) k_fused2(Pass2Args a) {
   typedef typename Vec2<R>::T V;
   extern __shared__ __align__(128) unsigned char smraw[];
   cpx<R>* sm = reinterpret_cast<cpx<R>*>(smraw);  // exchange buffer (swizzled)
+  double* sgrad = reinterpret_cast<double*>(smraw + (sizeof(cpx<R>) << KET_T2_BITS));  // [slot][warp]
+  if (GRAD) {
+    for (int i = threadIdx.x; i < a.nslots * 8; i += NT) sgrad[i] = 0.0;
+    __syncthreads();
+  }
   V* amp = reinterpret_cast<V*>(a.amp);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
@@ -505,6 +547,71 @@ __global__ void __launch_bounds__(NT, 2) k_fused2(Pass2Args a) {
           }
           break;
         }
+        case FO_GRADM: case FO_GRADD: {
+          if (!GRAD) break;
+          // <lambda|D|psi> over this thread's amplitudes: register bit 3 of the
+          // slot index selects psi (0) or lambda (1) -- the planner pins the
+          // ancilla there
+          const int slot = (int16_t)(h1.w >> 16);
+          double acc = 0.0;
+          if (type == FO_GRADM) {
+            R d[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) d[q] = (R)__ldg(M + q);
+            switch (oa) {
+              case 0: acc = grad_m<R, 0>(x, d, smask); break;
+              case 1: acc = grad_m<R, 1>(x, d, smask); break;
+              default: acc = grad_m<R, 2>(x, d, smask); break;
+            }
+          } else {
+            const R d0r = (R)__ldg(M + 0), d0i = (R)__ldg(M + 1), d1r = (R)__ldg(M + 2), d1i = (R)__ldg(M + 3);
+            if (fl & (FOF_TGT_THR | FOF_TGT_CTX)) {
+              const bool one = (fl & FOF_TGT_CTX)
+                                   ? (ctxbase & __ldg(reinterpret_cast<const unsigned long long*>(op) + 5)) != 0
+                                   : (bool)((tid >> oa) & 1);
+              acc = grad_d<R, -1>(x, one ? d1r : d0r, one ? d1i : d0i, one ? d1r : d0r, one ? d1i : d0i, smask);
+            } else {
+              switch (oa) {
+                case 0: acc = grad_d<R, 0>(x, d0r, d0i, d1r, d1i, smask); break;
+                case 1: acc = grad_d<R, 1>(x, d0r, d0i, d1r, d1i, smask); break;
+                default: acc = grad_d<R, 2>(x, d0r, d0i, d1r, d1i, smask); break;
+              }
+            }
+          }
+          grad_accum(sgrad, slot, warp, lane, acc);
+          break;
+        }
+        case FO_GRADM2: {
+          if (!GRAD) break;
+          __syncthreads();
+#pragma unroll
+          for (int j = 0; j < 16; j++) sm[SwzT<R>::f(L.tbase | rofs(L, j))] = x[j];
+          __syncthreads();
+          const int slot = (int16_t)(h1.w >> 16), anc = (int16_t)(h1.w & 0xffff);
+          const uint32_t ct = h1.z;
+          const int ta = oa, tb = ob;
+          int b3[3] = {ta, tb, anc};
+          for (int u = 1; u < 3; u++)
+            for (int v = u; v > 0 && b3[v - 1] > b3[v]; v--) { int t = b3[v]; b3[v] = b3[v - 1]; b3[v - 1] = t; }
+          double acc = 0.0;
+          for (uint32_t g = tid; g < (1u << (KET_T2_BITS - 3)); g += NT) {
+            uint32_t b0 = insert0_32(insert0_32(insert0_32(g, b3[0]), b3[1]), b3[2]);
+            if ((b0 & ct) != ct) continue;
+            const uint32_t idx[4] = {b0, b0 | (1u << tb), b0 | (1u << ta), b0 | (1u << ta) | (1u << tb)};
+            cpx<R> v[4];
+            for (int c = 0; c < 4; c++) v[c] = sm[SwzT<R>::f(idx[c])];
+            for (int r = 0; r < 4; r++) {
+              cpx<R> s0 = mac2<R>((R)__ldg(M + 8 * r), (R)__ldg(M + 8 * r + 1), v[0], (R)__ldg(M + 8 * r + 2),
+                                  (R)__ldg(M + 8 * r + 3), v[1]);
+              cpx<R> s1 = mac2<R>((R)__ldg(M + 8 * r + 4), (R)__ldg(M + 8 * r + 5), v[2], (R)__ldg(M + 8 * r + 6),
+                                  (R)__ldg(M + 8 * r + 7), v[3]);
+              cpx<R> lam = sm[SwzT<R>::f(idx[r] | (1u << anc))];
+              acc += (double)lam.re * (s0.re + s1.re) + (double)lam.im * (s0.im + s1.im);
+            }
+          }
+          grad_accum(sgrad, slot, warp, lane, acc);
+          continue;
+        }
         default: break;
       }
       if (pr) prune16<R>(x, thr, qthr);  // mixing ops only (the planner clears the flag elsewhere)
@@ -516,9 +623,23 @@ __global__ void __launch_bounds__(NT, 2) k_fused2(Pass2Args a) {
       for (int j = 0; j < 16; j++) st_amp<R>(amp + (ctxbase | gl.gthr | grofs(gl, j)), x[j]);
     }
   }
+  if (GRAD) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.nslots * 8; i += NT) a.gpart[(size_t)blockIdx.x * a.nslots * 8 + i] = sgrad[i];
+  }
 }
 
-template <typename R>
+// out[s] = sum over CTAs c and warps w of gpart[c][s][w], in a fixed order.
+__global__ void k_grad_reduce(const double* gpart, int nctas, int nslots, double* out) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots) return;
+  double acc = 0.0;
+  for (int c = 0; c < nctas; c++)
+    for (int w = 0; w < 8; w++) acc += gpart[((size_t)c * nslots + s) * 8 + w];
+  out[s] = acc;
+}
+
+template <typename R, bool GRAD>
 cudaError_t launch_t(const Pass2Args& a, cudaStream_t s) {
   const int NT = 256;
   static bool init = false;
@@ -531,20 +652,28 @@ cudaError_t launch_t(const Pass2Args& a, cudaStream_t s) {
       sm[c] = v;
     }
     cudaMemcpyToSymbol(c_slotmask, sm, sizeof(sm));
-    cudaFuncSetAttribute(k_fused2<R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaFuncSetAttribute(k_fused2<R, NT, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
     init = true;
   }
-  size_t smem = sizeof(cpx<R>) << KET_T2_BITS;
+  size_t smem = (sizeof(cpx<R>) << KET_T2_BITS) + (GRAD ? sizeof(double) * 8 * (size_t)a.nslots : 0);
   uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
-  unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)num_sms() * 2);
-  k_fused2<R, NT><<<blocks, NT, smem, s>>>(a);
+  unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)fused2_grid());
+  k_fused2<R, NT, GRAD><<<blocks, NT, smem, s>>>(a);
   return cudaGetLastError();
 }
 
 }  // namespace
 
+int fused2_grid() { return num_sms() * 2; }
+
 cudaError_t launch_fused2(const Pass2Args& a, int precision, cudaStream_t s) {
-  return precision == KET_C64 ? launch_t<float>(a, s) : launch_t<double>(a, s);
+  if (a.nslots > 0) return precision == KET_C64 ? launch_t<float, true>(a, s) : launch_t<double, true>(a, s);
+  return precision == KET_C64 ? launch_t<float, false>(a, s) : launch_t<double, false>(a, s);
+}
+
+cudaError_t launch_grad_reduce(const double* gpart, int nctas, int nslots, double* out, cudaStream_t s) {
+  k_grad_reduce<<<(nslots + 127) / 128, 128, 0, s>>>(gpart, nctas, nslots, out);
+  return cudaGetLastError();
 }
 
 }  // namespace ket

@@ -52,6 +52,9 @@ enum FOpType : uint8_t {
   FO_DIAGR = 8,   // diag(m0, m1) on register bit a
   FO_DIAGT = 9,   // diag(m0, m1) on thread-id bit a (lane 0-4 / warp 5-7): one phase per thread
   FO_DIAGX = 10,  // diag(m0, m1) on a qubit outside the tile (mask dg0): one phase per tile
+  FO_GRADM = 12,  // adjoint probe, D 2x2 on register bit a, ancilla register bit b, slot d1
+  FO_GRADD = 13,  // adjoint probe, D = diag(m0, m1) on target a (register / thread / outside, see flags)
+  FO_GRADM2 = 14  // adjoint probe, D 4x4 on tile bits a (MSB), b through shared memory; ancilla tile bit d0
 };
 
 // flags
@@ -59,7 +62,8 @@ enum FOpType : uint8_t {
 #define FOF_REAL 2u     // MAT1: every matrix entry is real
 #define FOF_D0ONE 4u    // DIAG*: m0 == 1 exactly (only bit-1 amplitudes change)
 #define FOF_RXFORM 8u   // MAT1: m00, m11 real and m01, m10 imaginary (Rx-like)
-#define FOF_LAZY 16u    // DIAGT/DIAGX without register controls: folded into a per-thread phase
+#define FOF_TGT_THR 32u // FO_GRADD: target is a thread-id bit (a)
+#define FOF_TGT_CTX 64u // FO_GRADD: target is outside the tile (mask dg0)
 
 struct FOp {
   uint8_t type, a, b, flags;
@@ -85,7 +89,13 @@ struct Pass2Args {
   int ctxbits[KET_MAX_CTX_BITS];
   double thr, qthr;
   int* status;                     // device status word: set to KET_ERR_TIMEOUT if a bounded wait ran out
+  double* gpart;                   // adjoint: per-CTA gradient partials [cta][slot][warp]
+  int nslots;                      // adjoint: gradient probes in this pass
 };
+
+// Sum the adjoint partials of one pass: out[s] = sum over CTAs and warps (fixed order).
+cudaError_t launch_grad_reduce(const double* gpart, int nctas, int nslots, double* out, cudaStream_t s);
+int fused2_grid();
 
 // Lower one fused pass to a register-tiled program (segments + exchanges).
 void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, std::vector<FOp>& prog,

@@ -35,9 +35,12 @@ int range_err(std::string& err, int q, int n) {
 
 uint64_t bit(int q) { return uint64_t(1) << q; }
 
+thread_local int g_anc = -1;  // ancilla of the plan being built (adjoint sweep)
+
 // Qubits a gate touches (targets and controls).
 uint64_t gate_qubits(const Gate& g) {
   uint64_t m = g.cmask;
+  if (is_grad(g) && g_anc >= 0) m |= bit(g_anc);
   if (g.t0 >= 0) m |= bit(g.t0);
   if (g.t1 >= 0) m |= bit(g.t1);
   for (int q : g.tk) m |= bit(q);
@@ -46,6 +49,12 @@ uint64_t gate_qubits(const Gate& g) {
 
 // Qubits whose amplitudes a gate mixes (must lie in the tile).
 uint64_t gate_mix(const Gate& g) {
+  if (is_grad(g)) {
+    uint64_t m = bit(g_anc);
+    if (g.type != G_GRADD) m |= bit(g.t0);
+    if (g.type == G_GRADM2) m |= bit(g.t1);
+    return m;
+  }
   switch (g.type) {
     case G_DIAG1: case G_DIAG2: return 0;
     case G_MAT1: case G_X1: return bit(g.t0);
@@ -216,6 +225,7 @@ int tile_qubits(int precision, int fusion) {
 
 void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& plan) {
   plan.passes.clear();
+  g_anc = plan.anc;
   const std::vector<Gate>& G = plan.gates;
   const int M = std::min(n, tile_qubits(precision, fusion));
   // L low qubits are contiguous in every tile: 2^L amplitudes per HBM chunk
@@ -268,6 +278,7 @@ void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& pl
     // Grow the tile's qubit set one step at a time, each time adding the
     // missing targets of whichever frontier gate lets the pass absorb most.
     uint64_t S = (M >= n) ? (n >= 64 ? ~uint64_t(0) : bit(n) - 1) : low;
+    if (plan.anc >= 0) S |= bit(plan.anc);
     while (__builtin_popcountll(S) < M) {
       std::vector<uint64_t> cand;
       absorbed(S, &cand);

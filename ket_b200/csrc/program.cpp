@@ -48,8 +48,13 @@ int tpos(const Pass& p, int q) {
 
 bool needs_two_regs(const Gate&) { return false; }
 
+thread_local int g_anc_tb = -1;  // tile bit of the adjoint ancilla in the pass being lowered
+
 bool fits(const Gate& g, const Pass& p, const Lay& l) {
   switch (g.type) {
+    case G_GRADM: return is_reg(l, tpos(p, g.t0)) && is_reg(l, g_anc_tb);
+    case G_GRADD: return is_reg(l, g_anc_tb);
+    case G_GRADM2: return true;
     case G_DIAG1: case G_DIAG2: case G_SWAP: case G_MAT2: return true;  // SWAP/MAT2 work in any layout
     case G_MAT1: case G_X1: {
       int t = tpos(p, g.t0);
@@ -66,18 +71,19 @@ Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision)
   for (int b = 0; b < NB; b++) { next[b] = INF; nreg[b] = 0; }
   for (size_t i = from; i < p.gates.size(); i++) {
     const Gate& g = plan.gates[p.gates[i]];
-    if (g.type == G_DIAG1 || g.type == G_DIAG2) continue;
+    if (g.type == G_DIAG1 || g.type == G_DIAG2 || g.type == G_GRADD || g.type == G_GRADM2) continue;
     int ts[2] = {tpos(p, g.t0), g.type == G_SWAP || g.type == G_MAT2 ? tpos(p, g.t1) : -1};
     for (int t : ts) {
       if (t < 0) continue;
       if (next[t] == INF) { next[t] = (int)i; nreg[t] = needs_two_regs(g) ? 1 : 0; }
     }
   }
-  // the current gate's two-qubit targets must be registers
+  // the adjoint ancilla always sits in registers; a 2x2 probe's target too
   std::vector<int> must;
+  if (g_anc_tb >= 0) must.push_back(g_anc_tb);
   if (from < p.gates.size()) {
     const Gate& g = plan.gates[p.gates[from]];
-    if (needs_two_regs(g)) { must.push_back(tpos(p, g.t0)); must.push_back(tpos(p, g.t1)); }
+    if (g.type == G_GRADM) must.push_back(tpos(p, g.t0));
   }
   std::vector<int> order(NB);
   for (int b = 0; b < NB; b++) order[b] = b;
@@ -113,6 +119,11 @@ Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision)
     for (int b : ln) out.push_back(b);
     lanes = out;
   }
+  // the adjoint ancilla always occupies register bit 3 (the kernel's probes
+  // address it at compile time)
+  if (g_anc_tb >= 0)
+    for (int i = 0; i < 3; i++)
+      if (regs[i] == g_anc_tb) std::swap(regs[i], regs[3]);
   for (int i = 0; i < 5; i++) l.pos[i] = lanes[i];
   for (int i = 0; i < 3; i++) l.pos[5 + i] = warps[i];
   for (int i = 0; i < 4; i++) l.pos[8 + i] = regs[i];
@@ -191,7 +202,36 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
         o.type = FO_DIAGT;
         o.a = (uint8_t)l.role[t0];  // lanes 0..4 -> tid bits 0..4, warps 5..7 -> tid bits 5..7
       }
-      if (o.type != FO_DIAGR && o.creg == 0) o.flags |= FOF_LAZY;
+      break;
+    }
+    case G_GRADM: {
+      o.type = FO_GRADM;
+      o.flags = 0;
+      o.a = (uint8_t)(l.role[t0] - 8);
+      o.b = (uint8_t)(l.role[g_anc_tb] - 8);
+      o.d1 = (int16_t)g.slot;
+      for (int k = 0; k < 4; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
+      break;
+    }
+    case G_GRADD: {
+      o.type = FO_GRADD;
+      o.flags = 0;
+      o.b = (uint8_t)(l.role[g_anc_tb] - 8);
+      o.d1 = (int16_t)g.slot;
+      if (t0 < 0) { o.flags |= FOF_TGT_CTX; o.dg0 = uint64_t(1) << g.t0; }
+      else if (is_reg(l, t0)) o.a = (uint8_t)(l.role[t0] - 8);
+      else { o.flags |= FOF_TGT_THR; o.a = (uint8_t)l.role[t0]; }
+      for (int k = 0; k < 2; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
+      break;
+    }
+    case G_GRADM2: {
+      o.type = FO_GRADM2;
+      o.flags = 0;
+      o.a = (uint8_t)t0;
+      o.b = (uint8_t)t1;
+      o.d0 = (int16_t)g_anc_tb;
+      o.d1 = (int16_t)g.slot;
+      for (int k = 0; k < 16; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
       break;
     }
     case G_DIAG2: {
@@ -216,20 +256,11 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
 void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, std::vector<FOp>& prog,
                   uint8_t load_pos[KET_T2_BITS], uint8_t store_pos[KET_T2_BITS]) {
   prog.clear();
+  g_anc_tb = plan.anc >= 0 ? tpos(p, plan.anc) : -1;
   Lay cur = choose(plan, p, 0, true, precision);
   for (int i = 0; i < NB; i++) load_pos[i] = (uint8_t)cur.pos[i];
   for (size_t i = 0; i < p.gates.size(); i++) {
     const Gate& g = plan.gates[p.gates[i]];
-    if (g.type == G_SWAP && g.cmask == 0) {
-      // An uncontrolled SWAP moves no data: the two tile bits trade roles.
-      int t0 = tpos(p, g.t0), t1 = tpos(p, g.t1);
-      std::swap(cur.pos[cur.role[t0]], cur.pos[cur.role[t1]]);
-      fill_roles(cur);
-      FOp o = make_exch(cur);
-      o.type = FO_RELABEL;
-      prog.push_back(o);
-      continue;
-    }
     if (!fits(g, p, cur)) {
       cur = choose(plan, p, i, false, precision);
       prog.push_back(make_exch(cur));

@@ -4,7 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/ket_sv.h"
+#include "ket_sv.h"
 
 namespace ket {
 

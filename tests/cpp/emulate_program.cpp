@@ -1,0 +1,210 @@
+// emulate_program.cpp -- TEST INFRASTRUCTURE: executes the fused-pass programs
+// that the engine's planner emits (ket_b200/csrc/planner.cpp, program.cpp) on
+// host arrays, following the semantics of the k_fused2 kernel op by op
+// (layouts, exchanges, relabels, register / lane / diagonal / shared-memory
+// ops, controls).  The tests compare it with direct gate-by-gate application,
+// so planner and program-generator bugs show up without a GPU.
+#include <complex>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "launch.h"
+
+namespace ket {
+int num_sms() { return 148; }
+}
+
+using namespace ket;
+typedef std::complex<double> cx;
+
+namespace {
+
+struct Lay {
+  uint32_t tbase[256];
+  uint32_t rp[4];
+};
+
+Lay make_lay(const uint8_t* pos) {
+  Lay L;
+  for (int t = 0; t < 256; t++) {
+    int lane = t & 31, warp = t >> 5;
+    uint32_t v = 0;
+    for (int l = 0; l < 5; l++) v |= (uint32_t)((lane >> l) & 1) << pos[l];
+    for (int w = 0; w < 3; w++) v |= (uint32_t)((warp >> w) & 1) << pos[5 + w];
+    L.tbase[t] = v;
+  }
+  for (int k = 0; k < 4; k++) L.rp[k] = 1u << pos[8 + k];
+  return L;
+}
+
+uint32_t rofs(const Lay& L, int j) {
+  uint32_t o = 0;
+  for (int k = 0; k < 4; k++)
+    if ((j >> k) & 1) o |= L.rp[k];
+  return o;
+}
+
+void prune(cx& a) {
+  double n2 = a.real() * a.real() + a.imag() * a.imag();
+  if (n2 < 1e-14) a = 0.0;
+}
+
+uint16_t slotmask(uint32_t creg) {
+  uint16_t v = 0;
+  for (int j = 0; j < 16; j++)
+    if (((uint32_t)j & creg) == creg) v |= (uint16_t)(1u << j);
+  return v;
+}
+
+void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
+  std::vector<FOp> prog;
+  uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
+  plan_program(plan, p, KET_C128, prunef, prog, lp, sp);
+  const int L = p.L;
+  auto gq = [&](int tb) { return tb < L ? tb : p.hbits[tb - L]; };
+  uint64_t S = (uint64_t(1) << L) - 1;
+  for (int q : p.hbits) S |= uint64_t(1) << q;
+  std::vector<int> ctxbits;
+  for (int q = 0; q < n; q++)
+    if (!((S >> q) & 1)) ctxbits.push_back(q);
+  const uint64_t ntiles = uint64_t(1) << (n - KET_T2_BITS);
+  std::vector<cx> x(256 * 16), sm(4096);
+  auto gaddr = [&](uint64_t ctx, uint32_t tidx) {
+    uint64_t g = ctx;
+    for (int b = 0; b < KET_T2_BITS; b++)
+      if ((tidx >> b) & 1) g |= uint64_t(1) << gq(b);
+    return g;
+  };
+  for (uint64_t tile = 0; tile < ntiles; tile++) {
+    uint64_t ctx = 0;
+    for (size_t j = 0; j < ctxbits.size(); j++)
+      if ((tile >> j) & 1) ctx |= uint64_t(1) << ctxbits[j];
+    Lay Lc = make_lay(lp);
+    for (int t = 0; t < 256; t++)
+      for (int j = 0; j < 16; j++) x[t * 16 + j] = amp[gaddr(ctx, Lc.tbase[t] | rofs(Lc, j))];
+    for (const FOp& op : prog) {
+      if (op.type == FO_EXCH || op.type == FO_RELABEL) {
+        if (op.type == FO_EXCH)
+          for (int t = 0; t < 256; t++)
+            for (int j = 0; j < 16; j++) sm[Lc.tbase[t] | rofs(Lc, j)] = x[t * 16 + j];
+        Lc = make_lay(op.pos);
+        if (op.type == FO_EXCH)
+          for (int t = 0; t < 256; t++)
+            for (int j = 0; j < 16; j++) x[t * 16 + j] = sm[Lc.tbase[t] | rofs(Lc, j)];
+        continue;
+      }
+      if ((ctx & op.cctx) != op.cctx) continue;
+      const bool pr = op.flags & FOF_PRUNE;
+      const cx m0(op.m[0], op.m[1]), m1(op.m[2], op.m[3]), m2(op.m[4], op.m[5]), m3(op.m[6], op.m[7]);
+      std::vector<cx> nx = x;
+      for (int t = 0; t < 256; t++) {
+        const uint32_t sm_ = ((uint32_t)(t & op.cthr) == op.cthr) ? slotmask(op.creg & 15) : 0;
+        cx* xt = &x[t * 16];
+        cx* nt = &nx[t * 16];
+        const int lane = t & 31;
+        switch (op.type) {
+          case FO_MAT1R: case FO_X1R:
+            for (int j = 0; j < 16; j++) {
+              if ((j >> op.a) & 1) continue;
+              int j1 = j | (1 << op.a);
+              if (!((sm_ >> j) & 1)) continue;
+              if (op.type == FO_X1R) { nt[j] = xt[j1]; nt[j1] = xt[j]; continue; }
+              nt[j] = m0 * xt[j] + m1 * xt[j1];
+              nt[j1] = m2 * xt[j] + m3 * xt[j1];
+            }
+            break;
+          case FO_MAT1L: case FO_X1L: {
+            int bitv = (lane >> op.a) & 1;
+            const cx* pt = &x[(t ^ (1 << op.a)) * 16];
+            for (int j = 0; j < 16; j++) {
+              if (!((sm_ >> j) & 1)) continue;
+              if (op.type == FO_X1L) { nt[j] = pt[j]; continue; }
+              nt[j] = bitv ? (m2 * pt[j] + m3 * xt[j]) : (m0 * xt[j] + m1 * pt[j]);
+            }
+            break;
+          }
+          case FO_DIAGR:
+            for (int j = 0; j < 16; j++)
+              if ((sm_ >> j) & 1) nt[j] = ((j >> op.a) & 1 ? m1 : m0) * xt[j];
+            break;
+          case FO_DIAGT: case FO_DIAGX: {
+            bool one = op.type == FO_DIAGT ? ((t >> op.a) & 1) : ((ctx & op.dg0) != 0);
+            for (int j = 0; j < 16; j++)
+              if ((sm_ >> j) & 1) nt[j] = (one ? m1 : m0) * xt[j];
+            break;
+          }
+          case FO_DIAG: {
+            for (int j = 0; j < 16; j++) {
+              uint32_t idx = Lc.tbase[t] | rofs(Lc, j);
+              if ((idx & op.ctile) != op.ctile) continue;
+              int k0 = op.d0 >= 0 ? (int)((idx >> op.d0) & 1) : (int)((ctx & op.dg0) != 0);
+              int k1 = op.d1 >= 0 ? (int)((idx >> op.d1) & 1) : (int)((ctx & op.dg1) != 0);
+              int kk = op.d1 != -2 ? 2 * k0 + k1 : k0;
+              nt[j] = cx(op.m[2 * kk], op.m[2 * kk + 1]) * xt[j];
+            }
+            break;
+          }
+          default: break;
+        }
+      }
+      if (op.type == FO_SWAPS || op.type == FO_MAT2S) {
+        for (int t = 0; t < 256; t++)
+          for (int j = 0; j < 16; j++) sm[Lc.tbase[t] | rofs(Lc, j)] = x[t * 16 + j];
+        const int ta = op.a, tb = op.b, lo = ta < tb ? ta : tb, hi = ta < tb ? tb : ta;
+        for (uint32_t g = 0; g < 1024; g++) {
+          uint32_t lo_m = (1u << lo) - 1;
+          uint32_t b0 = ((g & ~lo_m) << 1) | (g & lo_m);
+          uint32_t hi_m = (1u << hi) - 1;
+          b0 = ((b0 & ~hi_m) << 1) | (b0 & hi_m);
+          if ((b0 & op.ctile) != op.ctile) continue;
+          uint32_t idx[4] = {b0, b0 | (1u << tb), b0 | (1u << ta), b0 | (1u << ta) | (1u << tb)};
+          if (op.type == FO_SWAPS) { std::swap(sm[idx[1]], sm[idx[2]]); continue; }
+          cx v[4] = {sm[idx[0]], sm[idx[1]], sm[idx[2]], sm[idx[3]]};
+          for (int r = 0; r < 4; r++) {
+            cx y = 0;
+            for (int c = 0; c < 4; c++) y += cx(op.m[8 * r + 2 * c], op.m[8 * r + 2 * c + 1]) * v[c];
+            if (pr) prune(y);
+            sm[idx[r]] = y;
+          }
+        }
+        for (int t = 0; t < 256; t++)
+          for (int j = 0; j < 16; j++) nx[t * 16 + j] = sm[Lc.tbase[t] | rofs(Lc, j)];
+        x = nx;
+        continue;
+      }
+      if (pr)
+        for (auto& v : nx) prune(v);
+      x = nx;
+    }
+    Lay Ls = make_lay(sp);
+    for (int t = 0; t < 256; t++)
+      for (int j = 0; j < 16; j++) amp[gaddr(ctx, Ls.tbase[t] | rofs(Ls, j))] = x[t * 16 + j];
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Apply ops to the n-qubit state re_im (interleaved) through the planner's
+// fused programs, emulated.  Returns 0, or the lowering status; passes[0] =
+// emulated register-tiled passes, passes[1] = other passes (not emulated: -1).
+int emu_apply(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int prune, int fusion,
+              double* re_im, int64_t* passes) {
+  Plan plan;
+  std::string err;
+  int rc = lower_ops(n, ops, nops, mats, nmat, prune != 0, plan.gates, err);
+  if (rc) return rc;
+  plan_passes(n, KET_C128, fusion, prune != 0, plan);
+  cx* amp = reinterpret_cast<cx*>(re_im);
+  passes[0] = passes[1] = 0;
+  for (const Pass& p : plan.passes) {
+    if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) { passes[1]++; return -1; }
+    run_pass(plan, p, n, prune != 0, amp);
+    passes[0]++;
+  }
+  return 0;
+}
+}

@@ -1,0 +1,44 @@
+"""Builds and loads the fused-program emulator (tests/cpp/emulate_program.cpp)
+together with the engine's planner sources -- test infrastructure, CPU only."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(ROOT, "ket_b200", "csrc")
+OUT = os.path.join(HERE, "cpp", "_build", "libemu.so")
+SRCS = [os.path.join(HERE, "cpp", "emulate_program.cpp"), os.path.join(CSRC, "planner.cpp"),
+        os.path.join(CSRC, "program.cpp")]
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    deps = SRCS + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(d) for d in deps):
+        os.makedirs(os.path.dirname(OUT), exist_ok=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", CSRC, "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+                        "-o", OUT, *SRCS], check=True)
+    L = C.CDLL(OUT)
+    from ket_b200._lib import ket_op
+    L.emu_apply.restype = C.c_int
+    L.emu_apply.argtypes = [C.c_int, C.POINTER(ket_op), C.c_size_t, C.POINTER(C.c_double), C.c_size_t, C.c_int,
+                            C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    _lib = L
+    return L
+
+
+def emu_apply(n, ops, init_state, prune=True, fusion=-1):
+    from ket_b200.circuit import ops_to_abi
+    arr, m, k = ops_to_abi(ops)
+    st = np.ascontiguousarray(init_state, dtype=np.complex128).copy()
+    passes = (C.c_int64 * 2)()
+    mv = np.ascontiguousarray(m).view(np.float64)
+    rc = lib().emu_apply(n, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, 1 if prune else 0, fusion,
+                         st.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)), passes)
+    return rc, st, list(passes)

@@ -213,3 +213,22 @@ def test_invalid_ops_leave_state_untouched():
     with pytest.raises(K.RangeError):
         st.apply_abi(arr, m, k)
     assert np.array_equal(st.amplitudes_dense(), before)
+
+
+@pytest.mark.parametrize("n", [21, 22, 24, 26])
+def test_fused_equals_unfused_many_tiles(n):
+    """States with many tiles per CTA (the persistent loop's later iterations):
+    the fused passes give the unfused per-gate result, run twice (a race would
+    show up as a difference between runs)."""
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import DeviceState, flatten_ops, ops_to_abi
+    c, _ = W.brickwork_qft(n, 10, 42)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    res = []
+    for fusion in (-1, -1, 0):
+        st = DeviceState(n)
+        st.apply_abi(arr, m, k, fusion=fusion, prune=False)
+        res.append(st.amplitudes_dense())
+        del st
+    assert np.max(np.abs(res[0] - res[2])) < 1e-13
+    assert np.array_equal(res[0], res[1])
