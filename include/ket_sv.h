@@ -109,6 +109,10 @@ KET_API int ket_ctx_scratch_bytes(const ket_ctx* ctx, uint64_t* out);
  * counterpart in the reference (which only times whole calls, benchmark/run.mjs:16-35). */
 KET_API int ket_ctx_profile(ket_ctx* ctx, int enable);
 KET_API int ket_ctx_profile_read(ket_ctx* ctx, int* kinds, float* ms, size_t cap, size_t* count);
+/* The context's CUDA stream (a cudaStream_t), so that a caller can order its
+ * own work or record timing events against the engine's launches.  No
+ * counterpart in the reference. */
+KET_API int ket_ctx_stream(const ket_ctx* ctx, void** stream);
 /* Kernel launches made by the context so far. */
 KET_API int ket_ctx_launch_count(const ket_ctx* ctx, uint64_t* count);
 /* Bytes the context has copied host->device and device->host so far. */

@@ -222,6 +222,12 @@ int ket_ctx_io_bytes(const ket_ctx* c, uint64_t* h2d, uint64_t* d2h) {
   return KET_OK;
 }
 
+int ket_ctx_stream(const ket_ctx* c, void** out) {
+  if (!c || !out) return fail(KET_ERR_TYPE, "null argument");
+  *out = (void*)c->stream;
+  return KET_OK;
+}
+
 int ket_ctx_launch_count(const ket_ctx* c, uint64_t* out) {
   if (!c || !out) return fail(KET_ERR_TYPE, "null argument");
   *out = c->launches;
