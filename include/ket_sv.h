@@ -167,6 +167,21 @@ KET_API int ket_probs_sparse(const ket_state* st, double threshold, uint64_t* id
                      uint64_t* count);
 /* marginals() (circuit.ts:1508-1518): out[q] = P(qubit q = 1), q = 0..n-1. */
 KET_API int ket_marginals(const ket_state* st, double* out);
+/* marginals() for callers that cannot allocate device memory (code inside
+ * another framework's memory pool or allocator hooks, or that only lends
+ * buffers it already owns).  amp: the caller's device array of 2^nqubits
+ * amplitudes (precision KET_C128 or KET_C64); out: the caller's device array of
+ * nqubits doubles, out[q] = P(qubit q = 1).  The work is queued on `stream` (a
+ * cudaStream_t, NULL = the default stream) and the call returns without
+ * waiting.  The reduction scratch is a fixed device array of
+ * KET_NOALLOC_SCRATCH_BYTES held by every GPU that loads the library until the
+ * process exits; the call allocates nothing and rejects sizes whose scratch
+ * would exceed it.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race and give wrong results.
+ * No counterpart in the reference. */
+#define KET_NOALLOC_SCRATCH_BYTES (2048u * 40u * 8u)
+KET_API int ket_marginals_noalloc(const void* amp, int nqubits, int precision, double* out, void* stream);
 /* Joint distribution of m qubits: out[j] = P(bit k of j = qubit qubits[k], for all k), 2^m bins (1 <= m <= 12). */
 KET_API int ket_marginal_dist(const ket_state* st, const int* qubits, int m, double* out);
 /* Sum of |a|^2 (FP64 accumulation). */

@@ -73,6 +73,7 @@ def lib():
             "ket_ctx_profile_read": (i32, [vp, P(i32), P(C.c_float), sz, P(sz)]),
             "ket_ctx_launch_count": (i32, [vp, P(u64)]),
             "ket_ctx_stream": (i32, [vp, P(vp)]),
+            "ket_marginals_noalloc": (i32, [vp, i32, i32, vp, vp]),
             "ket_ctx_io_bytes": (i32, [vp, P(u64), P(u64)]),
             "ket_state_alloc": (i32, [vp, i32, i32, P(vp)]),
             "ket_state_free": (i32, [vp]),
