@@ -243,6 +243,7 @@ static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpa
     for (int q : p.hbits) S |= uint64_t(1) << q;
     for (int q = 0; q < s->n; q++)
       if (!((S >> q) & 1)) a.ctxbits[a.nctx++] = q;
+    a.pairbit = -1;  // the probes sum per CTA: one tile per thread
     a.thr = 1e-14;
     a.qthr = 1e-7;
     a.status = c->d_status;

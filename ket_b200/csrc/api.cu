@@ -429,6 +429,7 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
       a.nctx = 0;
       for (int q = 0; q < s->n; q++)
         if (!((S >> q) & 1)) a.ctxbits[a.nctx++] = q;
+      a.pairbit = choose_pairbit(prog, a);
       a.thr = 1e-14;
       a.qthr = 1e-7;
       a.status = c->d_status;

@@ -6,23 +6,35 @@
 // are split into 5 lane bits, 3 warp bits and 4 register bits; a gate whose
 // target is a register bit is applied inside each thread, a gate on a lane
 // bit uses warp shuffles, and a gate on a warp bit first re-lays the tile out
-// through shared memory (FO_EXCH, XOR-swizzled so lanes hit distinct banks).
-// Diagonal gates need no pairing and apply on any qubit, in or out of the
-// tile.  The global load and store use a layout whose lane bits are the
-// tile's low bits, so every warp touches whole 128-byte lines.  A pass costs
-// one read and one write of the state however many gates it holds; the
-// persistent grid keeps two CTAs per SM so one CTA's loads overlap the
-// other's arithmetic.
+// through shared memory (FO_EXCH).  Diagonal gates need no pairing and apply
+// on any qubit, in or out of the tile.  The global load and store use a
+// layout whose lane bits are the tile's low bits, so every warp touches whole
+// 128-byte lines.  A pass costs one read and one write of the state however
+// many gates it holds; the persistent grid keeps two CTAs per SM so one CTA's
+// loads overlap the other's arithmetic.
 //
-// Arithmetic is branch-free inside an op (controls become selects), so the
-// eight independent amplitude pairs of a register-bit gate interleave; the
-// per-gate pruning of the reference (|a|^2 < 1e-14 -> 0) is one integer test
-// on the exponent words of all 16 amplitudes, with the exact FP64 check only
-// in the rare case that some amplitude is below 1e-7 in magnitude.
+// The kernel is issue-bound, so the per-op overhead is kept small:
+//   * an op's first 16 bytes hold everything needed to skip or dispatch it,
+//     and the next op's header is fetched while the current one runs;
+//   * the exchange buffer is XOR-swizzled with a map that is linear over
+//     GF(2), so the 16 slot addresses of a thread are its base address XOR
+//     combinations of four per-layout constants (15 XORs per layout);
+//   * global addresses are a per-thread base plus sums of four per-layout
+//     byte offsets computed on the host;
+//   * threads whose thread-bit controls fail skip an op outright (shuffles
+//     use the mask of lanes that take part);
+//   * the per-gate pruning of the reference (|a|^2 < 1e-14 -> 0) is screened
+//     with FP32 min/max over the high words of all 16 amplitudes; the exact
+//     FP64 test runs only when some amplitude is below 1e-7 in magnitude.
 #include <algorithm>
 
 #include "common.cuh"
 #include "launch.h"
+
+// Resident CTAs per SM: the register budget per thread is 65536 / (256 * this).
+#ifndef KET_FUSED_CTAS_PER_SM
+#define KET_FUSED_CTAS_PER_SM 1
+#endif
 
 namespace ket {
 
@@ -30,101 +42,110 @@ namespace {
 
 __constant__ uint16_t c_slotmask[16];  // slots j with (j & creg) == creg
 
+// ---------------------------------------------------------------- shared memory
+__device__ __forceinline__ void sts(uint32_t a, const cpx<double>& v) {
+  asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(v.re), "d"(v.im) : "memory");
+}
+__device__ __forceinline__ void sts(uint32_t a, const cpx<float>& v) {
+  asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.re), "f"(v.im) : "memory");
+}
+__device__ __forceinline__ void lds(uint32_t a, cpx<double>& v) {
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.re), "=d"(v.im) : "r"(a) : "memory");
+}
+__device__ __forceinline__ void lds(uint32_t a, cpx<float>& v) {
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.re), "=f"(v.im) : "r"(a) : "memory");
+}
+
 template <typename R>
-struct SwzT;
-template <>
-struct SwzT<double> {  // 16-byte elements: 8 per 128-byte bank row
-  static __device__ __forceinline__ uint32_t f(uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7u); }
-};
-template <>
-struct SwzT<float> {  // 8-byte elements: 16 per bank row
-  static __device__ __forceinline__ uint32_t f(uint32_t i) { return i ^ (((i >> 4) ^ (i >> 8)) & 15u); }
+__device__ __forceinline__ uint32_t swz(uint32_t i) {
+  return exch_offset(i, sizeof(R) == 4);
+}
+
+// A thread's view of a layout in the exchange buffer: slot j lives at byte
+// b ^ (j0 ? s0 : 0) ^ (j1 ? s1 : 0) ^ (j2 ? s2 : 0) ^ (j3 ? s3 : 0).
+struct SLay {
+  uint32_t b, s0, s1, s2, s3;
 };
 
-// Magnitude word of a component for the quick pruning test.
-__device__ __forceinline__ uint32_t magw(double v) { return (uint32_t)__double2hiint(v) & 0x7fffffffu; }
-__device__ __forceinline__ uint32_t magw(float v) { return __float_as_uint(v) & 0x7fffffffu; }
-template <typename R> struct Tiny;
-template <> struct Tiny<double> { static constexpr uint32_t w = 0x3E7AD7F3u; };  // > hi word of 1e-7
-template <> struct Tiny<float> { static constexpr uint32_t w = 0x33D6BF96u; };   // > bits of 1e-7f
+__device__ __forceinline__ uint32_t soff(const SLay& l, int j) {
+  uint32_t o = l.b;
+  if (j & 1) o ^= l.s0;
+  if (j & 2) o ^= l.s1;
+  if (j & 4) o ^= l.s2;
+  if (j & 8) o ^= l.s3;
+  return o;
+}
+
+// bx[r] = exchange offset of role r's tile bit.
+__device__ __forceinline__ SLay make_slay(const uint32_t* bx, int lane, int warp) {
+  SLay l;
+  uint32_t b = 0;
+#pragma unroll
+  for (int r = 0; r < 5; r++)
+    if ((lane >> r) & 1) b ^= bx[r];
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+    if ((warp >> r) & 1) b ^= bx[5 + r];
+  l.b = b;
+  l.s0 = bx[8];
+  l.s1 = bx[9];
+  l.s2 = bx[10];
+  l.s3 = bx[11];
+  return l;
+}
+
+// FO_EXCH keeps the new layout's 12 offsets as uint16 in its matrix area.
+__device__ __forceinline__ SLay exch_slay(const FOp* op, int lane, int warp) {
+  const uint4 q0 = __ldg(reinterpret_cast<const uint4*>(op->m));
+  const uint2 q1 = __ldg(reinterpret_cast<const uint2*>(op->m) + 2);
+  const uint32_t w[6] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+  uint32_t bx[12];
+#pragma unroll
+  for (int r = 0; r < 12; r++) bx[r] = (w[r >> 1] >> (16 * (r & 1))) & 0xffffu;
+  return make_slay(bx, lane, warp);
+}
+
+template <typename R>
+__device__ __forceinline__ void write_tile(uint32_t smb, const SLay& l, const cpx<R>* x) {
+#pragma unroll
+  for (int j = 0; j < 16; j++) sts(smb + soff(l, j), x[j]);
+}
+template <typename R>
+__device__ __forceinline__ void read_tile(uint32_t smb, const SLay& l, cpx<R>* x) {
+#pragma unroll
+  for (int j = 0; j < 16; j++) lds(smb + soff(l, j), x[j]);
+}
+
+// ---------------------------------------------------------------- pruning screen
+__device__ __forceinline__ float hiabs(double v) { return fabsf(__int_as_float(__double2hiint(v))); }
+__device__ __forceinline__ float hiabs(float v) { return fabsf(v); }
+// Screening thresholds: for doubles the high word read as a float preserves
+// the order of |v|; 0x3E7AD7F3 lies just above the high word of 1e-7.
+__device__ __forceinline__ float tiny_screen(double) { return __int_as_float(0x3E7AD7F3); }
+__device__ __forceinline__ float tiny_screen(float) { return __int_as_float(0x33D6BF96); }  // just above 1e-7f
 
 template <typename R>
 __device__ __forceinline__ void prune16(cpx<R>* x, double thr, double qthr) {
-  uint32_t any = 0;
+  // an amplitude can be pruned only if both components are below 1e-7
+  float t[16];
 #pragma unroll
-  for (int j = 0; j < 16; j++) any |= (uint32_t)(max(magw(x[j].re), magw(x[j].im)) < Tiny<R>::w);
-  if (any) {
+  for (int j = 0; j < 16; j++) t[j] = fmaxf(hiabs(x[j].re), hiabs(x[j].im));
+#pragma unroll
+  for (int w = 8; w > 0; w >>= 1)
+#pragma unroll
+    for (int j = 0; j < w; j++) t[j] = fminf(t[j], t[j + w]);
+  if (t[0] < tiny_screen(R(0))) {
 #pragma unroll
     for (int j = 0; j < 16; j++) prune_amp(x[j], thr, qthr);
   }
 }
 
-struct Layout {
-  uint32_t tbase;   // tile index bits contributed by this thread's lane and warp
-  uint32_t rp[4];   // tile bit of each register bit (as a mask)
-};
-
-__device__ __forceinline__ Layout make_layout(const uint8_t* pos, int lane, int warp) {
-  Layout L;
-  uint32_t t = 0;
-#pragma unroll
-  for (int l = 0; l < 5; l++) t |= (uint32_t)((lane >> l) & 1) << pos[l];
-#pragma unroll
-  for (int w = 0; w < 3; w++) t |= (uint32_t)((warp >> w) & 1) << pos[5 + w];
-  L.tbase = t;
-#pragma unroll
-  for (int k = 0; k < 4; k++) L.rp[k] = 1u << pos[8 + k];
-  return L;
-}
-
-__device__ __forceinline__ uint32_t rofs(const Layout& L, int j) {
-  uint32_t o = 0;
-  if (j & 1) o |= L.rp[0];
-  if (j & 2) o |= L.rp[1];
-  if (j & 4) o |= L.rp[2];
-  if (j & 8) o |= L.rp[3];
-  return o;
-}
-
-// Global index of tile bit p: p < L -> qubit p, else hbits[p - L].
-__device__ __forceinline__ uint64_t gbit(const Pass2Args& a, int p) {
-  return uint64_t(1) << (p < a.L ? p : a.hbits[p - a.L]);
-}
-
-struct GLayout {
-  uint64_t gthr;
-  uint64_t gr[4];
-};
-
-__device__ __forceinline__ GLayout make_glayout(const Pass2Args& a, const uint8_t* pos, int lane, int warp) {
-  GLayout G;
-  uint64_t t = 0;
-#pragma unroll
-  for (int l = 0; l < 5; l++)
-    if ((lane >> l) & 1) t |= gbit(a, pos[l]);
-#pragma unroll
-  for (int w = 0; w < 3; w++)
-    if ((warp >> w) & 1) t |= gbit(a, pos[5 + w]);
-  G.gthr = t;
-#pragma unroll
-  for (int k = 0; k < 4; k++) G.gr[k] = gbit(a, pos[8 + k]);
-  return G;
-}
-
-__device__ __forceinline__ uint64_t grofs(const GLayout& G, int j) {
-  uint64_t o = 0;
-  if (j & 1) o |= G.gr[0];
-  if (j & 2) o |= G.gr[1];
-  if (j & 4) o |= G.gr[2];
-  if (j & 8) o |= G.gr[3];
-  return o;
-}
-
+// ---------------------------------------------------------------- register and lane ops
 template <typename R>
-__device__ __forceinline__ cpx<R> shfl_xor_c(cpx<R> v, int mask) {
+__device__ __forceinline__ cpx<R> shfl_xor_c(cpx<R> v, int mask, uint32_t members) {
   cpx<R> o;
-  o.re = __shfl_xor_sync(0xffffffffu, v.re, mask);
-  o.im = __shfl_xor_sync(0xffffffffu, v.im, mask);
+  o.re = __shfl_xor_sync(members, v.re, mask);
+  o.im = __shfl_xor_sync(members, v.im, mask);
   return o;
 }
 
@@ -136,28 +157,56 @@ __device__ __forceinline__ cpx<R> sel(bool p, cpx<R> a, cpx<R> b) {
   return o;
 }
 
-// y0 = m00 x0 + m01 x1, y1 = m10 x0 + m11 x1.  FORM 1: all entries real;
+// Register swaps go through inline PTX with tied operands: every amplitude
+// stays in its own loop-carried variable, so a permutation op does not force
+// the register allocator to re-home the whole tile across the op loop.
+__device__ __forceinline__ void swap_c(cpx<double>& a, cpx<double>& b) {
+  asm("{\n .reg .f64 t;\n mov.f64 t, %0;\n mov.f64 %0, %2;\n mov.f64 %2, t;\n"
+      " mov.f64 t, %1;\n mov.f64 %1, %3;\n mov.f64 %3, t;\n}"
+      : "+d"(a.re), "+d"(a.im), "+d"(b.re), "+d"(b.im));
+}
+__device__ __forceinline__ void swap_c(cpx<float>& a, cpx<float>& b) {
+  asm("{\n .reg .f32 t;\n mov.f32 t, %0;\n mov.f32 %0, %2;\n mov.f32 %2, t;\n"
+      " mov.f32 t, %1;\n mov.f32 %1, %3;\n mov.f32 %3, t;\n}"
+      : "+f"(a.re), "+f"(a.im), "+f"(b.re), "+f"(b.im));
+}
+// y0 = m00 x0 + m01 x1, y1 = m10 x0 + m11 x1, in place: the cross terms are
+// formed first, so each output overwrites its own input with its last use and
+// the loop-carried registers need no copies.  FORM 1: all entries real;
 // FORM 2: m00, m11 real and m01, m10 imaginary (Rx-like); 0: general.
 template <typename R, int FORM>
 __device__ __forceinline__ void mat2x2(cpx<R>& x0, cpx<R>& x1, const R* m) {
-  cpx<R> y0, y1;
   if (FORM == 2) {
-    // (a + i b)(xr + i xi) with a = 0: (-b xi, b xr)
-    y0.re = fma(m[0], x0.re, -m[3] * x1.im);
-    y0.im = fma(m[0], x0.im, m[3] * x1.re);
-    y1.re = fma(m[6], x1.re, -m[5] * x0.im);
-    y1.im = fma(m[6], x1.im, m[5] * x0.re);
+    const R p1 = m[3] * x1.im, p2 = m[3] * x1.re, p3 = m[5] * x0.im, p4 = m[5] * x0.re;
+    x0.re = fma(m[0], x0.re, -p1);
+    x0.im = fma(m[0], x0.im, p2);
+    x1.re = fma(m[6], x1.re, -p3);
+    x1.im = fma(m[6], x1.im, p4);
   } else if (FORM == 1) {
-    y0.re = fma(m[0], x0.re, m[2] * x1.re);
-    y0.im = fma(m[0], x0.im, m[2] * x1.im);
-    y1.re = fma(m[4], x0.re, m[6] * x1.re);
-    y1.im = fma(m[4], x0.im, m[6] * x1.im);
+    const R p1 = m[2] * x1.re, p2 = m[2] * x1.im, p3 = m[4] * x0.re, p4 = m[4] * x0.im;
+    x0.re = fma(m[0], x0.re, p1);
+    x0.im = fma(m[0], x0.im, p2);
+    x1.re = fma(m[6], x1.re, p3);
+    x1.im = fma(m[6], x1.im, p4);
   } else {
-    y0 = mac2<R>(m[0], m[1], x0, m[2], m[3], x1);
-    y1 = mac2<R>(m[4], m[5], x0, m[6], m[7], x1);
+    // cross terms m01 x1 and m10 x0
+    const R c0r = fma(m[2], x1.re, -m[3] * x1.im), c0i = fma(m[2], x1.im, m[3] * x1.re);
+    const R c1r = fma(m[4], x0.re, -m[5] * x0.im), c1i = fma(m[4], x0.im, m[5] * x0.re);
+    const R t0 = fma(-m[1], x0.im, c0r), u0 = fma(m[1], x0.re, c0i);
+    const R t1 = fma(-m[7], x1.im, c1r), u1 = fma(m[7], x1.re, c1i);
+    x0.re = fma(m[0], x0.re, t0);
+    x0.im = fma(m[0], x0.im, u0);
+    x1.re = fma(m[6], x1.re, t1);
+    x1.im = fma(m[6], x1.im, u1);
   }
-  x0 = y0;
-  x1 = y1;
+}
+
+// x *= (mr + i mi), in place.
+template <typename R>
+__device__ __forceinline__ void cmul_in(cpx<R>& x, R mr, R mi) {
+  const R p = mi * x.im, q = mi * x.re;
+  x.re = fma(mr, x.re, -p);
+  x.im = fma(mr, x.im, q);
 }
 
 template <typename R, int A, int FORM>
@@ -182,27 +231,28 @@ __device__ __forceinline__ void mat1_reg(cpx<R>* x, const R* m, uint32_t smask) 
   }
 }
 
+// X on register bit A where register bit C is 1 (a CNOT inside the thread).
+template <typename R, int A, int C>
+__device__ __forceinline__ void x1c_reg(cpx<R>* x) {
+#pragma unroll
+  for (int j = 0; j < 16; j++)
+    if (!(j & (1 << A)) && (j & (1 << C))) swap_c(x[j], x[j | (1 << A)]);
+}
+
+// diag(1, d1) on register bit A where register bit C is 1 (a controlled phase).
+template <typename R, int A, int C>
+__device__ __forceinline__ void diag1c_reg(cpx<R>* x, R d1r, R d1i) {
+#pragma unroll
+  for (int j = 0; j < 16; j++)
+    if ((j & (1 << A)) && (j & (1 << C))) cmul_in<R>(x[j], d1r, d1i);
+}
+
+// X on register bit A (no register controls: other controls skip the thread).
 template <typename R, int A>
-__device__ __forceinline__ void x1_reg(cpx<R>* x, uint32_t smask) {
-  if (smask == 0xffffu) {
+__device__ __forceinline__ void x1_reg(cpx<R>* x) {
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-      if (j & (1 << A)) continue;
-      cpx<R> t = x[j];
-      x[j] = x[j | (1 << A)];
-      x[j | (1 << A)] = t;
-    }
-    return;
-  }
-#pragma unroll
-  for (int j = 0; j < 16; j++) {
-    if (j & (1 << A)) continue;
-    const int j1 = j | (1 << A);
-    const bool p = (smask >> j) & 1;
-    cpx<R> t0 = x[j], t1 = x[j1];
-    x[j] = sel<R>(p, t1, t0);
-    x[j1] = sel<R>(p, t0, t1);
-  }
+  for (int j = 0; j < 16; j++)
+    if (!(j & (1 << A))) swap_c(x[j], x[j | (1 << A)]);
 }
 
 // diag(d0, d1) on register bit A; D0ONE: d0 == 1, so bit-0 slots are untouched.
@@ -213,7 +263,7 @@ __device__ __forceinline__ void diag_reg(cpx<R>* x, R d0r, R d0i, R d1r, R d1i, 
     for (int j = 0; j < 16; j++) {
       const bool one = (j >> A) & 1;
       if (D0ONE && !one) continue;
-      x[j] = cmul<R>(one ? d1r : d0r, one ? d1i : d0i, x[j]);
+      cmul_in<R>(x[j], one ? d1r : d0r, one ? d1i : d0i);
     }
     return;
   }
@@ -221,14 +271,18 @@ __device__ __forceinline__ void diag_reg(cpx<R>* x, R d0r, R d0i, R d1r, R d1i, 
   for (int j = 0; j < 16; j++) {
     const bool one = (j >> A) & 1;
     if (D0ONE && !one) continue;
-    const R dr = one ? d1r : d0r, di = one ? d1i : d0i;
-    cpx<R> y = cmul<R>(dr, di, x[j]);
+    cpx<R> y = cmul<R>(one ? d1r : d0r, one ? d1i : d0i, x[j]);
     x[j] = sel<R>((smask >> j) & 1, y, x[j]);
   }
 }
 
 template <typename R>
 __device__ __forceinline__ void phase_all(cpx<R>* x, R dr, R di, uint32_t smask) {
+  if (smask == 0xffffu) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) cmul_in<R>(x[j], dr, di);
+    return;
+  }
 #pragma unroll
   for (int j = 0; j < 16; j++) {
     cpx<R> y = cmul<R>(dr, di, x[j]);
@@ -236,61 +290,27 @@ __device__ __forceinline__ void phase_all(cpx<R>* x, R dr, R di, uint32_t smask)
   }
 }
 
-// ---------------------------------------------------------------- TMA staging
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-// Bulk copy (TMA engine, no tensor map): global -> shared, completion on bar.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-// Bounded wait: false when the iteration limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t it = 0; it < (1u << 26); it++)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-// Issue the bulk copies of one tile (2^(12-L) contiguous chunks of 2^L amplitudes) into buf.
 template <typename R>
-__device__ __forceinline__ void issue_tile(const Pass2Args& a, const typename Vec2<R>::T* amp, uint64_t tile,
-                                           cpx<R>* buf, uint64_t* bar, int tid) {
-  const uint32_t nch = 1u << (KET_T2_BITS - a.L);
-  const uint32_t cbytes = (uint32_t)sizeof(cpx<R>) << a.L;
-  if (tid < 32) {
-    uint64_t ctx = 0;
-    for (int j = 0; j < a.nctx; j++)
-      if ((tile >> j) & 1) ctx |= uint64_t(1) << a.ctxbits[j];
-    if (tid == 0) mbar_expect_tx(bar, nch * cbytes);
-    __syncwarp();
-    for (uint32_t c = tid; c < nch; c += 32) {
-      uint64_t g = ctx;
-      for (int j = 0; j < a.nh; j++)
-        if ((c >> j) & 1) g |= uint64_t(1) << a.hbits[j];
-      bulk_g2s(buf + ((size_t)c << a.L), amp + g, cbytes, bar);
-    }
+__device__ __forceinline__ void load_m8(const FOp* op, R* m) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(op->m) + q);
+    m[2 * q] = (R)v.x;
+    m[2 * q + 1] = (R)v.y;
   }
 }
 
-// Adjoint probes.  Register bit 3 selects psi (0) / lambda (1).
+// ---------------------------------------------------------------- tiles
+// Global index bits of a tile outside its 12 tile qubits.
+__device__ __forceinline__ uint64_t ctx_of(const Pass2Args& a, uint64_t tile) {
+  uint64_t cb = 0;
+  for (int j = 0; j < a.nctx; j++)
+    if ((tile >> j) & 1) cb |= uint64_t(1) << a.ctxbits[j];
+  return cb;
+}
+
+// ---------------------------------------------------------------- adjoint probes
+// Register bit 3 selects psi (0) / lambda (1).
 // Re<lambda| D |psi> with D 2x2 on register bit A.
 template <typename R, int A>
 __device__ __forceinline__ double grad_m(const cpx<R>* x, const R* d, uint32_t smask) {
@@ -327,300 +347,360 @@ __device__ __forceinline__ void grad_accum(double* sgrad, int slot, int warp, in
   if (lane == 0) sgrad[slot * 8 + warp] += v;
 }
 
-template <typename R, int NT, bool GRAD>
-__global__ void __launch_bounds__(NT, GRAD ? 1 : 2) k_fused2(Pass2Args a) {
+// ---------------------------------------------------------------- the pass
+template <typename R, int NT, bool GRAD, int TT>
+__global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
   typedef typename Vec2<R>::T V;
   extern __shared__ __align__(128) unsigned char smraw[];
-  cpx<R>* sm = reinterpret_cast<cpx<R>*>(smraw);  // exchange buffer (swizzled)
-  double* sgrad = reinterpret_cast<double*>(smraw + (sizeof(cpx<R>) << KET_T2_BITS));  // [slot][warp]
+  // shared memory: one exchange buffer per tile a thread holds | gradient partials
+  constexpr uint32_t TB = (uint32_t)sizeof(cpx<R>) << KET_T2_BITS;
+  const uint32_t smb = (uint32_t)__cvta_generic_to_shared(smraw);
+  double* sgrad = reinterpret_cast<double*>(smraw + TB * TT);  // [slot][warp]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (GRAD) {
     for (int i = threadIdx.x; i < a.nslots * 8; i += NT) sgrad[i] = 0.0;
     __syncthreads();
   }
-  V* amp = reinterpret_cast<V*>(a.amp);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
   constexpr double thr = 1e-14, qthr = 1e-7;  // accumulate()'s threshold (statevector.ts:24) and its root
-  cpx<R> x[16];
+  char* const amp = reinterpret_cast<char*>(a.amp);
+  // Each thread holds TT tiles that differ only in tile-index bit a.pairbit, a
+  // qubit outside the tile that no op of the pass reads: every op then acts
+  // on all TT tiles the same way.
+  const uint64_t ngroups = (uint64_t(1) << (a.n - KET_T2_BITS)) / TT;
+  const uint64_t pairq = TT > 1 ? uint64_t(1) << a.ctxbits[a.pairbit] : 0;
+  cpx<R> x[TT][16];
 
-  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    uint64_t ctxbase = 0;
-    for (int j = 0; j < a.nctx; j++)
-      if ((tile >> j) & 1) ctxbase |= uint64_t(1) << a.ctxbits[j];
+  for (uint64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const uint64_t tile0 = TT > 1 ? insert0(grp, a.pairbit) : grp;
+    const uint64_t ctx0 = ctx_of(a, tile0);
     {
-      // global addresses are rebuilt here and at the store rather than kept
-      // live through the op loop (register pressure); lane l holds tile bit l,
-      // so each warp load covers whole 128-byte lines
-      const GLayout gl = make_glayout(a, a.load_pos, lane, warp);
+      uint64_t gl = 0;
 #pragma unroll
-      for (int j = 0; j < 16; j++) x[j] = ld_amp<R>(amp + (ctxbase | gl.gthr | grofs(gl, j)));
+      for (int r = 0; r < 5; r++)
+        if ((lane >> r) & 1) gl += a.lgb[r];
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+        if ((warp >> r) & 1) gl += a.lgb[5 + r];
+#pragma unroll
+      for (int t = 0; t < TT; t++) {
+        const char* p = amp + (ctx0 | (t ? pairq : 0)) * sizeof(V) + gl;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          uint64_t o = 0;
+          if (j & 1) o += a.lgb[8];
+          if (j & 2) o += a.lgb[9];
+          if (j & 4) o += a.lgb[10];
+          if (j & 8) o += a.lgb[11];
+          x[t][j] = ld_amp<R>(reinterpret_cast<const V*>(p + o));
+        }
+      }
     }
-    Layout L = make_layout(a.load_pos, lane, warp);
+    SLay sl = make_slay(a.lbx, lane, warp);
+    uint4 hn = a.nops > 0 ? __ldg(reinterpret_cast<const uint4*>(a.ops)) : make_uint4(0u, 0u, 0u, 0u);
     for (int k = 0; k < a.nops; k++) {
       const FOp* op = a.ops + k;
-      const uint4 h0 = __ldg(reinterpret_cast<const uint4*>(op));
-      const int type = h0.x & 0xff, oa = (h0.x >> 8) & 0xff, ob = (h0.x >> 16) & 0xff, fl = h0.x >> 24;
-      if (type == FO_EXCH || type == FO_RELABEL) {
-        uint8_t pos[KET_T2_BITS];
-        const uint32_t pw[3] = {h0.y, h0.z, h0.w};
-#pragma unroll
-        for (int q = 0; q < KET_T2_BITS; q++) pos[q] = (uint8_t)(pw[q >> 2] >> (8 * (q & 3)));
-        if (type == FO_RELABEL) {
-          L = make_layout(pos, lane, warp);
-          continue;
-        }
+      const uint4 h = hn;
+      if (k + 1 < a.nops) hn = __ldg(reinterpret_cast<const uint4*>(op + 1));
+      const int opc = h.x & 0xff, oa = (h.x >> 8) & 0xff;
+      const uint32_t fl = (h.x >> 16) & 0xffu, creg = h.x >> 24, cthr = h.y & 0xffu;
+      if (opc == OC_EXCH) {
         __syncthreads();
 #pragma unroll
-        for (int j = 0; j < 16; j++) sm[SwzT<R>::f(L.tbase | rofs(L, j))] = x[j];
+        for (int t = 0; t < TT; t++) write_tile<R>(smb + t * TB, sl, x[t]);
         __syncthreads();
-        L = make_layout(pos, lane, warp);
+        sl = exch_slay(op, lane, warp);
 #pragma unroll
-        for (int j = 0; j < 16; j++) x[j] = sm[SwzT<R>::f(L.tbase | rofs(L, j))];
+        for (int t = 0; t < TT; t++) read_tile<R>(smb + t * TB, sl, x[t]);
         continue;
       }
-      const uint4 h1 = __ldg(reinterpret_cast<const uint4*>(op) + 1);  // creg, cthr, ctile, d0|d1
-      const uint64_t cctx = __ldg(reinterpret_cast<const unsigned long long*>(op) + 4);
-      if ((ctxbase & cctx) != cctx) continue;  // uniform over the CTA
-      const bool pr = fl & FOF_PRUNE;
-      const uint32_t creg = h1.x, cthr = h1.y;
-      const uint32_t smask = ((uint32_t)(tid & cthr) == cthr) ? (uint32_t)c_slotmask[creg & 15] : 0u;
+      const uint64_t cctx = ((uint64_t)h.w << 32) | h.z;
+      if ((ctx0 & cctx) != cctx) continue;  // uniform over the CTA (and the same for all TT tiles)
       const double* M = op->m;
-      switch (type) {
-        case FO_MAT1R: {
-          R m[8];
+      if (opc == OC_SWAPS || opc == OC_MAT2S || opc == OC_GRADM2 || opc == OC_DIAG || opc == OC_X1S) {
+        // Rare ops (controlled swaps, dense 4x4s, two-qubit diagonals,
+        // multi-controlled X, two-qubit probes) run on the shared-memory copy of
+        // the tiles, in the current layout, with small code.
+        if (opc == OC_GRADM2 && !GRAD) continue;
+        const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);
+        const uint32_t ct = h2.y;
+        const int ob = (int)(h2.w & 0xffu);
+        __syncthreads();
 #pragma unroll
-          for (int q = 0; q < 8; q++) m[q] = (R)__ldg(M + q);
-          const int form = (fl & FOF_REAL) ? 1 : ((fl & FOF_RXFORM) ? 2 : 0);
-#define KET_MAT1R(F)                                        \
-  switch (oa) {                                             \
-    case 0: mat1_reg<R, 0, F>(x, m, smask); break;          \
-    case 1: mat1_reg<R, 1, F>(x, m, smask); break;          \
-    case 2: mat1_reg<R, 2, F>(x, m, smask); break;          \
-    default: mat1_reg<R, 3, F>(x, m, smask); break;         \
-  }
-          if (form == 1) { KET_MAT1R(1) } else if (form == 2) { KET_MAT1R(2) } else { KET_MAT1R(0) }
-#undef KET_MAT1R
-          break;
-        }
-        case FO_MAT1L: {
-          const int bitv = (lane >> oa) & 1;
-          // own output = c0 * own + c1 * partner
-          const R c0r = (R)__ldg(M + (bitv ? 6 : 0)), c0i = (R)__ldg(M + (bitv ? 7 : 1));
-          const R c1r = (R)__ldg(M + (bitv ? 4 : 2)), c1i = (R)__ldg(M + (bitv ? 5 : 3));
-          const int msk = 1 << oa;
-          if (fl & FOF_REAL) {
-#pragma unroll
-            for (int j = 0; j < 16; j++) {
-              cpx<R> p = shfl_xor_c<R>(x[j], msk);
-              cpx<R> y;
-              y.re = fma(c0r, x[j].re, c1r * p.re);
-              y.im = fma(c0r, x[j].im, c1r * p.im);
-              x[j] = sel<R>((smask >> j) & 1, y, x[j]);
-            }
-          } else if (fl & FOF_RXFORM) {
-#pragma unroll
-            for (int j = 0; j < 16; j++) {
-              cpx<R> p = shfl_xor_c<R>(x[j], msk);
-              cpx<R> y;
-              y.re = fma(c0r, x[j].re, -c1i * p.im);
-              y.im = fma(c0r, x[j].im, c1i * p.re);
-              x[j] = sel<R>((smask >> j) & 1, y, x[j]);
-            }
-          } else {
-#pragma unroll
-            for (int j = 0; j < 16; j++) {
-              cpx<R> p = shfl_xor_c<R>(x[j], msk);
-              cpx<R> y = mac2<R>(c0r, c0i, x[j], c1r, c1i, p);
-              x[j] = sel<R>((smask >> j) & 1, y, x[j]);
-            }
-          }
-          break;
-        }
-        case FO_X1R:
-          switch (oa) {
-            case 0: x1_reg<R, 0>(x, smask); break;
-            case 1: x1_reg<R, 1>(x, smask); break;
-            case 2: x1_reg<R, 2>(x, smask); break;
-            default: x1_reg<R, 3>(x, smask); break;
-          }
-          break;
-        case FO_X1L: {
-          const int msk = 1 << oa;
-#pragma unroll
-          for (int j = 0; j < 16; j++) {
-            cpx<R> p = shfl_xor_c<R>(x[j], msk);
-            x[j] = sel<R>((smask >> j) & 1, p, x[j]);
-          }
-          break;
-        }
-        case FO_SWAPS: case FO_MAT2S: {
-          // Rare ops (controlled swaps, dense 4x4s) run on the shared-memory
-          // copy of the tile, in the current layout, with small code.
-          __syncthreads();
-#pragma unroll
-          for (int j = 0; j < 16; j++) sm[SwzT<R>::f(L.tbase | rofs(L, j))] = x[j];
-          __syncthreads();
-          const uint32_t ct = h1.z;
-          const int ta = oa, tb = ob, lo = ta < tb ? ta : tb, hi = ta < tb ? tb : ta;
-          for (uint32_t g = tid; g < (1u << (KET_T2_BITS - 2)); g += NT) {
-            uint32_t b0 = insert0_32(insert0_32(g, lo), hi);
-            if ((b0 & ct) != ct) continue;
-            const uint32_t i1 = b0 | (1u << tb), i2 = b0 | (1u << ta), i3 = b0 | (1u << ta) | (1u << tb);
-            if (type == FO_SWAPS) {
-              cpx<R> t = sm[SwzT<R>::f(i1)];
-              sm[SwzT<R>::f(i1)] = sm[SwzT<R>::f(i2)];
-              sm[SwzT<R>::f(i2)] = t;
-              continue;
-            }
-            cpx<R> v[4] = {sm[SwzT<R>::f(b0)], sm[SwzT<R>::f(i1)], sm[SwzT<R>::f(i2)], sm[SwzT<R>::f(i3)]};
-            const uint32_t idx[4] = {b0, i1, i2, i3};
-            for (int r = 0; r < 4; r++) {
-              cpx<R> s0 = mac2<R>((R)__ldg(M + 8 * r), (R)__ldg(M + 8 * r + 1), v[0], (R)__ldg(M + 8 * r + 2),
-                                  (R)__ldg(M + 8 * r + 3), v[1]);
-              cpx<R> s1 = mac2<R>((R)__ldg(M + 8 * r + 4), (R)__ldg(M + 8 * r + 5), v[2], (R)__ldg(M + 8 * r + 6),
-                                  (R)__ldg(M + 8 * r + 7), v[3]);
-              cpx<R> y;
-              y.re = s0.re + s1.re;
-              y.im = s0.im + s1.im;
-              if (pr) prune_amp(y, thr, qthr);
-              sm[SwzT<R>::f(idx[r])] = y;
-            }
-          }
-          __syncthreads();
-#pragma unroll
-          for (int j = 0; j < 16; j++) x[j] = sm[SwzT<R>::f(L.tbase | rofs(L, j))];
-          continue;  // pruning already done
-        }
-        case FO_DIAGR: {
-          const R d0r = (R)__ldg(M + 0), d0i = (R)__ldg(M + 1), d1r = (R)__ldg(M + 2), d1i = (R)__ldg(M + 3);
-          if (fl & FOF_D0ONE) {
-            switch (oa) {
-              case 0: diag_reg<R, 0, true>(x, d0r, d0i, d1r, d1i, smask); break;
-              case 1: diag_reg<R, 1, true>(x, d0r, d0i, d1r, d1i, smask); break;
-              case 2: diag_reg<R, 2, true>(x, d0r, d0i, d1r, d1i, smask); break;
-              default: diag_reg<R, 3, true>(x, d0r, d0i, d1r, d1i, smask); break;
-            }
-          } else {
-            switch (oa) {
-              case 0: diag_reg<R, 0, false>(x, d0r, d0i, d1r, d1i, smask); break;
-              case 1: diag_reg<R, 1, false>(x, d0r, d0i, d1r, d1i, smask); break;
-              case 2: diag_reg<R, 2, false>(x, d0r, d0i, d1r, d1i, smask); break;
-              default: diag_reg<R, 3, false>(x, d0r, d0i, d1r, d1i, smask); break;
-            }
-          }
-          break;
-        }
-        case FO_DIAGT: case FO_DIAGX: {
-          bool one;
-          if (type == FO_DIAGT) one = (tid >> oa) & 1;
-          else one = (ctxbase & __ldg(reinterpret_cast<const unsigned long long*>(op) + 5)) != 0;
-          if ((fl & FOF_D0ONE) && !one) break;
-          const R dr = (R)__ldg(M + (one ? 2 : 0)), di = (R)__ldg(M + (one ? 3 : 1));
-          phase_all<R>(x, dr, di, smask);
-          break;
-        }
-        case FO_DIAG: {
-          const int d0 = (int16_t)(h1.w & 0xffff), d1 = (int16_t)(h1.w >> 16);
-          const uint32_t ct = h1.z;
-          const uint64_t dg0 = __ldg(reinterpret_cast<const unsigned long long*>(op) + 5);
-          const uint64_t dg1 = __ldg(reinterpret_cast<const unsigned long long*>(op) + 6);
-          const int u0 = d0 < 0 ? (int)((ctxbase & dg0) != 0) : 0;
-          const int u1 = d1 == -1 ? (int)((ctxbase & dg1) != 0) : 0;
-          R dm[8];
-#pragma unroll
-          for (int q = 0; q < 8; q++) dm[q] = (R)__ldg(M + q);
-#pragma unroll
-          for (int j = 0; j < 16; j++) {
-            const uint32_t idx = L.tbase | rofs(L, j);
-            const int k0 = d0 >= 0 ? (int)((idx >> d0) & 1) : u0;
-            const int k1 = d1 >= 0 ? (int)((idx >> d1) & 1) : u1;
-            const int kk = d1 != -2 ? 2 * k0 + k1 : k0;
-            R dr = dm[0], di = dm[1];
-            dr = kk == 1 ? dm[2] : dr;
-            di = kk == 1 ? dm[3] : di;
-            dr = kk == 2 ? dm[4] : dr;
-            di = kk == 2 ? dm[5] : di;
-            dr = kk == 3 ? dm[6] : dr;
-            di = kk == 3 ? dm[7] : di;
-            cpx<R> y = cmul<R>(dr, di, x[j]);
-            x[j] = sel<R>((idx & ct) == ct, y, x[j]);
-          }
-          break;
-        }
-        case FO_GRADM: case FO_GRADD: {
-          if (!GRAD) break;
-          // <lambda|D|psi> over this thread's amplitudes: register bit 3 of the
-          // slot index selects psi (0) or lambda (1) -- the planner pins the
-          // ancilla there
-          const int slot = (int16_t)(h1.w >> 16);
-          double acc = 0.0;
-          if (type == FO_GRADM) {
-            R d[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) d[q] = (R)__ldg(M + q);
-            switch (oa) {
-              case 0: acc = grad_m<R, 0>(x, d, smask); break;
-              case 1: acc = grad_m<R, 1>(x, d, smask); break;
-              default: acc = grad_m<R, 2>(x, d, smask); break;
-            }
-          } else {
-            const R d0r = (R)__ldg(M + 0), d0i = (R)__ldg(M + 1), d1r = (R)__ldg(M + 2), d1i = (R)__ldg(M + 3);
-            if (fl & (FOF_TGT_THR | FOF_TGT_CTX)) {
-              const bool one = (fl & FOF_TGT_CTX)
-                                   ? (ctxbase & __ldg(reinterpret_cast<const unsigned long long*>(op) + 5)) != 0
-                                   : (bool)((tid >> oa) & 1);
-              acc = grad_d<R, -1>(x, one ? d1r : d0r, one ? d1i : d0i, one ? d1r : d0r, one ? d1i : d0i, smask);
-            } else {
-              switch (oa) {
-                case 0: acc = grad_d<R, 0>(x, d0r, d0i, d1r, d1i, smask); break;
-                case 1: acc = grad_d<R, 1>(x, d0r, d0i, d1r, d1i, smask); break;
-                default: acc = grad_d<R, 2>(x, d0r, d0i, d1r, d1i, smask); break;
-              }
-            }
-          }
-          grad_accum(sgrad, slot, warp, lane, acc);
-          break;
-        }
-        case FO_GRADM2: {
-          if (!GRAD) break;
-          __syncthreads();
-#pragma unroll
-          for (int j = 0; j < 16; j++) sm[SwzT<R>::f(L.tbase | rofs(L, j))] = x[j];
-          __syncthreads();
-          const int slot = (int16_t)(h1.w >> 16), anc = (int16_t)(h1.w & 0xffff);
-          const uint32_t ct = h1.z;
-          const int ta = oa, tb = ob;
+        for (int t = 0; t < TT; t++) write_tile<R>(smb + t * TB, sl, x[t]);
+        __syncthreads();
+        const int ta = oa, tb = ob;
+        if (GRAD && opc == OC_GRADM2) {
+          const int slot = (int16_t)(h2.z & 0xffff), anc = (int16_t)(h2.z >> 16);
           int b3[3] = {ta, tb, anc};
           for (int u = 1; u < 3; u++)
-            for (int v = u; v > 0 && b3[v - 1] > b3[v]; v--) { int t = b3[v]; b3[v] = b3[v - 1]; b3[v - 1] = t; }
+            for (int v = u; v > 0 && b3[v - 1] > b3[v]; v--) { int w = b3[v]; b3[v] = b3[v - 1]; b3[v - 1] = w; }
           double acc = 0.0;
           for (uint32_t g = tid; g < (1u << (KET_T2_BITS - 3)); g += NT) {
             uint32_t b0 = insert0_32(insert0_32(insert0_32(g, b3[0]), b3[1]), b3[2]);
             if ((b0 & ct) != ct) continue;
             const uint32_t idx[4] = {b0, b0 | (1u << tb), b0 | (1u << ta), b0 | (1u << ta) | (1u << tb)};
             cpx<R> v[4];
-            for (int c = 0; c < 4; c++) v[c] = sm[SwzT<R>::f(idx[c])];
+            for (int c = 0; c < 4; c++) lds(smb + swz<R>(idx[c]), v[c]);
             for (int r = 0; r < 4; r++) {
               cpx<R> s0 = mac2<R>((R)__ldg(M + 8 * r), (R)__ldg(M + 8 * r + 1), v[0], (R)__ldg(M + 8 * r + 2),
                                   (R)__ldg(M + 8 * r + 3), v[1]);
               cpx<R> s1 = mac2<R>((R)__ldg(M + 8 * r + 4), (R)__ldg(M + 8 * r + 5), v[2], (R)__ldg(M + 8 * r + 6),
                                   (R)__ldg(M + 8 * r + 7), v[3]);
-              cpx<R> lam = sm[SwzT<R>::f(idx[r] | (1u << anc))];
+              cpx<R> lam;
+              lds(smb + swz<R>(idx[r] | (1u << anc)), lam);
               acc += (double)lam.re * (s0.re + s1.re) + (double)lam.im * (s0.im + s1.im);
             }
           }
           grad_accum(sgrad, slot, warp, lane, acc);
+          continue;  // read-only: registers still hold the tile
+        }
+        if (opc == OC_X1S) {
+          for (uint32_t g = tid; g < (uint32_t)TT << (KET_T2_BITS - 1); g += NT) {
+            const uint32_t base = smb + (g >> (KET_T2_BITS - 1)) * TB;
+            const uint32_t i0 = insert0_32(g & ((1u << (KET_T2_BITS - 1)) - 1), ob);
+            if ((i0 & ct) != ct) continue;
+            cpx<R> t0, t1;
+            lds(base + swz<R>(i0), t0);
+            lds(base + swz<R>(i0 | (1u << ob)), t1);
+            sts(base + swz<R>(i0), t1);
+            sts(base + swz<R>(i0 | (1u << ob)), t0);
+          }
+          __syncthreads();
+#pragma unroll
+          for (int t = 0; t < TT; t++) read_tile<R>(smb + t * TB, sl, x[t]);
           continue;
+        }
+        if (opc == OC_DIAG) {
+          // d0, d1: tile bits of the two qubits, -1 = outside the tile
+          const int b0t = (int8_t)(h.y >> 8), b1t = (int8_t)(h.y >> 16);
+          const uint64_t dg0 = __ldg(reinterpret_cast<const unsigned long long*>(op) + 4);
+          const uint64_t dg1 = __ldg(reinterpret_cast<const unsigned long long*>(op) + 5);
+          const int u0 = (int)((ctx0 & dg0) != 0), u1 = (int)((ctx0 & dg1) != 0);
+          for (uint32_t g = tid; g < (uint32_t)TT << KET_T2_BITS; g += NT) {
+            const uint32_t base = smb + (g >> KET_T2_BITS) * TB, i = g & ((1u << KET_T2_BITS) - 1);
+            if ((i & ct) != ct) continue;
+            const int k0 = b0t >= 0 ? (int)((i >> b0t) & 1) : u0;
+            const int k1 = b1t >= 0 ? (int)((i >> b1t) & 1) : u1;
+            const int kk = 2 * k0 + k1;
+            cpx<R> v;
+            lds(base + swz<R>(i), v);
+            v = cmul<R>((R)__ldg(M + 2 * kk), (R)__ldg(M + 2 * kk + 1), v);
+            sts(base + swz<R>(i), v);
+          }
+          __syncthreads();
+#pragma unroll
+          for (int t = 0; t < TT; t++) read_tile<R>(smb + t * TB, sl, x[t]);
+          continue;
+        }
+        const int lo = ta < tb ? ta : tb, hi = ta < tb ? tb : ta;
+        const bool pr = fl & FOF_PRUNE;
+        for (uint32_t g = tid; g < (uint32_t)TT << (KET_T2_BITS - 2); g += NT) {
+          const uint32_t base = smb + (g >> (KET_T2_BITS - 2)) * TB;
+          uint32_t b0 = insert0_32(insert0_32(g & ((1u << (KET_T2_BITS - 2)) - 1), lo), hi);
+          if ((b0 & ct) != ct) continue;
+          const uint32_t i1 = b0 | (1u << tb), i2 = b0 | (1u << ta), i3 = b0 | (1u << ta) | (1u << tb);
+          if (opc == OC_SWAPS) {
+            cpx<R> t1, t2;
+            lds(base + swz<R>(i1), t1);
+            lds(base + swz<R>(i2), t2);
+            sts(base + swz<R>(i1), t2);
+            sts(base + swz<R>(i2), t1);
+            continue;
+          }
+          const uint32_t idx[4] = {b0, i1, i2, i3};
+          cpx<R> v[4];
+          for (int c = 0; c < 4; c++) lds(base + swz<R>(idx[c]), v[c]);
+          for (int r = 0; r < 4; r++) {
+            cpx<R> s0 = mac2<R>((R)__ldg(M + 8 * r), (R)__ldg(M + 8 * r + 1), v[0], (R)__ldg(M + 8 * r + 2),
+                                (R)__ldg(M + 8 * r + 3), v[1]);
+            cpx<R> s1 = mac2<R>((R)__ldg(M + 8 * r + 4), (R)__ldg(M + 8 * r + 5), v[2], (R)__ldg(M + 8 * r + 6),
+                                (R)__ldg(M + 8 * r + 7), v[3]);
+            cpx<R> y;
+            y.re = s0.re + s1.re;
+            y.im = s0.im + s1.im;
+            if (pr) prune_amp(y, thr, qthr);
+            sts(base + swz<R>(idx[r]), y);
+          }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < TT; t++) read_tile<R>(smb + t * TB, sl, x[t]);
+        continue;  // pruning already done
+      }
+      const bool thr_ok = ((uint32_t)tid & cthr) == cthr;
+      if (opc >= OC_GRADM) {
+        if (!GRAD) continue;
+        // <lambda|D|psi> over this thread's amplitudes: register bit 3 of the
+        // slot index selects psi (0) or lambda (1) -- the planner pins the
+        // ancilla there.  Every lane takes part in the warp sum.  (TT == 1)
+        const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);
+        const int slot = (int16_t)(h2.z & 0xffff);
+        const uint32_t smask = thr_ok ? (uint32_t)c_slotmask[creg & 15] : 0u;
+        double acc = 0.0;
+        if (opc != OC_GRADD) {
+          R d[8];
+          load_m8<R>(op, d);
+          switch (oa) {
+            case 0: acc = grad_m<R, 0>(x[0], d, smask); break;
+            case 1: acc = grad_m<R, 1>(x[0], d, smask); break;
+            default: acc = grad_m<R, 2>(x[0], d, smask); break;
+          }
+        } else {
+          const R d0r = (R)__ldg(M + 0), d0i = (R)__ldg(M + 1), d1r = (R)__ldg(M + 2), d1i = (R)__ldg(M + 3);
+          if (fl & (FOF_TGT_THR | FOF_TGT_CTX)) {
+            const bool one = (fl & FOF_TGT_CTX) ? (ctx0 & op->dg0) != 0 : (bool)((tid >> oa) & 1);
+            acc = grad_d<R, -1>(x[0], one ? d1r : d0r, one ? d1i : d0i, one ? d1r : d0r, one ? d1i : d0i, smask);
+          } else {
+            switch (oa) {
+              case 0: acc = grad_d<R, 0>(x[0], d0r, d0i, d1r, d1i, smask); break;
+              case 1: acc = grad_d<R, 1>(x[0], d0r, d0i, d1r, d1i, smask); break;
+              default: acc = grad_d<R, 2>(x[0], d0r, d0i, d1r, d1i, smask); break;
+            }
+          }
+        }
+        grad_accum(sgrad, slot, warp, lane, acc);
+        continue;
+      }
+      // Thread-local ops and shuffles among the lanes that take part: a thread
+      // whose thread-bit controls fail leaves its amplitudes alone.
+      if (!thr_ok) continue;
+      const uint32_t smask = creg ? (uint32_t)c_slotmask[creg & 15] : 0xffffu;
+      switch (opc) {
+#define KET_MAT1R(A, F)                             \
+  case OC_MAT1R + 3 * A + F: {                      \
+    R m[8];                                         \
+    load_m8<R>(op, m);                              \
+    for (int t = 0; t < TT; t++) mat1_reg<R, A, F>(x[t], m, smask);                 \
+    break;                                          \
+  }
+        KET_MAT1R(0, 0) KET_MAT1R(0, 1) KET_MAT1R(0, 2)
+        KET_MAT1R(1, 0) KET_MAT1R(1, 1) KET_MAT1R(1, 2)
+        KET_MAT1R(2, 0) KET_MAT1R(2, 1) KET_MAT1R(2, 2)
+        KET_MAT1R(3, 0) KET_MAT1R(3, 1) KET_MAT1R(3, 2)
+#undef KET_MAT1R
+        case OC_MAT1L: case OC_MAT1L + 1: case OC_MAT1L + 2: {
+          const uint32_t members = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
+          const int bitv = (lane >> oa) & 1;
+          // own output = c0 * own + c1 * partner
+          const double2 e0 = __ldg(reinterpret_cast<const double2*>(M) + (bitv ? 3 : 0));
+          const double2 e1 = __ldg(reinterpret_cast<const double2*>(M) + (bitv ? 2 : 1));
+          const R c0r = (R)e0.x, c0i = (R)e0.y, c1r = (R)e1.x, c1i = (R)e1.y;
+          const int msk = 1 << oa;
+          if (opc == OC_MAT1L + 1) {
+#pragma unroll
+            for (int t = 0; t < TT; t++)
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+              cpx<R> p = shfl_xor_c<R>(x[t][j], msk, members);
+              cpx<R> y;
+              y.re = fma(c0r, x[t][j].re, c1r * p.re);
+              y.im = fma(c0r, x[t][j].im, c1r * p.im);
+              x[t][j] = smask == 0xffffu ? y : sel<R>((smask >> j) & 1, y, x[t][j]);
+            }
+          } else if (opc == OC_MAT1L + 2) {
+#pragma unroll
+            for (int t = 0; t < TT; t++)
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+              cpx<R> p = shfl_xor_c<R>(x[t][j], msk, members);
+              cpx<R> y;
+              y.re = fma(c0r, x[t][j].re, -c1i * p.im);
+              y.im = fma(c0r, x[t][j].im, c1i * p.re);
+              x[t][j] = smask == 0xffffu ? y : sel<R>((smask >> j) & 1, y, x[t][j]);
+            }
+          } else {
+#pragma unroll
+            for (int t = 0; t < TT; t++)
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+              cpx<R> p = shfl_xor_c<R>(x[t][j], msk, members);
+              cpx<R> y = mac2<R>(c0r, c0i, x[t][j], c1r, c1i, p);
+              x[t][j] = smask == 0xffffu ? y : sel<R>((smask >> j) & 1, y, x[t][j]);
+            }
+          }
+          break;
+        }
+        case OC_X1R + 0: for (int t = 0; t < TT; t++) x1_reg<R, 0>(x[t]); break;
+        case OC_X1R + 1: for (int t = 0; t < TT; t++) x1_reg<R, 1>(x[t]); break;
+        case OC_X1R + 2: for (int t = 0; t < TT; t++) x1_reg<R, 2>(x[t]); break;
+        case OC_X1R + 3: for (int t = 0; t < TT; t++) x1_reg<R, 3>(x[t]); break;
+#define KET_X1RC(A, C) \
+  case OC_X1RC + 4 * A + C: for (int t = 0; t < TT; t++) x1c_reg<R, A, C>(x[t]); break;
+        KET_X1RC(0, 1) KET_X1RC(0, 2) KET_X1RC(0, 3)
+        KET_X1RC(1, 0) KET_X1RC(1, 2) KET_X1RC(1, 3)
+        KET_X1RC(2, 0) KET_X1RC(2, 1) KET_X1RC(2, 3)
+        KET_X1RC(3, 0) KET_X1RC(3, 1) KET_X1RC(3, 2)
+#undef KET_X1RC
+        case OC_X1L: {
+          const uint32_t members = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
+          const int msk = 1 << oa;
+#pragma unroll
+          for (int t = 0; t < TT; t++)
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            cpx<R> p = shfl_xor_c<R>(x[t][j], msk, members);
+            x[t][j] = smask == 0xffffu ? p : sel<R>((smask >> j) & 1, p, x[t][j]);
+          }
+          break;
+        }
+#define KET_DIAGR(A, ONE)                                                         \
+  case (ONE ? OC_DIAGR1 : OC_DIAGR) + A: {                                        \
+    const double2 e0 = __ldg(reinterpret_cast<const double2*>(M));              \
+    const double2 e1 = __ldg(reinterpret_cast<const double2*>(M) + 1);          \
+    for (int t = 0; t < TT; t++) diag_reg<R, A, ONE>(x[t], (R)e0.x, (R)e0.y, (R)e1.x, (R)e1.y, smask);          \
+    break;                                                                        \
+  }
+        KET_DIAGR(0, false) KET_DIAGR(1, false) KET_DIAGR(2, false) KET_DIAGR(3, false)
+        KET_DIAGR(0, true) KET_DIAGR(1, true) KET_DIAGR(2, true) KET_DIAGR(3, true)
+#undef KET_DIAGR
+#define KET_DIAGR1C(A, C)                                                         \
+  case OC_DIAGR1C + 4 * A + C: {                                                  \
+    const double2 e1 = __ldg(reinterpret_cast<const double2*>(M) + 1);          \
+    for (int t = 0; t < TT; t++) diag1c_reg<R, A, C>(x[t], (R)e1.x, (R)e1.y);                                     \
+    break;                                                                        \
+  }
+        KET_DIAGR1C(0, 1) KET_DIAGR1C(0, 2) KET_DIAGR1C(0, 3)
+        KET_DIAGR1C(1, 0) KET_DIAGR1C(1, 2) KET_DIAGR1C(1, 3)
+        KET_DIAGR1C(2, 0) KET_DIAGR1C(2, 1) KET_DIAGR1C(2, 3)
+        KET_DIAGR1C(3, 0) KET_DIAGR1C(3, 1) KET_DIAGR1C(3, 2)
+#undef KET_DIAGR1C
+        case OC_DIAGT: case OC_DIAGX: {
+          bool one;
+          if (opc == OC_DIAGT) one = (tid >> oa) & 1;
+          else one = (ctx0 & __ldg(reinterpret_cast<const unsigned long long*>(op) + 4)) != 0;
+          if ((fl & FOF_D0ONE) && !one) break;
+          const double2 e = __ldg(reinterpret_cast<const double2*>(M) + (one ? 1 : 0));
+          for (int t = 0; t < TT; t++) phase_all<R>(x[t], (R)e.x, (R)e.y, smask);
+          break;
         }
         default: break;
       }
-      if (pr) prune16<R>(x, thr, qthr);  // mixing ops only (the planner clears the flag elsewhere)
+      if (fl & FOF_PRUNE)  // mixing ops only (the planner clears the flag elsewhere)
+#pragma unroll
+        for (int t = 0; t < TT; t++) prune16<R>(x[t], thr, qthr);
     }
     // the planner leaves the store layout in force here
     {
-      const GLayout gl = make_glayout(a, a.store_pos, lane, warp);
+      uint64_t gs = 0;
 #pragma unroll
-      for (int j = 0; j < 16; j++) st_amp<R>(amp + (ctxbase | gl.gthr | grofs(gl, j)), x[j]);
+      for (int r = 0; r < 5; r++)
+        if ((lane >> r) & 1) gs += a.sgb[r];
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+        if ((warp >> r) & 1) gs += a.sgb[5 + r];
+#pragma unroll
+      for (int t = 0; t < TT; t++) {
+        char* p = amp + (ctx0 | (t ? pairq : 0)) * sizeof(V) + gs;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          uint64_t o = 0;
+          if (j & 1) o += a.sgb[8];
+          if (j & 2) o += a.sgb[9];
+          if (j & 4) o += a.sgb[10];
+          if (j & 8) o += a.sgb[11];
+          st_amp<R>(reinterpret_cast<V*>(p + o), x[t][j]);
+        }
+      }
     }
   }
   if (GRAD) {
@@ -639,9 +719,24 @@ __global__ void k_grad_reduce(const double* gpart, int nctas, int nslots, double
   out[s] = acc;
 }
 
-template <typename R, bool GRAD>
-cudaError_t launch_t(const Pass2Args& a, cudaStream_t s) {
+template <typename R, bool GRAD, int TT>
+cudaError_t launch_tt(const Pass2Args& a, cudaStream_t s) {
   const int NT = 256;
+  static bool init = false;
+  if (!init) {
+    cudaFuncSetAttribute(k_fused2<R, NT, GRAD, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    init = true;
+  }
+  const size_t tb = sizeof(cpx<R>) << KET_T2_BITS;
+  const size_t smem = TT * tb + (GRAD ? sizeof(double) * 8 * (size_t)a.nslots : 0);
+  const uint64_t ngroups = (uint64_t(1) << (a.n - KET_T2_BITS)) / TT;
+  const unsigned blocks = (unsigned)std::min<uint64_t>(ngroups, (uint64_t)fused2_grid());
+  k_fused2<R, NT, GRAD, TT><<<blocks, NT, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename R, bool GRAD>
+cudaError_t launch_t(const Pass2Args& in, cudaStream_t s) {
   static bool init = false;
   if (!init) {
     uint16_t sm[16];
@@ -652,19 +747,36 @@ cudaError_t launch_t(const Pass2Args& a, cudaStream_t s) {
       sm[c] = v;
     }
     cudaMemcpyToSymbol(c_slotmask, sm, sizeof(sm));
-    cudaFuncSetAttribute(k_fused2<R, NT, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
     init = true;
   }
-  size_t smem = (sizeof(cpx<R>) << KET_T2_BITS) + (GRAD ? sizeof(double) * 8 * (size_t)a.nslots : 0);
-  uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
-  unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)fused2_grid());
-  k_fused2<R, NT, GRAD><<<blocks, NT, smem, s>>>(a);
-  return cudaGetLastError();
+  Pass2Args a = in;
+  // per-role byte offsets in the state and in the exchange buffer
+  auto gbit = [&](int tb) -> uint64_t {
+    const int q = tb < a.L ? tb : a.hbits[tb - a.L];
+    return (uint64_t(1) << q) * sizeof(typename Vec2<R>::T);
+  };
+  for (int r = 0; r < KET_T2_BITS; r++) {
+    a.lgb[r] = gbit(a.load_pos[r]);
+    a.sgb[r] = gbit(a.store_pos[r]);
+    a.lbx[r] = exch_offset(1u << a.load_pos[r], sizeof(R) == 4);
+  }
+  if constexpr (!GRAD) {
+    if (a.pairbit >= 0 && a.nctx > 0) return launch_tt<R, GRAD, 2>(a, s);
+  }
+  return launch_tt<R, GRAD, 1>(a, s);
 }
 
 }  // namespace
 
-int fused2_grid() { return num_sms() * 2; }
+int fused2_grid() { return num_sms() * KET_FUSED_CTAS_PER_SM; }
+
+int choose_pairbit(const std::vector<FOp>& prog, const Pass2Args& a) {
+  uint64_t used = 0;
+  for (const FOp& o : prog) used |= o.cctx | o.dg0 | o.dg1;
+  for (int j = 0; j < a.nctx; j++)
+    if (!((used >> a.ctxbits[j]) & 1)) return j;
+  return -1;
+}
 
 cudaError_t launch_fused2(const Pass2Args& a, int precision, cudaStream_t s) {
   if (a.nslots > 0) return precision == KET_C64 ? launch_t<float, true>(a, s) : launch_t<double, true>(a, s);

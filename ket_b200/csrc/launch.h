@@ -45,16 +45,15 @@ enum FOpType : uint8_t {
   FO_MAT1L = 2,   // 2x2 on lane bit a (warp shuffles)
   FO_X1R = 3,     // X on register bit a
   FO_X1L = 4,     // X on lane bit a
-  FO_SWAPS = 5,   // swap tile bits a, b (controls allowed) through shared memory
+  FO_SWAPS = 5,   // swap tile bits a, b (controls on tile bits: ctile) through shared memory
   FO_MAT2S = 6,   // 4x4 on tile bits a (MSB), b through shared memory
-  FO_RELABEL = 11,// no data movement: the layout's role -> tile-bit map changes (uncontrolled SWAP)
-  FO_DIAG = 7,    // diag phase on tile bits d0 (and d1), anywhere (general form)
+  FO_DIAG = 7,    // 4-entry diagonal on tile bits d0 (MSB), d1 (-1 = outside the tile), through shared memory
   FO_DIAGR = 8,   // diag(m0, m1) on register bit a
   FO_DIAGT = 9,   // diag(m0, m1) on thread-id bit a (lane 0-4 / warp 5-7): one phase per thread
   FO_DIAGX = 10,  // diag(m0, m1) on a qubit outside the tile (mask dg0): one phase per tile
-  FO_GRADM = 12,  // adjoint probe, D 2x2 on register bit a, ancilla register bit b, slot d1
+  FO_GRADM = 12,  // adjoint probe, D 2x2 on register bit a (ancilla on register bit 3)
   FO_GRADD = 13,  // adjoint probe, D = diag(m0, m1) on target a (register / thread / outside, see flags)
-  FO_GRADM2 = 14  // adjoint probe, D 4x4 on tile bits a (MSB), b through shared memory; ancilla tile bit d0
+  FO_GRADM2 = 14  // adjoint probe, D 4x4 on tile bits a (MSB), b through shared memory; ancilla tile bit anc
 };
 
 // flags
@@ -65,18 +64,65 @@ enum FOpType : uint8_t {
 #define FOF_TGT_THR 32u // FO_GRADD: target is a thread-id bit (a)
 #define FOF_TGT_CTX 64u // FO_GRADD: target is outside the tile (mask dg0)
 
+// Kernel op codes: one flat dispatch per op (the type, the target's register
+// bit, the matrix form and a register control are folded in by the host).
+enum FOpCode : uint8_t {
+  OC_EXCH = 0,
+  OC_MAT1R = 1,       // + 3 * A + form (form 0 general, 1 real, 2 Rx-like): 1..12
+  OC_MAT1L = 13,      // + form: 13..15
+  OC_X1R = 16,        // + A: 16..19 (no register control)
+  OC_X1RC = 20,       // + 4 * A + C: 20..35, X on register bit A controlled by register bit C only
+  OC_X1L = 36,
+  OC_DIAGR = 37,      // + A: 37..40 (general diag)
+  OC_DIAGR1 = 41,     // + A: 41..44 (m0 == 1)
+  OC_DIAGR1C = 45,    // + 4 * A + C: 45..60 (m0 == 1, controlled by register bit C only)
+  OC_DIAGT = 61,
+  OC_DIAGX = 62,
+  OC_DIAG = 63,
+  OC_SWAPS = 64,
+  OC_MAT2S = 65,
+  OC_GRADM = 66,      // + A: 66..68
+  OC_GRADD = 69,
+  OC_GRADM2 = 70,
+  OC_X1S = 71         // X on tile bit b with controls ctile, through shared memory (multi-controlled X)
+};
+
+// Roles in a layout: 0..4 lane bits, 5..7 warp bits, 8..11 register bits.
 struct FOp {
-  uint8_t type, a, b, flags;
-  uint8_t pos[KET_T2_BITS];   // FO_EXCH: new layout
-  uint32_t creg;              // controls on register bits (bit k = register bit k)
-  uint32_t cthr;              // controls on thread-id bits (lane bits 0-4, warp bits 5-7)
-  uint32_t ctile;             // FO_DIAG: controls inside the tile (tile-bit mask)
-  int16_t d0, d1;             // FO_DIAG: tile bit of t0 / t1, -1 = outside the tile, -2 = none
+  // bytes 0..15: everything the kernel needs to decide whether and how an op runs
+  uint8_t opc;                // FOpCode
+  uint8_t a;                  // target: register bit / lane bit / thread-id bit / tile bit (by type)
+  uint8_t flags;
+  uint8_t creg;               // controls on register bits (bit k = register bit k)
+  uint8_t cthr;               // controls on thread-id bits (lane bits 0-4, warp bits 5-7)
+  int8_t d0, d1;              // FO_DIAG: tile bits of t0 (MSB) and t1, -1 = outside the tile
+  uint8_t type;               // FOpType (host-side classification, used by the planner's tests)
   uint64_t cctx;              // controls on global bits outside the tile
-  uint64_t dg0, dg1;          // FO_DIAG*: global mask of t0 / t1 when outside the tile
-  uint64_t pad;               // header = 64 bytes
+  // bytes 16..31
+  uint32_t lmask;             // lanes whose lane-bit controls hold (shuffle member mask)
+  uint32_t ctile;             // shared-memory ops: controls as a tile-bit mask
+  int16_t slot, anc;          // adjoint probes: gradient slot; FO_GRADM2: ancilla tile bit
+  uint8_t b;                  // shared-memory ops: second tile bit
+  uint8_t pad0[3];
+  // bytes 32..63
+  uint64_t dg0, dg1;          // DIAGX / DIAG / GRADD: global mask of the target(s) outside the tile
+  uint8_t pos[KET_T2_BITS];   // FO_EXCH: new layout (role -> tile bit)
+  uint32_t pad1;
+  // FO_EXCH: m holds, as 12 uint16, the swizzled byte offset of each role's tile
+  // bit in the exchange buffer (see exch_offset); other ops: the matrix
   double m[32];
 };
+static_assert(sizeof(FOp) == 64 + 256, "FOp layout");
+
+// Fill in op.opc from op.type, op.a, op.flags and op.creg.
+void assign_opcode(FOp& op);
+
+// Byte offset of tile index i in the XOR-swizzled exchange buffer.  The map is
+// linear over GF(2), so the offset of a sum of disjoint bits is the XOR of
+// their offsets.
+__host__ __device__ inline uint32_t exch_offset(uint32_t i, bool c64) {
+  return c64 ? ((i ^ (((i >> 4) ^ (i >> 8)) & 15u)) << 3) : ((i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7u)) << 4);
+}
 
 struct Pass2Args {
   void* amp;
@@ -91,11 +137,20 @@ struct Pass2Args {
   int* status;                     // device status word: set to KET_ERR_TIMEOUT if a bounded wait ran out
   double* gpart;                   // adjoint: per-CTA gradient partials [cta][slot][warp]
   int nslots;                      // adjoint: gradient probes in this pass
+  int pairbit;                     // index into ctxbits of the qubit that tells apart the two tiles a
+                                   // thread holds, -1 = one tile per thread (see choose_pairbit)
+  // filled by launch_fused2 from the fields above:
+  uint64_t lgb[KET_T2_BITS];       // byte offset in the state of each role's tile bit, load layout
+  uint64_t sgb[KET_T2_BITS];       // same, store layout
+  uint32_t lbx[KET_T2_BITS];       // exchange-buffer offset of each role's tile bit, load layout
 };
 
 // Sum the adjoint partials of one pass: out[s] = sum over CTAs and warps (fixed order).
 cudaError_t launch_grad_reduce(const double* gpart, int nctas, int nslots, double* out, cudaStream_t s);
 int fused2_grid();
+// A qubit outside the tile (index into a.ctxbits) that no op of the program
+// reads as a control or a diagonal target, or -1.
+int choose_pairbit(const std::vector<FOp>& prog, const Pass2Args& a);
 
 // Lower one fused pass to a register-tiled program (segments + exchanges).
 void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, std::vector<FOp>& prog,

@@ -131,24 +131,39 @@ Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision)
   return l;
 }
 
-FOp make_exch(const Lay& l) {
+FOp make_exch(const Lay& l, int precision) {
   FOp o;
   memset(&o, 0, sizeof(o));
   o.type = FO_EXCH;
-  for (int i = 0; i < NB; i++) o.pos[i] = (uint8_t)l.pos[i];
+  uint16_t bx[NB];
+  for (int i = 0; i < NB; i++) {
+    o.pos[i] = (uint8_t)l.pos[i];
+    bx[i] = (uint16_t)exch_offset(1u << l.pos[i], precision == KET_C64);
+  }
+  memcpy(o.m, bx, sizeof(bx));
   return o;
 }
 
 // Split a control mask over the current layout.
 void controls(const Gate& g, const Pass& p, const Lay& l, FOp& o) {
+  o.lmask = 0xffffffffu;
   for (int q = 0; q < 64; q++) {
     if (!((g.cmask >> q) & 1)) continue;
     int t = tpos(p, q);
     if (t < 0) { o.cctx |= uint64_t(1) << q; continue; }
     o.ctile |= 1u << t;
     int r = l.role[t];
-    if (r >= 8) o.creg |= 1u << (r - 8);
-    else o.cthr |= 1u << r;  // lanes 0..4 -> tid bits 0..4, warps 5..7 -> tid bits 5..7
+    if (r >= 8) {
+      o.creg |= (uint8_t)(1u << (r - 8));
+    } else {
+      o.cthr |= (uint8_t)(1u << r);  // lanes 0..4 -> tid bits 0..4, warps 5..7 -> tid bits 5..7
+      if (r < 5) {
+        uint32_t lanes = 0;
+        for (int ln = 0; ln < 32; ln++)
+          if ((ln >> r) & 1) lanes |= 1u << ln;
+        o.lmask &= lanes;
+      }
+    }
   }
 }
 
@@ -164,6 +179,7 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
       bool reg = is_reg(l, t0);
       o.type = g.type == G_MAT1 ? (reg ? FO_MAT1R : FO_MAT1L) : (reg ? FO_X1R : FO_X1L);
       o.a = (uint8_t)(reg ? l.role[t0] - 8 : l.role[t0]);
+      o.b = (uint8_t)t0;  // tile bit (the shared-memory form of a multi-controlled X)
       bool real = true;
       for (int k = 0; k < 4; k++) {
         o.m[2 * k] = g.m[k].re;
@@ -209,7 +225,7 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
       o.flags = 0;
       o.a = (uint8_t)(l.role[t0] - 8);
       o.b = (uint8_t)(l.role[g_anc_tb] - 8);
-      o.d1 = (int16_t)g.slot;
+      o.slot = (int16_t)g.slot;
       for (int k = 0; k < 4; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
       break;
     }
@@ -217,7 +233,7 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
       o.type = FO_GRADD;
       o.flags = 0;
       o.b = (uint8_t)(l.role[g_anc_tb] - 8);
-      o.d1 = (int16_t)g.slot;
+      o.slot = (int16_t)g.slot;
       if (t0 < 0) { o.flags |= FOF_TGT_CTX; o.dg0 = uint64_t(1) << g.t0; }
       else if (is_reg(l, t0)) o.a = (uint8_t)(l.role[t0] - 8);
       else { o.flags |= FOF_TGT_THR; o.a = (uint8_t)l.role[t0]; }
@@ -229,21 +245,19 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
       o.flags = 0;
       o.a = (uint8_t)t0;
       o.b = (uint8_t)t1;
-      o.d0 = (int16_t)g_anc_tb;
-      o.d1 = (int16_t)g.slot;
+      o.anc = (int16_t)g_anc_tb;
+      o.slot = (int16_t)g.slot;
       for (int k = 0; k < 16; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
       break;
     }
     case G_DIAG2: {
       o.flags &= ~FOF_PRUNE;
       o.type = FO_DIAG;
-      o.d0 = (int16_t)(t0 >= 0 ? t0 : -1);
+      o.d0 = (int8_t)(t0 >= 0 ? t0 : -1);
       if (t0 < 0) o.dg0 = uint64_t(1) << g.t0;
-      o.d1 = (int16_t)(t1 >= 0 ? t1 : -1);
+      o.d1 = (int8_t)(t1 >= 0 ? t1 : -1);
       if (t1 < 0) o.dg1 = uint64_t(1) << g.t1;
       for (int k = 0; k < 4; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
-      o.creg = 0;
-      o.cthr = 0;
       break;
     }
     default: break;
@@ -252,6 +266,39 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
 }
 
 }  // namespace
+
+void assign_opcode(FOp& o) {
+  const bool real = o.flags & FOF_REAL, rx = o.flags & FOF_RXFORM, d0one = o.flags & FOF_D0ONE;
+  // a single control on a register bit (and none elsewhere) gets a compile-time variant
+  int c1 = -1;
+  if (o.creg && !(o.creg & (o.creg - 1)) && !o.cthr && !o.cctx)
+    for (int k = 0; k < 4; k++)
+      if (o.creg == (1u << k)) c1 = k;
+  switch (o.type) {
+    case FO_EXCH: o.opc = OC_EXCH; break;
+    case FO_MAT1R: o.opc = (uint8_t)(OC_MAT1R + 3 * o.a + (real ? 1 : rx ? 2 : 0)); break;
+    case FO_MAT1L: o.opc = (uint8_t)(OC_MAT1L + (real ? 1 : rx ? 2 : 0)); break;
+    case FO_X1R:
+      if (!o.creg) o.opc = (uint8_t)(OC_X1R + o.a);
+      else if (c1 >= 0) o.opc = (uint8_t)(OC_X1RC + 4 * o.a + c1);
+      else o.opc = OC_X1S;  // several controls, some on register bits: rare
+      break;
+    case FO_X1L: o.opc = OC_X1L; break;
+    case FO_DIAGR:
+      if (d0one) o.opc = c1 >= 0 ? (uint8_t)(OC_DIAGR1C + 4 * o.a + c1) : (uint8_t)(OC_DIAGR1 + o.a);
+      else o.opc = (uint8_t)(OC_DIAGR + o.a);
+      break;
+    case FO_DIAGT: o.opc = OC_DIAGT; break;
+    case FO_DIAGX: o.opc = OC_DIAGX; break;
+    case FO_DIAG: o.opc = OC_DIAG; break;
+    case FO_SWAPS: o.opc = OC_SWAPS; break;
+    case FO_MAT2S: o.opc = OC_MAT2S; break;
+    case FO_GRADM: o.opc = (uint8_t)(OC_GRADM + o.a); break;
+    case FO_GRADD: o.opc = OC_GRADD; break;
+    case FO_GRADM2: o.opc = OC_GRADM2; break;
+    default: o.opc = 0xff; break;
+  }
+}
 
 void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, std::vector<FOp>& prog,
                   uint8_t load_pos[KET_T2_BITS], uint8_t store_pos[KET_T2_BITS]) {
@@ -263,16 +310,17 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, st
     const Gate& g = plan.gates[p.gates[i]];
     if (!fits(g, p, cur)) {
       cur = choose(plan, p, i, false, precision);
-      prog.push_back(make_exch(cur));
+      prog.push_back(make_exch(cur, precision));
     }
     prog.push_back(make_op(g, p, cur, prune));
   }
   if (!a0_compatible(cur)) {
     Lay last = choose(plan, p, p.gates.size(), true, precision);
     cur = last;
-    prog.push_back(make_exch(cur));
+    prog.push_back(make_exch(cur, precision));
   }
   for (int i = 0; i < NB; i++) store_pos[i] = (uint8_t)cur.pos[i];
+  for (FOp& o : prog) assign_opcode(o);
 }
 
 }  // namespace ket

@@ -1,7 +1,7 @@
 // emulate_program.cpp -- TEST INFRASTRUCTURE: executes the fused-pass programs
 // that the engine's planner emits (ket_b200/csrc/planner.cpp, program.cpp) on
 // host arrays, following the semantics of the k_fused2 kernel op by op
-// (layouts, exchanges, relabels, register / lane / diagonal / shared-memory
+// (layouts, exchanges, register / lane / diagonal / shared-memory
 // ops, controls).  The tests compare it with direct gate-by-gate application,
 // so planner and program-generator bugs show up without a GPU.
 #include <complex>
@@ -85,14 +85,12 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
     for (int t = 0; t < 256; t++)
       for (int j = 0; j < 16; j++) x[t * 16 + j] = amp[gaddr(ctx, Lc.tbase[t] | rofs(Lc, j))];
     for (const FOp& op : prog) {
-      if (op.type == FO_EXCH || op.type == FO_RELABEL) {
-        if (op.type == FO_EXCH)
-          for (int t = 0; t < 256; t++)
-            for (int j = 0; j < 16; j++) sm[Lc.tbase[t] | rofs(Lc, j)] = x[t * 16 + j];
+      if (op.type == FO_EXCH) {
+        for (int t = 0; t < 256; t++)
+          for (int j = 0; j < 16; j++) sm[Lc.tbase[t] | rofs(Lc, j)] = x[t * 16 + j];
         Lc = make_lay(op.pos);
-        if (op.type == FO_EXCH)
-          for (int t = 0; t < 256; t++)
-            for (int j = 0; j < 16; j++) x[t * 16 + j] = sm[Lc.tbase[t] | rofs(Lc, j)];
+        for (int t = 0; t < 256; t++)
+          for (int j = 0; j < 16; j++) x[t * 16 + j] = sm[Lc.tbase[t] | rofs(Lc, j)];
         continue;
       }
       if ((ctx & op.cctx) != op.cctx) continue;
@@ -136,12 +134,13 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
             break;
           }
           case FO_DIAG: {
+            // d0, d1: tile bits, -1 = outside the tile; controls as a tile-bit mask
             for (int j = 0; j < 16; j++) {
               uint32_t idx = Lc.tbase[t] | rofs(Lc, j);
               if ((idx & op.ctile) != op.ctile) continue;
               int k0 = op.d0 >= 0 ? (int)((idx >> op.d0) & 1) : (int)((ctx & op.dg0) != 0);
               int k1 = op.d1 >= 0 ? (int)((idx >> op.d1) & 1) : (int)((ctx & op.dg1) != 0);
-              int kk = op.d1 != -2 ? 2 * k0 + k1 : k0;
+              int kk = 2 * k0 + k1;
               nt[j] = cx(op.m[2 * kk], op.m[2 * kk + 1]) * xt[j];
             }
             break;
