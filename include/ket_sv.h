@@ -184,6 +184,11 @@ KET_API int ket_marginals(const ket_state* st, double* out);
 KET_API int ket_marginals_noalloc(const void* amp, int nqubits, int precision, double* out, void* stream);
 /* Joint distribution of m qubits: out[j] = P(bit k of j = qubit qubits[k], for all k), 2^m bins (1 <= m <= 12). */
 KET_API int ket_marginal_dist(const ket_state* st, const int* qubits, int m, double* out);
+/* Compare two states of the same size (any precisions, same context):
+ * overlap = <a|b> (re, im) and max_abs_diff = max_i |a_i - b_i|, accumulated in
+ * FP64.  States the fidelity and amplitude error of a complex64 state against a
+ * complex128 one.  No counterpart in the reference. */
+KET_API int ket_state_compare(const ket_state* a, const ket_state* b, double* overlap_re_im, double* max_abs_diff);
 /* Sum of |a|^2 (FP64 accumulation). */
 KET_API int ket_norm2(const ket_state* st, double* out);
 /* run() pure fast path sampler (circuit.ts:3424-3453): r[s] are the caller's

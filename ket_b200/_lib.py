@@ -74,6 +74,7 @@ def lib():
             "ket_ctx_launch_count": (i32, [vp, P(u64)]),
             "ket_ctx_stream": (i32, [vp, P(vp)]),
             "ket_marginals_noalloc": (i32, [vp, i32, i32, vp, vp]),
+            "ket_state_compare": (i32, [vp, vp, P(dbl), P(dbl)]),
             "ket_ctx_io_bytes": (i32, [vp, P(u64), P(u64)]),
             "ket_state_alloc": (i32, [vp, i32, i32, P(vp)]),
             "ket_state_free": (i32, [vp]),

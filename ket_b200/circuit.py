@@ -734,6 +734,13 @@ class DeviceState:
         check(lib().ket_norm2(self.h, C.byref(out)))
         return out.value
 
+    def compare(self, other: "DeviceState"):
+        """(<self|other>, max_i |self_i - other_i|), accumulated in FP64 on the GPU."""
+        ov = (C.c_double * 2)()
+        mx = C.c_double()
+        check(lib().ket_state_compare(self.h, other.h, ov, C.byref(mx)))
+        return complex(ov[0], ov[1]), mx.value
+
     def sample(self, r: np.ndarray, thr: float = PRUNE) -> np.ndarray:
         r = np.ascontiguousarray(r, dtype=np.float64)
         out = np.empty(max(r.size, 1), dtype=np.uint64)

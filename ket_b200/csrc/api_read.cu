@@ -76,6 +76,25 @@ int ket_norm2(const ket_state* s, double* out) {
   return ctx_wait(s->ctx);
 }
 
+int ket_state_compare(const ket_state* a, const ket_state* b, double* overlap_re_im, double* max_abs_diff) {
+  TRY(check_state(a));
+  TRY(check_state(b));
+  if (!overlap_re_im && !max_abs_diff) return fail(KET_ERR_TYPE, "null argument");
+  if (a->n != b->n) return fail(KET_ERR_TYPE, "states of different sizes");
+  if (a->ctx != b->ctx) return fail(KET_ERR_TYPE, "states of different contexts");
+  void* scr;
+  TRY(ctx_scratch(a->ctx, compare_scratch(a->n) + 64, &scr));
+  double* res = (double*)scr;
+  TRY(LAUNCH_READ(a->ctx, launch_compare(a->amp, a->precision, b->amp, b->precision, a->n, res + 8, res,
+                                         a->ctx->stream)));
+  double h[3];
+  TRY(d2h(a->ctx, h, res, 24));
+  TRY(ctx_wait(a->ctx));
+  if (overlap_re_im) { overlap_re_im[0] = h[0]; overlap_re_im[1] = h[1]; }
+  if (max_abs_diff) *max_abs_diff = h[2];
+  return KET_OK;
+}
+
 int ket_probs_dense(const ket_state* s, double thr, double* out) {
   TRY(check_state(s));
   if (!out) return fail(KET_ERR_TYPE, "null argument");

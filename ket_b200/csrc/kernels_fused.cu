@@ -10,8 +10,8 @@
 // on any qubit, in or out of the tile.  The global load and store use a
 // layout whose lane bits are the tile's low bits, so every warp touches whole
 // 128-byte lines.  A pass costs one read and one write of the state however
-// many gates it holds; the persistent grid keeps two CTAs per SM so one CTA's
-// loads overlap the other's arithmetic.
+// many gates it holds.  The persistent grid runs one CTA per SM whose threads
+// each hold two tiles (every op decode then serves 32 amplitudes).
 //
 // The kernel is issue-bound, so the per-op overhead is kept small:
 //   * an op's first 16 bytes hold everything needed to skip or dispatch it,
@@ -401,6 +401,9 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
       const FOp* op = a.ops + k;
       const uint4 h = hn;
       if (k + 1 < a.nops) hn = __ldg(reinterpret_cast<const uint4*>(op + 1));
+      // the matrix is loaded before decoding, so its latency overlaps the dispatch
+      const double2* mp = reinterpret_cast<const double2*>(op->m);
+      const double2 q0 = __ldg(mp), q1 = __ldg(mp + 1), q2 = __ldg(mp + 2), q3 = __ldg(mp + 3);
       const int opc = h.x & 0xff, oa = (h.x >> 8) & 0xff;
       const uint32_t fl = (h.x >> 16) & 0xffu, creg = h.x >> 24, cthr = h.y & 0xffu;
       if (opc == OC_EXCH) {
@@ -568,8 +571,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
       switch (opc) {
 #define KET_MAT1R(A, F)                             \
   case OC_MAT1R + 3 * A + F: {                      \
-    R m[8];                                         \
-    load_m8<R>(op, m);                              \
+    const R m[8] = {(R)q0.x, (R)q0.y, (R)q1.x, (R)q1.y, (R)q2.x, (R)q2.y, (R)q3.x, (R)q3.y}; \
     for (int t = 0; t < TT; t++) mat1_reg<R, A, F>(x[t], m, smask);                 \
     break;                                          \
   }
@@ -582,8 +584,8 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
           const uint32_t members = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
           const int bitv = (lane >> oa) & 1;
           // own output = c0 * own + c1 * partner
-          const double2 e0 = __ldg(reinterpret_cast<const double2*>(M) + (bitv ? 3 : 0));
-          const double2 e1 = __ldg(reinterpret_cast<const double2*>(M) + (bitv ? 2 : 1));
+          const double2 e0 = bitv ? q3 : q0;
+          const double2 e1 = bitv ? q2 : q1;
           const R c0r = (R)e0.x, c0i = (R)e0.y, c1r = (R)e1.x, c1i = (R)e1.y;
           const int msk = 1 << oa;
           if (opc == OC_MAT1L + 1) {
@@ -645,8 +647,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
         }
 #define KET_DIAGR(A, ONE)                                                         \
   case (ONE ? OC_DIAGR1 : OC_DIAGR) + A: {                                        \
-    const double2 e0 = __ldg(reinterpret_cast<const double2*>(M));              \
-    const double2 e1 = __ldg(reinterpret_cast<const double2*>(M) + 1);          \
+    const double2 e0 = q0, e1 = q1;                                             \
     for (int t = 0; t < TT; t++) diag_reg<R, A, ONE>(x[t], (R)e0.x, (R)e0.y, (R)e1.x, (R)e1.y, smask);          \
     break;                                                                        \
   }
@@ -655,7 +656,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
 #undef KET_DIAGR
 #define KET_DIAGR1C(A, C)                                                         \
   case OC_DIAGR1C + 4 * A + C: {                                                  \
-    const double2 e1 = __ldg(reinterpret_cast<const double2*>(M) + 1);          \
+    const double2 e1 = q1;                                                      \
     for (int t = 0; t < TT; t++) diag1c_reg<R, A, C>(x[t], (R)e1.x, (R)e1.y);                                     \
     break;                                                                        \
   }
@@ -669,7 +670,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
           if (opc == OC_DIAGT) one = (tid >> oa) & 1;
           else one = (ctx0 & __ldg(reinterpret_cast<const unsigned long long*>(op) + 4)) != 0;
           if ((fl & FOF_D0ONE) && !one) break;
-          const double2 e = __ldg(reinterpret_cast<const double2*>(M) + (one ? 1 : 0));
+          const double2 e = one ? q1 : q0;
           for (int t = 0; t < TT; t++) phase_all<R>(x[t], (R)e.x, (R)e.y, smask);
           break;
         }

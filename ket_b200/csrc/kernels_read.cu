@@ -49,6 +49,52 @@ __global__ void k_sum_columns(const double* partial, uint64_t nblocks, int width
   out[j] = acc;
 }
 
+// ------------------------------------------------------------------ state comparison
+// Per block: sum of conj(a_i) b_i (re, im) and max |a_i - b_i|, all in FP64.
+template <typename RA, typename RB, int NT>
+__global__ void __launch_bounds__(NT) k_compare(const typename Vec2<RA>::T* a, const typename Vec2<RB>::T* b,
+                                                uint64_t N, uint64_t chunk, double* partial) {
+  __shared__ double red[32];
+  uint64_t lo = blockIdx.x * chunk, hi = min(N, lo + chunk);
+  double sr = 0.0, si = 0.0, mx = 0.0;
+  for (uint64_t i = lo + threadIdx.x; i < hi; i += NT) {
+    const typename Vec2<RA>::T u = a[i];
+    const typename Vec2<RB>::T v = b[i];
+    const double ur = u.x, ui = u.y, vr = v.x, vi = v.y;
+    sr += ur * vr + ui * vi;
+    si += ur * vi - ui * vr;
+    const double dr = ur - vr, di = ui - vi;
+    mx = fmax(mx, sqrt(dr * dr + di * di));
+  }
+  const double tr = block_sum<NT>(sr, red);
+  const double ti = block_sum<NT>(si, red);
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < NT / 32; w++) m = fmax(m, red[w]);
+    partial[3 * blockIdx.x] = tr;
+    partial[3 * blockIdx.x + 1] = ti;
+    partial[3 * blockIdx.x + 2] = m;
+  }
+}
+
+// Fixed-order combine of the block partials (one thread).
+__global__ void k_compare_combine(const double* partial, uint64_t nb, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double r = 0.0, i = 0.0, m = 0.0;
+  for (uint64_t b = 0; b < nb; b++) {
+    r += partial[3 * b];
+    i += partial[3 * b + 1];
+    m = fmax(m, partial[3 * b + 2]);
+  }
+  out[0] = r;
+  out[1] = i;
+  out[2] = m;
+}
+
 // ------------------------------------------------------------------ probabilities
 template <typename R>
 __global__ void k_probs_dense(const typename Vec2<R>::T* a, uint64_t off, uint64_t cnt, double thr, double* out) {
@@ -477,5 +523,24 @@ cudaError_t launch_pauli_group(const void* amp, int n, int prec, const PauliGrou
   return prec == KET_C64 ? pauli_t<float>(amp, n, g, partial, out, s) : pauli_t<double>(amp, n, g, partial, out, s);
 }
 size_t pauli_scratch(int n) { return 8 * 4096 + 64; }
+
+template <typename RA, typename RB>
+static cudaError_t compare_t(const void* a, const void* b, int n, double* scratch, double* out, cudaStream_t s) {
+  const uint64_t N = uint64_t(1) << n;
+  const uint64_t chunk = std::max<uint64_t>(N / 4096, 4096);
+  const uint64_t nb = (N + chunk - 1) / chunk;
+  k_compare<RA, RB, 256><<<(unsigned)nb, 256, 0, s>>>((const typename Vec2<RA>::T*)a,
+                                                      (const typename Vec2<RB>::T*)b, N, chunk, scratch);
+  k_compare_combine<<<1, 32, 0, s>>>(scratch, nb, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_compare(const void* a, int pa, const void* b, int pb, int n, double* scratch, double* out,
+                           cudaStream_t s) {
+  if (pa == KET_C64 && pb == KET_C64) return compare_t<float, float>(a, b, n, scratch, out, s);
+  if (pa == KET_C64) return compare_t<float, double>(a, b, n, scratch, out, s);
+  if (pb == KET_C64) return compare_t<double, float>(a, b, n, scratch, out, s);
+  return compare_t<double, double>(a, b, n, scratch, out, s);
+}
+size_t compare_scratch(int) { return 3 * 8 * 4096 + 64; }
 
 }  // namespace ket

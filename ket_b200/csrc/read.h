@@ -51,4 +51,9 @@ cudaError_t launch_pauli_group(const void* amp, int n, int prec, const PauliGrou
                                cudaStream_t s);
 size_t pauli_scratch(int n);
 
+// <a|b> (re, im) and max |a_i - b_i| of two states of the same size, any precisions.
+cudaError_t launch_compare(const void* a, int pa, const void* b, int pb, int n, double* scratch, double* out,
+                           cudaStream_t s);
+size_t compare_scratch(int n);
+
 }  // namespace ket

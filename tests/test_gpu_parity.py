@@ -202,6 +202,20 @@ def test_c64_state_close_to_c128():
     assert fid > 1 - 1e-9 and np.max(np.abs(a128 - a64)) < 1e-5
 
 
+def test_state_compare_matches_host():
+    """ket_state_compare: <a|b> and max |a - b| across precisions, against numpy."""
+    from ket_b200 import KET_C64, workloads as W
+    kc, _ = W.brickwork_circuit(15, 8, 7)
+    s128 = kc._state(None, precision=0)
+    s64 = kc._state(None, precision=KET_C64)
+    a128, a64 = s128.amplitudes_dense(), s64.amplitudes_dense()
+    ov, mx = s128.compare(s64)
+    assert abs(ov - np.vdot(a128, a64)) < 1e-12
+    assert abs(mx - np.max(np.abs(a128 - a64))) < 1e-15
+    ov2, mx2 = s128.compare(s128)
+    assert abs(ov2 - 1) < 1e-13 and mx2 == 0.0
+
+
 def test_invalid_ops_leave_state_untouched():
     import ket_b200 as K
     from ket_b200.circuit import DeviceState, ops_to_abi
