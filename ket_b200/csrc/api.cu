@@ -346,6 +346,7 @@ int ket_plan_stats(int n, int precision, const ket_op* ops, size_t nops, const d
   std::string err;
   int rc = lower_ops(n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
   if (rc) return fail(rc, err);
+  if (o.fusion != 0) fold_single_qubit(plan.gates, o.prune != 0);
   plan_passes(n, precision, o.fusion, o.prune != 0, plan);
   passes[0] = passes[1] = passes[2] = 0;
   for (auto& p : plan.passes) {
@@ -364,6 +365,7 @@ int ket_plan_program_stats(int n, int precision, const ket_op* ops, size_t nops,
   std::string err;
   int rc = lower_ops(n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
   if (rc) return fail(rc, err);
+  if (o.fusion != 0) fold_single_qubit(plan.gates, o.prune != 0);
   plan_passes(n, precision, o.fusion, o.prune != 0, plan);
   for (int i = 0; i < 16; i++) counts[i] = 0;
   for (auto& p : plan.passes) {
@@ -371,7 +373,8 @@ int ket_plan_program_stats(int n, int precision, const ket_op* ops, size_t nops,
     std::vector<FOp> prog;
     uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
     plan_program(plan, p, precision, o.prune != 0, prog, lp, sp);
-    for (auto& f : prog) counts[f.type]++;
+    for (const FOp& f : prog)
+      if (f.type != FO_CONT) counts[f.type]++;
     counts[14]++;
   }
   return KET_OK;
@@ -387,6 +390,7 @@ int ket_apply_ops(ket_state* s, const ket_op* ops, size_t nops, const double* ma
   std::string err;
   int rc = lower_ops(s->n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
   if (rc) return fail(rc, err);
+  if (o.fusion != 0) fold_single_qubit(plan.gates, o.prune != 0);
   if (plan.gates.empty()) return KET_OK;
   plan_passes(s->n, s->precision, o.fusion, o.prune != 0, plan);
   return run_plan(s, plan, o);

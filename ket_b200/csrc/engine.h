@@ -62,6 +62,9 @@ inline bool is_grad(const Gate& g) { return g.type == G_GRADM || g.type == G_GRA
 // Lower and validate an op list (mirrors #checkOp, circuit.ts:1113-1146).
 int lower_ops(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, bool prune,
               std::vector<Gate>& out, std::string& err);
+// Merge uncontrolled single-qubit gates on the same qubit where that is exact
+// (with pruning: only when one of the two preserves magnitudes).
+void fold_single_qubit(std::vector<Gate>& gates, bool prune);
 // Greedy fusion planner.
 void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& plan);
 

@@ -309,6 +309,47 @@ __device__ __forceinline__ uint64_t ctx_of(const Pass2Args& a, uint64_t tile) {
   return cb;
 }
 
+// ---------------------------------------------------------------- phase fans
+// FO_CPHASE on register bit A for the TT tiles of a thread; tile t's context is
+// ctx0 | (t ? pairq : 0).
+template <typename R, int A, int TT>
+__device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][16], const FOp* op, uint32_t nterms, uint64_t ctx0,
+                                          uint64_t pairq, int tid) {
+  double th0 = 0.0, thp = 0.0;
+  for (uint32_t i = 0; i < nterms; i++) {
+    const uint32_t r = i / KET_CPHASE_TERMS_PER_RECORD, w = i - r * KET_CPHASE_TERMS_PER_RECORD;
+    const double2 t = __ldg(reinterpret_cast<const double2*>(reinterpret_cast<const char*>(op + 1 + r) + 16) + w);
+    const uint64_t mk = (uint64_t)__double_as_longlong(t.y);
+    if (ctx0 & mk) th0 += t.x;
+    if (pairq & mk) thp += t.x;
+  }
+  const double2* mp = reinterpret_cast<const double2*>(op->m);
+  // thread factor: H[s] for every thread-id bit s that is set
+  double fr = 1.0, fi = 0.0;
+#pragma unroll
+  for (int sb = 0; sb < 8; sb++) {
+    const double2 h = __ldg(mp + 8 + sb);
+    const bool on = (tid >> sb) & 1;
+    const double hr = on ? h.x : 1.0, hi = on ? h.y : 0.0;
+    const double r = fr * hr - fi * hi;
+    fi = fr * hi + fi * hr;
+    fr = r;
+  }
+#pragma unroll
+  for (int t = 0; t < TT; t++) {
+    double sn, cs;
+    sincos(th0 + (t ? thp : 0.0), &sn, &cs);
+    const double gr = cs * fr - sn * fi, gi = cs * fi + sn * fr;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int j = ((k >> A) << (A + 1)) | (1 << A) | (k & ((1 << A) - 1));
+      const double2 tk = __ldg(mp + k);
+      const R pr = (R)(tk.x * gr - tk.y * gi), pi = (R)(tk.x * gi + tk.y * gr);
+      cmul_in<R>(x[t][j], pr, pi);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- adjoint probes
 // Register bit 3 selects psi (0) / lambda (1).
 // Re<lambda| D |psi> with D 2x2 on register bit A.
@@ -531,8 +572,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
         continue;  // pruning already done
       }
       const bool thr_ok = ((uint32_t)tid & cthr) == cthr;
-      if (opc >= OC_GRADM) {
-        if (!GRAD) continue;
+      if (GRAD && opc >= OC_GRADM) {  // adjoint passes hold no phase fans (the host merges none there)
         // <lambda|D|psi> over this thread's amplitudes: register bit 3 of the
         // slot index selects psi (0) or lambda (1) -- the planner pins the
         // ancilla there.  Every lane takes part in the warp sum.  (TT == 1)
@@ -665,6 +705,14 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
         KET_DIAGR1C(2, 0) KET_DIAGR1C(2, 1) KET_DIAGR1C(2, 3)
         KET_DIAGR1C(3, 0) KET_DIAGR1C(3, 1) KET_DIAGR1C(3, 2)
 #undef KET_DIAGR1C
+#define KET_CPHASE(A)                                                                         \
+  case OC_CPHASE + A: {                                                                       \
+    const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);                          \
+    phase_fan<R, A, TT>(x, op, h2.x, ctx0, pairq, tid);                                       \
+    break; /* the continuation records that follow run as no-ops */                          \
+  }
+        KET_CPHASE(0) KET_CPHASE(1) KET_CPHASE(2) KET_CPHASE(3)
+#undef KET_CPHASE
         case OC_DIAGT: case OC_DIAGX: {
           bool one;
           if (opc == OC_DIAGT) one = (tid >> oa) & 1;
@@ -772,8 +820,9 @@ cudaError_t launch_t(const Pass2Args& in, cudaStream_t s) {
 int fused2_grid() { return num_sms() * KET_FUSED_CTAS_PER_SM; }
 
 int choose_pairbit(const std::vector<FOp>& prog, const Pass2Args& a) {
-  uint64_t used = 0;
-  for (const FOp& o : prog) used |= o.cctx | o.dg0 | o.dg1;
+  uint64_t used = 0;  // (a phase fan's out-of-tile terms are evaluated per tile: not counted)
+  for (const FOp& o : prog)
+    if (o.type != FO_CONT) used |= o.cctx | o.dg0 | o.dg1;
   for (int j = 0; j < a.nctx; j++)
     if (!((used >> a.ctxbits[j]) & 1)) return j;
   return -1;

@@ -51,9 +51,11 @@ enum FOpType : uint8_t {
   FO_DIAGR = 8,   // diag(m0, m1) on register bit a
   FO_DIAGT = 9,   // diag(m0, m1) on thread-id bit a (lane 0-4 / warp 5-7): one phase per thread
   FO_DIAGX = 10,  // diag(m0, m1) on a qubit outside the tile (mask dg0): one phase per tile
+  FO_CPHASE = 11, // fan of phases on register bit a (see below), followed by continuation records
   FO_GRADM = 12,  // adjoint probe, D 2x2 on register bit a (ancilla on register bit 3)
   FO_GRADD = 13,  // adjoint probe, D = diag(m0, m1) on target a (register / thread / outside, see flags)
-  FO_GRADM2 = 14  // adjoint probe, D 4x4 on tile bits a (MSB), b through shared memory; ancilla tile bit anc
+  FO_GRADM2 = 14, // adjoint probe, D 4x4 on tile bits a (MSB), b through shared memory; ancilla tile bit anc
+  FO_CONT = 15    // continuation record of the op before it (data only, never dispatched)
 };
 
 // flags
@@ -84,7 +86,24 @@ enum FOpCode : uint8_t {
   OC_GRADM = 66,      // + A: 66..68
   OC_GRADD = 69,
   OC_GRADM2 = 70,
-  OC_X1S = 71         // X on tile bit b with controls ctile, through shared memory (multi-controlled X)
+  OC_X1S = 71,        // X on tile bit b with controls ctile, through shared memory (multi-controlled X)
+  OC_CPHASE = 72,     // + A: 72..75, phase fan on register bit A
+  OC_NOP = 0xFF       // continuation record: dispatched as an op that does nothing
+};
+
+// FO_CPHASE: a run of phase gates diag(1, e^{i phi}) on one target (register
+// bit A), each with at most one control, merged into one op.  Every amplitude
+// whose bit A is 1 is multiplied by
+//   T[k] * prod_{thread-id bits s set} H[s] * exp(i * sum_{terms: ctx & mask} angle)
+// where k is the slot index with bit A removed.  m[0..15] hold T[0..7]
+// (constant and register-bit controls), m[16..31] hold H[0..7] (lane bits
+// 0-4, warp bits 5-7).  The out-of-tile controls are (angle, global qubit
+// mask) pairs stored as double2 in the continuation records (FO_CONT) that
+// follow the op: each record has a 16-byte header that makes it a no-op
+// (OC_NOP, no controls) and 19 pairs after it; the op's `lmask` field holds the
+// number of pairs and `ctile` the number of records.
+enum : int {
+  KET_CPHASE_TERMS_PER_RECORD = 19
 };
 
 // Roles in a layout: 0..4 lane bits, 5..7 warp bits, 8..11 register bits.

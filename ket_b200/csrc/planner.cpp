@@ -217,6 +217,114 @@ int lower_ops(int n, const ket_op* ops, size_t nops, const double* mats, size_t 
   return KET_OK;
 }
 
+namespace {
+
+void mat_of(const Gate& g, cd m[4]) {
+  if (g.type == G_MAT1) {
+    for (int k = 0; k < 4; k++) m[k] = g.m[k];
+  } else if (g.type == G_DIAG1) {
+    m[0] = g.m[0]; m[1] = cd{0, 0}; m[2] = cd{0, 0}; m[3] = g.m[1];
+  } else {  // G_X1
+    m[0] = cd{0, 0}; m[1] = cd{1, 0}; m[2] = cd{1, 0}; m[3] = cd{0, 0};
+  }
+}
+
+cd cmulh(cd a, cd b) { return cd{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+cd caddh(cd a, cd b) { return cd{a.re + b.re, a.im + b.im}; }
+
+// Classify a 2x2 as identity (returns false), diagonal, X or general.
+bool set_single(Gate& g, const cd m[4], bool prune) {
+  if (is0(m[1]) && is0(m[2])) {
+    if (is1(m[0]) && is1(m[3])) return false;
+    g.type = G_DIAG1; g.m[0] = m[0]; g.m[1] = m[3]; g.prune = prune;
+  } else if (is0(m[0]) && is0(m[3]) && is1(m[1]) && is1(m[2])) {
+    g.type = G_X1; g.prune = false;
+  } else {
+    g.type = G_MAT1; g.prune = prune;
+    for (int k = 0; k < 4; k++) g.m[k] = m[k];
+  }
+  return true;
+}
+
+}  // namespace
+
+// Folding of uncontrolled single-qubit gates.  A gate G on qubit q merges with
+// the previous uncontrolled single-qubit gate P on q into the one gate G*P when
+// the gate that has to move to the other's position commutes with everything
+// on q in between: a diagonal commutes with gates that use q only as a control
+// and with other diagonals on q; an X or a general 2x2 needs q untouched.
+// With the reference's pruning two magnitude-changing gates never merge (the
+// reference prunes between them); a diagonal or an X preserves magnitudes, so
+// merging it is exact.  The merged gate takes the position of the gate that
+// can change magnitudes, so the order of those gates is unchanged.
+void fold_single_qubit(std::vector<Gate>& gs, bool prune) {
+  const size_t ng = gs.size();
+  std::vector<int> cand(64, -1);
+  std::vector<char> tmix(64, 0), tany(64, 0), dead(ng, 0);
+  for (size_t i = 0; i < ng; i++) {
+    Gate& g = gs[i];
+    const bool single = (g.type == G_MAT1 || g.type == G_DIAG1 || g.type == G_X1) && g.cmask == 0;
+    if (!single) {
+      uint64_t tgt = 0, all = g.cmask;
+      switch (g.type) {
+        case G_MAT1: case G_X1: tgt = bit(g.t0); break;
+        case G_SWAP: case G_MAT2: tgt = bit(g.t0) | bit(g.t1); break;
+        case G_MATK: for (int q : g.tk) tgt |= bit(q); break;
+        case G_DIAG1: all |= bit(g.t0); break;
+        case G_DIAG2: all |= bit(g.t0) | bit(g.t1); break;
+        default: break;
+      }
+      all |= tgt;
+      for (int q = 0; q < 64; q++) {
+        if ((all >> q) & 1) tany[q] = 1;
+        if ((tgt >> q) & 1) tmix[q] = 1;
+      }
+      continue;
+    }
+    const int q = g.t0, p = cand[q];
+    if (p >= 0) {
+      Gate& P = gs[p];
+      const bool pd = P.type == G_DIAG1, gd = g.type == G_DIAG1;
+      const bool pm = P.type == G_MAT1, gm = g.type == G_MAT1;
+      bool ok = (pd || gd) ? !tmix[q] : !tany[q];
+      if (prune && pm && gm) ok = false;
+      if (ok) {
+        cd a[4], b[4], m[4];
+        mat_of(g, a);
+        mat_of(P, b);
+        for (int r = 0; r < 2; r++)
+          for (int c = 0; c < 2; c++) m[2 * r + c] = caddh(cmulh(a[2 * r], b[c]), cmulh(a[2 * r + 1], b[2 + c]));
+        // the merged gate goes where the magnitude-changing gate was; between
+        // two magnitude-preserving gates, where the moving diagonal allows
+        const size_t pos = pm ? (size_t)p : (gm ? i : (pd ? i : (size_t)p));
+        const size_t other = pos == i ? (size_t)p : i;
+        Gate merged = gs[pos];
+        const bool keep = set_single(merged, m, prune);
+        dead[other] = 1;
+        if (!keep) {
+          dead[pos] = 1;
+          cand[q] = -1;
+        } else {
+          gs[pos] = merged;
+          cand[q] = (int)pos;
+          if (pos == i) { tmix[q] = 0; tany[q] = 0; }
+        }
+        continue;
+      }
+    }
+    cand[q] = (int)i;
+    tmix[q] = 0;
+    tany[q] = 0;
+  }
+  size_t w = 0;
+  for (size_t i = 0; i < ng; i++)
+    if (!dead[i]) {
+      if (w != i) gs[w] = std::move(gs[i]);
+      w++;
+    }
+  gs.resize(w);
+}
+
 int tile_qubits(int precision, int fusion) {
   int mx = 12;
   if (fusion > 0) return std::max(6, std::min(fusion, mx));

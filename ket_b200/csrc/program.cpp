@@ -9,6 +9,7 @@
 // layouts keep lane bit l on tile bit l (l < 5) so the global load and store
 // of each warp touch contiguous 128-byte lines.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "launch.h"
@@ -267,6 +268,86 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
 
 }  // namespace
 
+namespace {
+
+int popc(uint64_t v) { return __builtin_popcountll(v); }
+
+bool fan_member(const FOp& o) {
+  return o.type == FO_DIAGR && (o.flags & FOF_D0ONE) && popc(o.creg) + popc(o.cthr) + popc(o.cctx) <= 1;
+}
+
+// Merge runs of phase gates on the same register bit into FO_CPHASE ops.
+void merge_phase_fans(std::vector<FOp>& prog) {
+  std::vector<FOp> out;
+  out.reserve(prog.size());
+  size_t i = 0;
+  while (i < prog.size()) {
+    size_t j = i;
+    while (j < prog.size() && fan_member(prog[j]) && prog[j].a == prog[i].a) j++;
+    if (!fan_member(prog[i]) || j - i < 2) {
+      out.push_back(prog[i]);
+      i++;
+      continue;
+    }
+    const int A = prog[i].a;
+    cd T[8], H[8];
+    for (int k = 0; k < 8; k++) { T[k] = cd{1, 0}; H[k] = cd{1, 0}; }
+    std::vector<std::pair<uint64_t, double>> terms;  // (mask, angle)
+    auto mul = [](cd a, cd b) { return cd{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; };
+    for (size_t g = i; g < j; g++) {
+      const FOp& o = prog[g];
+      const cd ph{o.m[2], o.m[3]};
+      if (o.cctx) {
+        const double ang = std::atan2(ph.im, ph.re);
+        bool found = false;
+        for (auto& t : terms)
+          if (t.first == o.cctx) { t.second += ang; found = true; }
+        if (!found) terms.push_back({o.cctx, ang});
+      } else if (o.cthr) {
+        for (int sb = 0; sb < 8; sb++)
+          if (o.cthr == (1u << sb)) H[sb] = mul(H[sb], ph);
+      } else {
+        for (int k = 0; k < 8; k++) {
+          const int slot = ((k >> A) << (A + 1)) | (1 << A) | (k & ((1 << A) - 1));
+          if ((slot & o.creg) == o.creg) T[k] = mul(T[k], ph);
+        }
+      }
+    }
+    FOp f;
+    memset(&f, 0, sizeof(f));
+    f.type = FO_CPHASE;
+    f.a = (uint8_t)A;
+    f.d0 = f.d1 = -2;
+    for (int k = 0; k < 8; k++) {
+      f.m[2 * k] = T[k].re; f.m[2 * k + 1] = T[k].im;
+      f.m[16 + 2 * k] = H[k].re; f.m[16 + 2 * k + 1] = H[k].im;
+    }
+    const size_t nrec = (terms.size() + KET_CPHASE_TERMS_PER_RECORD - 1) / KET_CPHASE_TERMS_PER_RECORD;
+    f.lmask = (uint32_t)terms.size();
+    f.ctile = (uint32_t)nrec;
+    out.push_back(f);
+    for (size_t r = 0; r < nrec; r++) {
+      FOp c;
+      memset(&c, 0, sizeof(c));
+      c.opc = OC_NOP;
+      c.type = FO_CONT;
+      c.d0 = c.d1 = -2;
+      double* d = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(&c) + 16);
+      for (size_t t = 0; t < KET_CPHASE_TERMS_PER_RECORD; t++) {
+        const size_t ti = r * KET_CPHASE_TERMS_PER_RECORD + t;
+        if (ti >= terms.size()) break;
+        d[2 * t] = terms[ti].second;
+        memcpy(&d[2 * t + 1], &terms[ti].first, 8);
+      }
+      out.push_back(c);
+    }
+    i = j;
+  }
+  prog.swap(out);
+}
+
+}  // namespace
+
 void assign_opcode(FOp& o) {
   const bool real = o.flags & FOF_REAL, rx = o.flags & FOF_RXFORM, d0one = o.flags & FOF_D0ONE;
   // a single control on a register bit (and none elsewhere) gets a compile-time variant
@@ -296,6 +377,8 @@ void assign_opcode(FOp& o) {
     case FO_GRADM: o.opc = (uint8_t)(OC_GRADM + o.a); break;
     case FO_GRADD: o.opc = OC_GRADD; break;
     case FO_GRADM2: o.opc = OC_GRADM2; break;
+    case FO_CPHASE: o.opc = (uint8_t)(OC_CPHASE + o.a); break;
+    case FO_CONT: o.opc = OC_NOP; break;
     default: o.opc = 0xff; break;
   }
 }
@@ -320,6 +403,7 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, st
     prog.push_back(make_exch(cur, precision));
   }
   for (int i = 0; i < NB; i++) store_pos[i] = (uint8_t)cur.pos[i];
+  if (g_anc_tb < 0) merge_phase_fans(prog);
   for (FOp& o : prog) assign_opcode(o);
 }
 

@@ -84,7 +84,32 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
     Lay Lc = make_lay(lp);
     for (int t = 0; t < 256; t++)
       for (int j = 0; j < 16; j++) x[t * 16 + j] = amp[gaddr(ctx, Lc.tbase[t] | rofs(Lc, j))];
-    for (const FOp& op : prog) {
+    for (size_t oi = 0; oi < prog.size(); oi++) {
+      const FOp& op = prog[oi];
+      if (op.type == FO_CPHASE) {
+        // phase fan on register bit a: T[k] * prod H[thread bits] * exp(i sum ctx angles)
+        double th = 0.0;
+        for (uint32_t t = 0; t < op.lmask; t++) {
+          const size_t rec = t / KET_CPHASE_TERMS_PER_RECORD, w = t % KET_CPHASE_TERMS_PER_RECORD;
+          const double* rd = reinterpret_cast<const double*>(reinterpret_cast<const unsigned char*>(&prog[oi + 1 + rec]) + 16);
+          uint64_t mk;
+          memcpy(&mk, &rd[2 * w + 1], 8);
+          if (ctx & mk) th += rd[2 * w];
+        }
+        const cx E = std::polar(1.0, th);
+        for (int t = 0; t < 256; t++) {
+          cx F = E;
+          for (int sb = 0; sb < 8; sb++)
+            if ((t >> sb) & 1) F *= cx(op.m[16 + 2 * sb], op.m[17 + 2 * sb]);
+          for (int j = 0; j < 16; j++) {
+            if (!((j >> op.a) & 1)) continue;
+            const int k = ((j >> (op.a + 1)) << op.a) | (j & ((1 << op.a) - 1));
+            x[t * 16 + j] *= cx(op.m[2 * k], op.m[2 * k + 1]) * F;
+          }
+        }
+        oi += op.ctile;
+        continue;
+      }
       if (op.type == FO_EXCH) {
         for (int t = 0; t < 256; t++)
           for (int j = 0; j < 16; j++) sm[Lc.tbase[t] | rofs(Lc, j)] = x[t * 16 + j];
@@ -196,6 +221,7 @@ int emu_apply(int n, const ket_op* ops, size_t nops, const double* mats, size_t 
   std::string err;
   int rc = lower_ops(n, ops, nops, mats, nmat, prune != 0, plan.gates, err);
   if (rc) return rc;
+  if (fusion != 0) fold_single_qubit(plan.gates, prune != 0);
   plan_passes(n, KET_C128, fusion, prune != 0, plan);
   cx* amp = reinterpret_cast<cx*>(re_im);
   passes[0] = passes[1] = 0;

@@ -186,7 +186,8 @@ def test_planner_statistics():
     fused = plan(c)
     unf = plan(c, fusion=0)
     assert unf[0] == 0 and unf[1] == unf[2]
-    assert fused[2] == unf[2]
+    # folding merges diagonals into neighbouring single-qubit gates on the same qubit
+    assert unf[2] * 0.6 < fused[2] <= unf[2]
     assert fused[0] < unf[1] / 5, fused
     # validation runs in the planner without a GPU
     bad = K.Circuit(2).h(0)
