@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--layers", type=int, default=40)
     ap.add_argument("--prune", type=int, default=1, help="1: reference pruning semantics (default), 0: plain dense")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the VQE-gradient, QAOA-batch and complex64 measurements")
     return ap.parse_args()
 
 
@@ -65,19 +67,25 @@ def dist_env():
 
 
 class Dist:
-    """torch.distributed plumbing for replicas: barrier and max over ranks."""
+    """torch.distributed plumbing for replicas: barrier and max over ranks.
+    backend "nccl" (one GPU per rank) or "gloo" (host tensors, used by the CPU
+    tests of this plumbing)."""
 
-    def __init__(self, world, rank, local):
+    def __init__(self, world, rank, local, backend="nccl", timeout_s=600):
         self.world, self.rank, self.local = world, rank, local
         self.pg = None
+        self.device = "cpu"
         if world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", local))
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+                kw["device_id"] = torch.device("cuda", local)
+                self.device = "cuda"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
             self.dist = dist
             self.torch = torch
             self.pg = True
@@ -89,7 +97,7 @@ class Dist:
     def max(self, v):
         if not self.pg:
             return v
-        t = self.torch.tensor([float(v)], device="cuda")
+        t = self.torch.tensor([float(v)], device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -357,10 +365,78 @@ def run_ket(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, _ = cpu_rate(1)
         line["cpu_baseline"] = {"value": v, "unit": "gates/s", "cores": 1, "kind": "port", "sample": sample_desc(1)}
+    if world == 1 and not args.no_extras and n == 30:
+        del st
+        line.update(extras())
     dist.close()
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+# ---------------------------------------------------------------- other workloads of the metric
+def extras():
+    """The other measurements the headline metric names, each on its own
+    synthetic workload (device-timed where it is one launch sequence, wall
+    clock through the public API otherwise):
+      vqe24      adjoint gradients of the 24-qubit TFIM VQE (8 layers of Ry, Rz
+                 and a CNOT ladder, 384 parameters), 64 parameter vectors, against
+                 the reference's parameter-shift rule run on the same engine
+      qaoa_batch 4096 QAOA MaxCut instances (3-regular graphs, n in 10..22 even,
+                 p = 4) in one persistent launch
+      precision  complex64 state against complex128 at 31 qubits (brickwork, 30
+                 layers) and the complex64 33-qubit run of the same family"""
+    import numpy as np
+
+    from ket_b200 import KET_C64, workloads as W
+    from ket_b200.adjoint import adjoint_gradient, shift_gradient
+    from ket_b200.batch import batch_qaoa
+    from ket_b200.circuit import DeviceState, flatten_ops, ops_to_abi
+    out = {}
+    ans, H, P = W.tfim_vqe(24, 8, 64)
+    P = np.array(P)
+    adjoint_gradient(ans, H, P[:2])
+    t = time.perf_counter()
+    e, g = adjoint_gradient(ans, H, P)
+    ta = time.perf_counter() - t
+    t = time.perf_counter()
+    e2, g2 = shift_gradient(ans, H, P[:1])
+    ts = time.perf_counter() - t
+    out["vqe24"] = {"adjoint_grads_per_s": len(P) / ta, "shift_grads_per_s": 1.0 / ts,
+                    "speedup": ts / (ta / len(P)), "max_abs_grad_diff": float(np.max(np.abs(g2[0] - g[0]))),
+                    "params": int(P.shape[1]), "batch": int(P.shape[0]), "unit": "gradients/s (wall clock)"}
+    inst = W.qaoa_batch(4096, 4, 42)
+    batch_qaoa(inst[:64])
+    batch_qaoa(inst)
+    t = time.perf_counter()
+    res = batch_qaoa(inst)
+    tq = time.perf_counter() - t
+    out["qaoa_batch"] = {"instances": 4096, "seconds": tq, "instances_per_s": 4096 / tq,
+                         "mean_expected_cut": float(np.mean(res)), "unit": "instances/s (wall clock)"}
+    c31, _ = W.brickwork_circuit(31, 30, 42)
+    arr, m, k = ops_to_abi(flatten_ops(c31.ops))
+    a = DeviceState(31)
+    a.set_basis(0)
+    a.apply_abi(arr, m, k)
+    b = DeviceState(31, KET_C64)
+    b.set_basis(0)
+    b.apply_abi(arr, m, k)
+    ov, mx = a.compare(b)
+    na, nb = a.norm2(), b.norm2()
+    del a, b
+    c33, _ = W.brickwork_circuit(33, 30, 42)
+    arr, m, k = ops_to_abi(flatten_ops(c33.ops))
+    s33 = DeviceState(33, KET_C64)
+    s33.set_basis(0)
+    t = time.perf_counter()
+    s33.apply_abi(arr, m, k)
+    t33 = time.perf_counter() - t
+    n33 = s33.norm2()
+    del s33
+    out["precision"] = {"fidelity_31q": abs(ov) ** 2 / (na * nb), "max_abs_amp_err_31q": mx,
+                        "norm_c128_31q": na, "norm_c64_31q": nb, "c64_33q_seconds": t33,
+                        "c64_33q_gates_per_s": k / t33, "c64_33q_norm": n33}
+    return out
 
 
 def main():
