@@ -121,6 +121,12 @@ KET_API int ket_ctx_io_bytes(const ket_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
  * on (0 = the next one) fails with KET_ERR_OOM; a negative value disables it.
  * No counterpart in the reference (which has no allocator). */
 KET_API int ket_debug_fail_alloc(int after);
+/* Test hook for the bounded waits of ket_batch_qaoa: drop_item >= 0 removes that
+ * work item from the queue (tiles that depend on it then wait in vain) and
+ * spin_limit sets how many polls a wait makes before it gives up and the call
+ * returns KET_ERR_TIMEOUT (0 = the default, 2^24); drop_item = -1 disables.
+ * No counterpart in the reference (which has no device waits). */
+KET_API int ket_debug_batch_hook(int drop_item, uint32_t spin_limit);
 
 /* Dense state of 2^nqubits amplitudes, resident in device memory, set to |0..0>
  * (zero(n), statevector.ts:16).  precision: KET_C128 or KET_C64. */

@@ -29,7 +29,12 @@ class RangeError(ValueError):
 
 
 class KetError(RuntimeError):
-    """An engine failure with no reference counterpart (device, memory, timeout)."""
+    """An engine failure with no reference counterpart (device, memory, timeout);
+    `code` is the ket_status value."""
+
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
 
 
 class ket_op(C.Structure):
@@ -66,6 +71,7 @@ def lib():
             "ket_abi_version": (i32, []),
             "ket_exec_opts_default": (None, [P(ket_exec_opts)]),
             "ket_debug_fail_alloc": (i32, [i32]),
+            "ket_debug_batch_hook": (i32, [i32, C.c_uint32]),
             "ket_ctx_create": (i32, [i32, P(vp)]),
             "ket_ctx_destroy": (i32, [vp]),
             "ket_ctx_scratch_bytes": (i32, [vp, P(u64)]),
@@ -119,7 +125,7 @@ def check(rc: int):
         raise RangeError(msg)
     if rc == KET_ERR_TYPE:
         raise TypeError(msg)
-    raise KetError(f"ket engine error {rc}: {msg}")
+    raise KetError(f"ket engine error {rc}: {msg}", rc)
 
 
 _ctx = None

@@ -61,6 +61,7 @@ struct QArgs {
   unsigned int* next;       // queue head
   unsigned int* done;       // per instance: tiles finished (pass-major)
   int* status;
+  uint32_t spin_limit;      // polls before a wait gives up (status KET_ERR_TIMEOUT)
   int nitems;
   int tile;                 // tile qubits
 };
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
         volatile unsigned int* d = a.done + w.inst;
         uint32_t spins = 0;
         while (*d < need) {
-          if (++spins > (1u << 24)) { atomicExch(a.status, (int)KET_ERR_TIMEOUT); break; }
+          if (++spins > a.spin_limit) { atomicExch(a.status, (int)KET_ERR_TIMEOUT); break; }
           __nanosleep(200);
         }
         __threadfence();
@@ -232,10 +233,21 @@ __global__ void k_qaoa_reduce(const QInst* inst, int ninst, const double* part, 
   out[i] = acc;
 }
 
+// Test hook (ket_debug_batch_hook): drop one work item from the queue and
+// shorten the waits, so that the tiles depending on it time out.
+int g_drop_item = -1;
+uint32_t g_spin_limit = 1u << 24;
+
 }  // namespace
 }  // namespace ket
 
 using namespace ket;
+
+extern "C" int ket_debug_batch_hook(int drop_item, uint32_t spin_limit) {
+  g_drop_item = drop_item;
+  g_spin_limit = spin_limit ? spin_limit : (1u << 24);
+  return KET_OK;
+}
 
 extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne, const int64_t* eoff,
                               const int* edges, int p, const double* gamma, const double* beta, int use_graph,
@@ -286,6 +298,7 @@ extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne
     }
   for (int i : order)
     if (!(inst[i].n > T && p > 0)) items.push_back(QItem{i, -1, 0});
+  if (g_drop_item >= 0 && (size_t)g_drop_item < items.size()) items.erase(items.begin() + g_drop_item);
   // device buffers in the second scratch pool
   auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
   size_t off_inst = 0, off_items = al(sizeof(QInst) * ninst), off_mask = off_items + al(sizeof(QItem) * items.size());
@@ -327,6 +340,7 @@ extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne
   a.next = (unsigned int*)(base + off_cnt);
   a.done = a.next + 2;
   a.status = c->d_status;
+  a.spin_limit = g_spin_limit;
   a.work = (double2*)(base + off_work);
   a.nitems = (int)items.size();
   a.tile = T;
