@@ -224,7 +224,8 @@ static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpa
     std::vector<FOp> prog;
     Pass2Args a;
     memset(&a, 0, sizeof(a));
-    plan_program(one, p, s->precision, false, prog, a.load_pos, a.store_pos);
+    plan_program(one, p, s->precision, false, 4, prog, a.load_pos, a.store_pos);
+    a.nreg = 4;  // probes: 256 threads, ancilla on register bit 3
     void* dev;
     size_t fb = sizeof(FOp) * prog.size();
     int rc = ctx_scratch(c, fb + 256, &dev);
@@ -249,7 +250,7 @@ static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpa
     a.status = c->d_status;
     a.gpart = gpart;
     a.nslots = nprobe;
-    const int nctas = std::min<int>(fused2_grid(), 1 << (s->n - KET_T2_BITS));
+    const int nctas = std::min<int>(fused2_grid(4), 1 << (s->n - KET_T2_BITS));
     if ((size_t)nctas * nprobe * 8 > gpart_cap) return fail(KET_ERR_UNSUPPORTED, "too many gradient probes in a pass");
     prof_begin(c);
     e = launch_fused2(a, s->precision, c->stream);
@@ -403,7 +404,7 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
   }
   const int hblocks = 1024;
   rc = dev_alloc((void**)&w.slot_out, sizeof(double) * std::max<size_t>(nbinds, 1));
-  if (!rc) { w.gpart_cap = (size_t)fused2_grid() * 8 * 512; rc = dev_alloc((void**)&w.gpart, sizeof(double) * w.gpart_cap); }
+  if (!rc) { w.gpart_cap = (size_t)fused2_grid(4) * 8 * 512; rc = dev_alloc((void**)&w.gpart, sizeof(double) * w.gpart_cap); }
   if (!rc) rc = dev_alloc((void**)&w.terms, sizeof(DevTerm) * std::max<size_t>(dterms.size(), 1));
   if (!rc) rc = dev_alloc((void**)&w.epart, sizeof(double) * (hblocks + 8));
   if (rc) { cleanup(); return rc; }

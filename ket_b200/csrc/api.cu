@@ -372,7 +372,7 @@ int ket_plan_program_stats(int n, int precision, const ket_op* ops, size_t nops,
     if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) { counts[15]++; continue; }
     std::vector<FOp> prog;
     uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
-    plan_program(plan, p, precision, o.prune != 0, prog, lp, sp);
+    plan_program(plan, p, precision, o.prune != 0, KET_FUSED_NREG, prog, lp, sp);
     for (const FOp& f : prog)
       if (f.type != FO_CONT) counts[f.type]++;
     counts[14]++;
@@ -419,7 +419,8 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
       std::vector<FOp> prog;
       Pass2Args& a = p2[i];
       memset(&a, 0, sizeof(a));
-      plan_program(plan, p, s->precision, prune, prog, a.load_pos, a.store_pos);
+      plan_program(plan, p, s->precision, prune, KET_FUSED_NREG, prog, a.load_pos, a.store_pos);
+      a.nreg = KET_FUSED_NREG;
       off[i] = fops.size();
       fops.insert(fops.end(), prog.begin(), prog.end());
       a.amp = s->amp;

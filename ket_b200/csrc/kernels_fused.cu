@@ -1,17 +1,18 @@
 // kernels_fused.cu -- the register-tiled fused gate pass.
 //
-// One CTA of 256 threads owns a tile of 2^12 amplitudes at a time: the L
-// lowest qubits (contiguous in HBM) plus 12-L high qubits chosen by the
-// planner.  Each thread keeps 16 amplitudes in registers.  The tile's 12 bits
-// are split into 5 lane bits, 3 warp bits and 4 register bits; a gate whose
+// A CTA owns a tile of 2^12 amplitudes at a time: the L lowest qubits
+// (contiguous in HBM) plus 12-L high qubits chosen by the planner.  The tile's
+// 12 bits are split into 5 lane bits, NW warp bits and NR register bits
+// (NW + NR = 7): ordinary passes use NR = 5 (128 threads holding 32 amplitudes
+// each, two CTAs per SM, so one CTA's tile loads overlap the other's
+// arithmetic), adjoint passes NR = 4 (256 threads, 16 amplitudes).  A gate whose
 // target is a register bit is applied inside each thread, a gate on a lane
 // bit uses warp shuffles, and a gate on a warp bit first re-lays the tile out
 // through shared memory (FO_EXCH).  Diagonal gates need no pairing and apply
 // on any qubit, in or out of the tile.  The global load and store use a
 // layout whose lane bits are the tile's low bits, so every warp touches whole
 // 128-byte lines.  A pass costs one read and one write of the state however
-// many gates it holds.  The persistent grid runs one CTA per SM whose threads
-// each hold two tiles (every op decode then serves 32 amplitudes).
+// many gates it holds.
 //
 // The kernel is issue-bound, so the per-op overhead is kept small:
 //   * an op's first 16 bytes hold everything needed to skip or dispatch it,
@@ -31,16 +32,11 @@
 #include "common.cuh"
 #include "launch.h"
 
-// Resident CTAs per SM: the register budget per thread is 65536 / (256 * this).
-#ifndef KET_FUSED_CTAS_PER_SM
-#define KET_FUSED_CTAS_PER_SM 1
-#endif
-
 namespace ket {
 
 namespace {
 
-__constant__ uint16_t c_slotmask[16];  // slots j with (j & creg) == creg
+__constant__ uint32_t c_slotmask[32];  // slots j < 32 with (j & creg) == creg
 
 // ---------------------------------------------------------------- shared memory
 __device__ __forceinline__ void sts(uint32_t a, const cpx<double>& v) {
@@ -62,58 +58,66 @@ __device__ __forceinline__ uint32_t swz(uint32_t i) {
 }
 
 // A thread's view of a layout in the exchange buffer: slot j lives at byte
-// b ^ (j0 ? s0 : 0) ^ (j1 ? s1 : 0) ^ (j2 ? s2 : 0) ^ (j3 ? s3 : 0).
+// b ^ XOR over the set bits k of j of s[k].
+template <int NR>
 struct SLay {
-  uint32_t b, s0, s1, s2, s3;
+  uint32_t b, s[NR];
 };
 
-__device__ __forceinline__ uint32_t soff(const SLay& l, int j) {
+template <int NR>
+__device__ __forceinline__ uint32_t soff(const SLay<NR>& l, int j) {
   uint32_t o = l.b;
-  if (j & 1) o ^= l.s0;
-  if (j & 2) o ^= l.s1;
-  if (j & 4) o ^= l.s2;
-  if (j & 8) o ^= l.s3;
+#pragma unroll
+  for (int k = 0; k < NR; k++)
+    if (j & (1 << k)) o ^= l.s[k];
   return o;
 }
 
-// bx[r] = exchange offset of role r's tile bit.
-__device__ __forceinline__ SLay make_slay(const uint32_t* bx, int lane, int warp) {
-  SLay l;
+// bx[r] = exchange offset of role r's tile bit (roles: 5 lanes, 7-NR warps, NR registers).
+template <int NR>
+__device__ __forceinline__ SLay<NR> make_slay(const uint32_t* bx, int lane, int warp) {
+  constexpr int NW = 7 - NR;
+  SLay<NR> l;
   uint32_t b = 0;
 #pragma unroll
   for (int r = 0; r < 5; r++)
     if ((lane >> r) & 1) b ^= bx[r];
 #pragma unroll
-  for (int r = 0; r < 3; r++)
+  for (int r = 0; r < NW; r++)
     if ((warp >> r) & 1) b ^= bx[5 + r];
   l.b = b;
-  l.s0 = bx[8];
-  l.s1 = bx[9];
-  l.s2 = bx[10];
-  l.s3 = bx[11];
+#pragma unroll
+  for (int k = 0; k < NR; k++) l.s[k] = bx[5 + NW + k];
   return l;
 }
 
 // FO_EXCH keeps the new layout's 12 offsets as uint16 in its matrix area.
-__device__ __forceinline__ SLay exch_slay(const FOp* op, int lane, int warp) {
+template <int NR>
+__device__ __forceinline__ SLay<NR> exch_slay(const FOp* op, int lane, int warp) {
   const uint4 q0 = __ldg(reinterpret_cast<const uint4*>(op->m));
   const uint2 q1 = __ldg(reinterpret_cast<const uint2*>(op->m) + 2);
   const uint32_t w[6] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
   uint32_t bx[12];
 #pragma unroll
   for (int r = 0; r < 12; r++) bx[r] = (w[r >> 1] >> (16 * (r & 1))) & 0xffffu;
-  return make_slay(bx, lane, warp);
+  return make_slay<NR>(bx, lane, warp);
 }
 
-template <typename R>
-__device__ __forceinline__ void write_tile(uint32_t smb, const SLay& l, const cpx<R>* x) {
+template <typename R, int NR>
+__device__ __forceinline__ void write_tile(uint32_t smb, const SLay<NR>& l, const cpx<R>* x) {
 #pragma unroll
-  for (int j = 0; j < 16; j++) sts(smb + soff(l, j), x[j]);
+  for (int j = 0; j < (1 << NR); j++) sts(smb + soff<NR>(l, j), x[j]);
 }
-template <typename R>
-__device__ __forceinline__ void read_tile(uint32_t smb, const SLay& l, cpx<R>* x) {
+template <typename R, int NR>
+__device__ __forceinline__ void read_tile(uint32_t smb, const SLay<NR>& l, cpx<R>* x) {
 #pragma unroll
-  for (int j = 0; j < 16; j++) lds(smb + soff(l, j), x[j]);
+  for (int j = 0; j < (1 << NR); j++) lds(smb + soff<NR>(l, j), x[j]);
+}
+
+// Mask of all NS slots.
+template <int NS>
+__device__ __forceinline__ constexpr uint32_t full_mask() {
+  return NS == 32 ? 0xffffffffu : ((1u << NS) - 1u);
 }
 
 // ---------------------------------------------------------------- pruning screen
@@ -124,19 +128,19 @@ __device__ __forceinline__ float hiabs(float v) { return fabsf(v); }
 __device__ __forceinline__ float tiny_screen(double) { return __int_as_float(0x3E7AD7F3); }
 __device__ __forceinline__ float tiny_screen(float) { return __int_as_float(0x33D6BF96); }  // just above 1e-7f
 
-template <typename R>
-__device__ __forceinline__ void prune16(cpx<R>* x, double thr, double qthr) {
+template <typename R, int NS>
+__device__ __forceinline__ void prune_slots(cpx<R>* x, double thr, double qthr) {
   // an amplitude can be pruned only if both components are below 1e-7
-  float t[16];
+  float t[NS];
 #pragma unroll
-  for (int j = 0; j < 16; j++) t[j] = fmaxf(hiabs(x[j].re), hiabs(x[j].im));
+  for (int j = 0; j < NS; j++) t[j] = fmaxf(hiabs(x[j].re), hiabs(x[j].im));
 #pragma unroll
-  for (int w = 8; w > 0; w >>= 1)
+  for (int w = NS / 2; w > 0; w >>= 1)
 #pragma unroll
     for (int j = 0; j < w; j++) t[j] = fminf(t[j], t[j + w]);
   if (t[0] < tiny_screen(R(0))) {
 #pragma unroll
-    for (int j = 0; j < 16; j++) prune_amp(x[j], thr, qthr);
+    for (int j = 0; j < NS; j++) prune_amp(x[j], thr, qthr);
   }
 }
 
@@ -209,17 +213,17 @@ __device__ __forceinline__ void cmul_in(cpx<R>& x, R mr, R mi) {
   x.im = fma(mr, x.im, q);
 }
 
-template <typename R, int A, int FORM>
+template <typename R, int A, int FORM, int NS>
 __device__ __forceinline__ void mat1_reg(cpx<R>* x, const R* m, uint32_t smask) {
-  if (smask == 0xffffu) {
+  if (smask == full_mask<NS>()) {
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
+    for (int j = 0; j < NS; j++) {
       if (j & (1 << A)) continue;
       mat2x2<R, FORM>(x[j], x[j | (1 << A)], m);
     }
   } else {
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
+    for (int j = 0; j < NS; j++) {
       if (j & (1 << A)) continue;
       const int j1 = j | (1 << A);
       cpx<R> a0 = x[j], a1 = x[j1];
@@ -232,35 +236,35 @@ __device__ __forceinline__ void mat1_reg(cpx<R>* x, const R* m, uint32_t smask) 
 }
 
 // X on register bit A where register bit C is 1 (a CNOT inside the thread).
-template <typename R, int A, int C>
+template <typename R, int A, int C, int NS>
 __device__ __forceinline__ void x1c_reg(cpx<R>* x) {
 #pragma unroll
-  for (int j = 0; j < 16; j++)
+  for (int j = 0; j < NS; j++)
     if (!(j & (1 << A)) && (j & (1 << C))) swap_c(x[j], x[j | (1 << A)]);
 }
 
 // diag(1, d1) on register bit A where register bit C is 1 (a controlled phase).
-template <typename R, int A, int C>
+template <typename R, int A, int C, int NS>
 __device__ __forceinline__ void diag1c_reg(cpx<R>* x, R d1r, R d1i) {
 #pragma unroll
-  for (int j = 0; j < 16; j++)
+  for (int j = 0; j < NS; j++)
     if ((j & (1 << A)) && (j & (1 << C))) cmul_in<R>(x[j], d1r, d1i);
 }
 
 // X on register bit A (no register controls: other controls skip the thread).
-template <typename R, int A>
+template <typename R, int A, int NS>
 __device__ __forceinline__ void x1_reg(cpx<R>* x) {
 #pragma unroll
-  for (int j = 0; j < 16; j++)
+  for (int j = 0; j < NS; j++)
     if (!(j & (1 << A))) swap_c(x[j], x[j | (1 << A)]);
 }
 
 // diag(d0, d1) on register bit A; D0ONE: d0 == 1, so bit-0 slots are untouched.
-template <typename R, int A, bool D0ONE>
+template <typename R, int A, bool D0ONE, int NS>
 __device__ __forceinline__ void diag_reg(cpx<R>* x, R d0r, R d0i, R d1r, R d1i, uint32_t smask) {
-  if (smask == 0xffffu) {
+  if (smask == full_mask<NS>()) {
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
+    for (int j = 0; j < NS; j++) {
       const bool one = (j >> A) & 1;
       if (D0ONE && !one) continue;
       cmul_in<R>(x[j], one ? d1r : d0r, one ? d1i : d0i);
@@ -268,7 +272,7 @@ __device__ __forceinline__ void diag_reg(cpx<R>* x, R d0r, R d0i, R d1r, R d1i, 
     return;
   }
 #pragma unroll
-  for (int j = 0; j < 16; j++) {
+  for (int j = 0; j < NS; j++) {
     const bool one = (j >> A) & 1;
     if (D0ONE && !one) continue;
     cpx<R> y = cmul<R>(one ? d1r : d0r, one ? d1i : d0i, x[j]);
@@ -276,15 +280,15 @@ __device__ __forceinline__ void diag_reg(cpx<R>* x, R d0r, R d0i, R d1r, R d1i, 
   }
 }
 
-template <typename R>
+template <typename R, int NS>
 __device__ __forceinline__ void phase_all(cpx<R>* x, R dr, R di, uint32_t smask) {
-  if (smask == 0xffffu) {
+  if (smask == full_mask<NS>()) {
 #pragma unroll
-    for (int j = 0; j < 16; j++) cmul_in<R>(x[j], dr, di);
+    for (int j = 0; j < NS; j++) cmul_in<R>(x[j], dr, di);
     return;
   }
 #pragma unroll
-  for (int j = 0; j < 16; j++) {
+  for (int j = 0; j < NS; j++) {
     cpx<R> y = cmul<R>(dr, di, x[j]);
     x[j] = sel<R>((smask >> j) & 1, y, x[j]);
   }
@@ -312,13 +316,16 @@ __device__ __forceinline__ uint64_t ctx_of(const Pass2Args& a, uint64_t tile) {
 // ---------------------------------------------------------------- phase fans
 // FO_CPHASE on register bit A for the TT tiles of a thread; tile t's context is
 // ctx0 | (t ? pairq : 0).
-template <typename R, int A, int TT>
-__device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][16], const FOp* op, uint32_t nterms, uint64_t ctx0,
+template <typename R, int A, int TT, int NS>
+__device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][NS], const FOp* op, uint32_t nterms, uint64_t ctx0,
                                           uint64_t pairq, int tid) {
+  // record 0 after the op: H[0..7]; records 1..: (angle, mask) pairs; each
+  // record's data starts after its 16-byte no-op header
+  const double2* H = reinterpret_cast<const double2*>(reinterpret_cast<const char*>(op + 1) + 16);
   double th0 = 0.0, thp = 0.0;
   for (uint32_t i = 0; i < nterms; i++) {
     const uint32_t r = i / KET_CPHASE_TERMS_PER_RECORD, w = i - r * KET_CPHASE_TERMS_PER_RECORD;
-    const double2 t = __ldg(reinterpret_cast<const double2*>(reinterpret_cast<const char*>(op + 1 + r) + 16) + w);
+    const double2 t = __ldg(reinterpret_cast<const double2*>(reinterpret_cast<const char*>(op + 2 + r) + 16) + w);
     const uint64_t mk = (uint64_t)__double_as_longlong(t.y);
     if (ctx0 & mk) th0 += t.x;
     if (pairq & mk) thp += t.x;
@@ -328,7 +335,7 @@ __device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][16], const FOp* op, ui
   double fr = 1.0, fi = 0.0;
 #pragma unroll
   for (int sb = 0; sb < 8; sb++) {
-    const double2 h = __ldg(mp + 8 + sb);
+    const double2 h = __ldg(H + sb);
     const bool on = (tid >> sb) & 1;
     const double hr = on ? h.x : 1.0, hi = on ? h.y : 0.0;
     const double r = fr * hr - fi * hi;
@@ -341,7 +348,7 @@ __device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][16], const FOp* op, ui
     sincos(th0 + (t ? thp : 0.0), &sn, &cs);
     const double gr = cs * fr - sn * fi, gi = cs * fi + sn * fr;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
+    for (int k = 0; k < NS / 2; k++) {
       const int j = ((k >> A) << (A + 1)) | (1 << A) | (k & ((1 << A) - 1));
       const double2 tk = __ldg(mp + k);
       const R pr = (R)(tk.x * gr - tk.y * gi), pi = (R)(tk.x * gi + tk.y * gr);
@@ -351,7 +358,7 @@ __device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][16], const FOp* op, ui
 }
 
 // ---------------------------------------------------------------- adjoint probes
-// Register bit 3 selects psi (0) / lambda (1).
+// Adjoint passes use 16 slots per thread: register bit 3 selects psi (0) / lambda (1).
 // Re<lambda| D |psi> with D 2x2 on register bit A.
 template <typename R, int A>
 __device__ __forceinline__ double grad_m(const cpx<R>* x, const R* d, uint32_t smask) {
@@ -389,8 +396,9 @@ __device__ __forceinline__ void grad_accum(double* sgrad, int slot, int warp, in
 }
 
 // ---------------------------------------------------------------- the pass
-template <typename R, int NT, bool GRAD, int TT>
-__global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
+template <typename R, bool GRAD, int TT, int NR>
+__global__ void __launch_bounds__(32 << (7 - NR), NR == 5 ? 2 : 1) k_fused2(Pass2Args a) {
+  constexpr int NW = 7 - NR, NT = 32 << NW, NS = 1 << NR;  // warp bits, threads, slots per thread
   typedef typename Vec2<R>::T V;
   extern __shared__ __align__(128) unsigned char smraw[];
   // shared memory: one exchange buffer per tile a thread holds | gradient partials
@@ -409,7 +417,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
   // on all TT tiles the same way.
   const uint64_t ngroups = (uint64_t(1) << (a.n - KET_T2_BITS)) / TT;
   const uint64_t pairq = TT > 1 ? uint64_t(1) << a.ctxbits[a.pairbit] : 0;
-  cpx<R> x[TT][16];
+  cpx<R> x[TT][NS];
 
   for (uint64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     const uint64_t tile0 = TT > 1 ? insert0(grp, a.pairbit) : grp;
@@ -420,23 +428,22 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
       for (int r = 0; r < 5; r++)
         if ((lane >> r) & 1) gl += a.lgb[r];
 #pragma unroll
-      for (int r = 0; r < 3; r++)
+      for (int r = 0; r < NW; r++)
         if ((warp >> r) & 1) gl += a.lgb[5 + r];
 #pragma unroll
       for (int t = 0; t < TT; t++) {
         const char* p = amp + (ctx0 | (t ? pairq : 0)) * sizeof(V) + gl;
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
+        for (int j = 0; j < NS; j++) {
           uint64_t o = 0;
-          if (j & 1) o += a.lgb[8];
-          if (j & 2) o += a.lgb[9];
-          if (j & 4) o += a.lgb[10];
-          if (j & 8) o += a.lgb[11];
+#pragma unroll
+          for (int k = 0; k < NR; k++)
+            if (j & (1 << k)) o += a.lgb[5 + NW + k];
           x[t][j] = ld_amp<R>(reinterpret_cast<const V*>(p + o));
         }
       }
     }
-    SLay sl = make_slay(a.lbx, lane, warp);
+    SLay<NR> sl = make_slay<NR>(a.lbx, lane, warp);
     uint4 hn = a.nops > 0 ? __ldg(reinterpret_cast<const uint4*>(a.ops)) : make_uint4(0u, 0u, 0u, 0u);
     for (int k = 0; k < a.nops; k++) {
       const FOp* op = a.ops + k;
@@ -450,11 +457,11 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
       if (opc == OC_EXCH) {
         __syncthreads();
 #pragma unroll
-        for (int t = 0; t < TT; t++) write_tile<R>(smb + t * TB, sl, x[t]);
+        for (int t = 0; t < TT; t++) write_tile<R, NR>(smb + t * TB, sl, x[t]);
         __syncthreads();
-        sl = exch_slay(op, lane, warp);
+        sl = exch_slay<NR>(op, lane, warp);
 #pragma unroll
-        for (int t = 0; t < TT; t++) read_tile<R>(smb + t * TB, sl, x[t]);
+        for (int t = 0; t < TT; t++) read_tile<R, NR>(smb + t * TB, sl, x[t]);
         continue;
       }
       const uint64_t cctx = ((uint64_t)h.w << 32) | h.z;
@@ -470,7 +477,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
         const int ob = (int)(h2.w & 0xffu);
         __syncthreads();
 #pragma unroll
-        for (int t = 0; t < TT; t++) write_tile<R>(smb + t * TB, sl, x[t]);
+        for (int t = 0; t < TT; t++) write_tile<R, NR>(smb + t * TB, sl, x[t]);
         __syncthreads();
         const int ta = oa, tb = ob;
         if (GRAD && opc == OC_GRADM2) {
@@ -511,7 +518,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
           }
           __syncthreads();
 #pragma unroll
-          for (int t = 0; t < TT; t++) read_tile<R>(smb + t * TB, sl, x[t]);
+          for (int t = 0; t < TT; t++) read_tile<R, NR>(smb + t * TB, sl, x[t]);
           continue;
         }
         if (opc == OC_DIAG) {
@@ -533,7 +540,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
           }
           __syncthreads();
 #pragma unroll
-          for (int t = 0; t < TT; t++) read_tile<R>(smb + t * TB, sl, x[t]);
+          for (int t = 0; t < TT; t++) read_tile<R, NR>(smb + t * TB, sl, x[t]);
           continue;
         }
         const int lo = ta < tb ? ta : tb, hi = ta < tb ? tb : ta;
@@ -568,7 +575,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
         }
         __syncthreads();
 #pragma unroll
-        for (int t = 0; t < TT; t++) read_tile<R>(smb + t * TB, sl, x[t]);
+        for (int t = 0; t < TT; t++) read_tile<R, NR>(smb + t * TB, sl, x[t]);
         continue;  // pruning already done
       }
       const bool thr_ok = ((uint32_t)tid & cthr) == cthr;
@@ -578,7 +585,7 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
         // ancilla there.  Every lane takes part in the warp sum.  (TT == 1)
         const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);
         const int slot = (int16_t)(h2.z & 0xffff);
-        const uint32_t smask = thr_ok ? (uint32_t)c_slotmask[creg & 15] : 0u;
+        const uint32_t smask = thr_ok ? (c_slotmask[creg] & full_mask<NS>()) : 0u;
         double acc = 0.0;
         if (opc != OC_GRADD) {
           R d[8];
@@ -607,18 +614,20 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
       // Thread-local ops and shuffles among the lanes that take part: a thread
       // whose thread-bit controls fail leaves its amplitudes alone.
       if (!thr_ok) continue;
-      const uint32_t smask = creg ? (uint32_t)c_slotmask[creg & 15] : 0xffffu;
+      const uint32_t smask = creg ? (c_slotmask[creg] & full_mask<NS>()) : full_mask<NS>();
       switch (opc) {
-#define KET_MAT1R(A, F)                             \
-  case OC_MAT1R + 3 * A + F: {                      \
-    const R m[8] = {(R)q0.x, (R)q0.y, (R)q1.x, (R)q1.y, (R)q2.x, (R)q2.y, (R)q3.x, (R)q3.y}; \
-    for (int t = 0; t < TT; t++) mat1_reg<R, A, F>(x[t], m, smask);                 \
-    break;                                          \
-  }
+#define KET_MAT1R(A, F)                                                                   \
+  case OC_MAT1R + 3 * A + F:                                                              \
+    if constexpr (A < NR) {                                                               \
+      const R m[8] = {(R)q0.x, (R)q0.y, (R)q1.x, (R)q1.y, (R)q2.x, (R)q2.y, (R)q3.x, (R)q3.y}; \
+      for (int t = 0; t < TT; t++) mat1_reg<R, A, F, NS>(x[t], m, smask);                 \
+    }                                                                                     \
+    break;
         KET_MAT1R(0, 0) KET_MAT1R(0, 1) KET_MAT1R(0, 2)
         KET_MAT1R(1, 0) KET_MAT1R(1, 1) KET_MAT1R(1, 2)
         KET_MAT1R(2, 0) KET_MAT1R(2, 1) KET_MAT1R(2, 2)
         KET_MAT1R(3, 0) KET_MAT1R(3, 1) KET_MAT1R(3, 2)
+        KET_MAT1R(4, 0) KET_MAT1R(4, 1) KET_MAT1R(4, 2)
 #undef KET_MAT1R
         case OC_MAT1L: case OC_MAT1L + 1: case OC_MAT1L + 2: {
           const uint32_t members = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
@@ -632,46 +641,47 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
 #pragma unroll
             for (int t = 0; t < TT; t++)
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
+            for (int j = 0; j < NS; j++) {
               cpx<R> p = shfl_xor_c<R>(x[t][j], msk, members);
               cpx<R> y;
               y.re = fma(c0r, x[t][j].re, c1r * p.re);
               y.im = fma(c0r, x[t][j].im, c1r * p.im);
-              x[t][j] = smask == 0xffffu ? y : sel<R>((smask >> j) & 1, y, x[t][j]);
+              x[t][j] = smask == full_mask<NS>() ? y : sel<R>((smask >> j) & 1, y, x[t][j]);
             }
           } else if (opc == OC_MAT1L + 2) {
 #pragma unroll
             for (int t = 0; t < TT; t++)
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
+            for (int j = 0; j < NS; j++) {
               cpx<R> p = shfl_xor_c<R>(x[t][j], msk, members);
               cpx<R> y;
               y.re = fma(c0r, x[t][j].re, -c1i * p.im);
               y.im = fma(c0r, x[t][j].im, c1i * p.re);
-              x[t][j] = smask == 0xffffu ? y : sel<R>((smask >> j) & 1, y, x[t][j]);
+              x[t][j] = smask == full_mask<NS>() ? y : sel<R>((smask >> j) & 1, y, x[t][j]);
             }
           } else {
 #pragma unroll
             for (int t = 0; t < TT; t++)
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
+            for (int j = 0; j < NS; j++) {
               cpx<R> p = shfl_xor_c<R>(x[t][j], msk, members);
               cpx<R> y = mac2<R>(c0r, c0i, x[t][j], c1r, c1i, p);
-              x[t][j] = smask == 0xffffu ? y : sel<R>((smask >> j) & 1, y, x[t][j]);
+              x[t][j] = smask == full_mask<NS>() ? y : sel<R>((smask >> j) & 1, y, x[t][j]);
             }
           }
           break;
         }
-        case OC_X1R + 0: for (int t = 0; t < TT; t++) x1_reg<R, 0>(x[t]); break;
-        case OC_X1R + 1: for (int t = 0; t < TT; t++) x1_reg<R, 1>(x[t]); break;
-        case OC_X1R + 2: for (int t = 0; t < TT; t++) x1_reg<R, 2>(x[t]); break;
-        case OC_X1R + 3: for (int t = 0; t < TT; t++) x1_reg<R, 3>(x[t]); break;
+#define KET_X1R(A) \
+  case OC_X1R + A: if constexpr (A < NR) { for (int t = 0; t < TT; t++) x1_reg<R, A, NS>(x[t]); } break;
+        KET_X1R(0) KET_X1R(1) KET_X1R(2) KET_X1R(3) KET_X1R(4)
+#undef KET_X1R
 #define KET_X1RC(A, C) \
-  case OC_X1RC + 4 * A + C: for (int t = 0; t < TT; t++) x1c_reg<R, A, C>(x[t]); break;
-        KET_X1RC(0, 1) KET_X1RC(0, 2) KET_X1RC(0, 3)
-        KET_X1RC(1, 0) KET_X1RC(1, 2) KET_X1RC(1, 3)
-        KET_X1RC(2, 0) KET_X1RC(2, 1) KET_X1RC(2, 3)
-        KET_X1RC(3, 0) KET_X1RC(3, 1) KET_X1RC(3, 2)
+  case OC_X1RC + 5 * A + C: if constexpr (A < NR && C < NR) { for (int t = 0; t < TT; t++) x1c_reg<R, A, C, NS>(x[t]); } break;
+        KET_X1RC(0, 1) KET_X1RC(0, 2) KET_X1RC(0, 3) KET_X1RC(0, 4)
+        KET_X1RC(1, 0) KET_X1RC(1, 2) KET_X1RC(1, 3) KET_X1RC(1, 4)
+        KET_X1RC(2, 0) KET_X1RC(2, 1) KET_X1RC(2, 3) KET_X1RC(2, 4)
+        KET_X1RC(3, 0) KET_X1RC(3, 1) KET_X1RC(3, 2) KET_X1RC(3, 4)
+        KET_X1RC(4, 0) KET_X1RC(4, 1) KET_X1RC(4, 2) KET_X1RC(4, 3)
 #undef KET_X1RC
         case OC_X1L: {
           const uint32_t members = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
@@ -679,39 +689,41 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
 #pragma unroll
           for (int t = 0; t < TT; t++)
 #pragma unroll
-          for (int j = 0; j < 16; j++) {
+          for (int j = 0; j < NS; j++) {
             cpx<R> p = shfl_xor_c<R>(x[t][j], msk, members);
-            x[t][j] = smask == 0xffffu ? p : sel<R>((smask >> j) & 1, p, x[t][j]);
+            x[t][j] = smask == full_mask<NS>() ? p : sel<R>((smask >> j) & 1, p, x[t][j]);
           }
           break;
         }
-#define KET_DIAGR(A, ONE)                                                         \
-  case (ONE ? OC_DIAGR1 : OC_DIAGR) + A: {                                        \
-    const double2 e0 = q0, e1 = q1;                                             \
-    for (int t = 0; t < TT; t++) diag_reg<R, A, ONE>(x[t], (R)e0.x, (R)e0.y, (R)e1.x, (R)e1.y, smask);          \
-    break;                                                                        \
-  }
-        KET_DIAGR(0, false) KET_DIAGR(1, false) KET_DIAGR(2, false) KET_DIAGR(3, false)
-        KET_DIAGR(0, true) KET_DIAGR(1, true) KET_DIAGR(2, true) KET_DIAGR(3, true)
+#define KET_DIAGR(A, ONE)                                                                   \
+  case (ONE ? OC_DIAGR1 : OC_DIAGR) + A:                                                    \
+    if constexpr (A < NR) {                                                                 \
+      for (int t = 0; t < TT; t++) diag_reg<R, A, ONE, NS>(x[t], (R)q0.x, (R)q0.y, (R)q1.x, (R)q1.y, smask); \
+    }                                                                                       \
+    break;
+        KET_DIAGR(0, false) KET_DIAGR(1, false) KET_DIAGR(2, false) KET_DIAGR(3, false) KET_DIAGR(4, false)
+        KET_DIAGR(0, true) KET_DIAGR(1, true) KET_DIAGR(2, true) KET_DIAGR(3, true) KET_DIAGR(4, true)
 #undef KET_DIAGR
-#define KET_DIAGR1C(A, C)                                                         \
-  case OC_DIAGR1C + 4 * A + C: {                                                  \
-    const double2 e1 = q1;                                                      \
-    for (int t = 0; t < TT; t++) diag1c_reg<R, A, C>(x[t], (R)e1.x, (R)e1.y);                                     \
-    break;                                                                        \
-  }
-        KET_DIAGR1C(0, 1) KET_DIAGR1C(0, 2) KET_DIAGR1C(0, 3)
-        KET_DIAGR1C(1, 0) KET_DIAGR1C(1, 2) KET_DIAGR1C(1, 3)
-        KET_DIAGR1C(2, 0) KET_DIAGR1C(2, 1) KET_DIAGR1C(2, 3)
-        KET_DIAGR1C(3, 0) KET_DIAGR1C(3, 1) KET_DIAGR1C(3, 2)
+#define KET_DIAGR1C(A, C)                                                                   \
+  case OC_DIAGR1C + 5 * A + C:                                                              \
+    if constexpr (A < NR && C < NR) {                                                       \
+      for (int t = 0; t < TT; t++) diag1c_reg<R, A, C, NS>(x[t], (R)q1.x, (R)q1.y);         \
+    }                                                                                       \
+    break;
+        KET_DIAGR1C(0, 1) KET_DIAGR1C(0, 2) KET_DIAGR1C(0, 3) KET_DIAGR1C(0, 4)
+        KET_DIAGR1C(1, 0) KET_DIAGR1C(1, 2) KET_DIAGR1C(1, 3) KET_DIAGR1C(1, 4)
+        KET_DIAGR1C(2, 0) KET_DIAGR1C(2, 1) KET_DIAGR1C(2, 3) KET_DIAGR1C(2, 4)
+        KET_DIAGR1C(3, 0) KET_DIAGR1C(3, 1) KET_DIAGR1C(3, 2) KET_DIAGR1C(3, 4)
+        KET_DIAGR1C(4, 0) KET_DIAGR1C(4, 1) KET_DIAGR1C(4, 2) KET_DIAGR1C(4, 3)
 #undef KET_DIAGR1C
 #define KET_CPHASE(A)                                                                         \
-  case OC_CPHASE + A: {                                                                       \
-    const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);                          \
-    phase_fan<R, A, TT>(x, op, h2.x, ctx0, pairq, tid);                                       \
-    break; /* the continuation records that follow run as no-ops */                          \
-  }
-        KET_CPHASE(0) KET_CPHASE(1) KET_CPHASE(2) KET_CPHASE(3)
+  case OC_CPHASE + A:                                                                         \
+    if constexpr (A < NR) {                                                                   \
+      const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);                        \
+      phase_fan<R, A, TT, NS>(x, op, h2.x, ctx0, pairq, tid);                                 \
+    }                                                                                         \
+    break; /* the continuation records that follow run as no-ops */
+        KET_CPHASE(0) KET_CPHASE(1) KET_CPHASE(2) KET_CPHASE(3) KET_CPHASE(4)
 #undef KET_CPHASE
         case OC_DIAGT: case OC_DIAGX: {
           bool one;
@@ -719,14 +731,14 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
           else one = (ctx0 & __ldg(reinterpret_cast<const unsigned long long*>(op) + 4)) != 0;
           if ((fl & FOF_D0ONE) && !one) break;
           const double2 e = one ? q1 : q0;
-          for (int t = 0; t < TT; t++) phase_all<R>(x[t], (R)e.x, (R)e.y, smask);
+          for (int t = 0; t < TT; t++) phase_all<R, NS>(x[t], (R)e.x, (R)e.y, smask);
           break;
         }
         default: break;
       }
       if (fl & FOF_PRUNE)  // mixing ops only (the planner clears the flag elsewhere)
 #pragma unroll
-        for (int t = 0; t < TT; t++) prune16<R>(x[t], thr, qthr);
+        for (int t = 0; t < TT; t++) prune_slots<R, NS>(x[t], thr, qthr);
     }
     // the planner leaves the store layout in force here
     {
@@ -735,18 +747,17 @@ __global__ void __launch_bounds__(NT, 1) k_fused2(Pass2Args a) {
       for (int r = 0; r < 5; r++)
         if ((lane >> r) & 1) gs += a.sgb[r];
 #pragma unroll
-      for (int r = 0; r < 3; r++)
+      for (int r = 0; r < NW; r++)
         if ((warp >> r) & 1) gs += a.sgb[5 + r];
 #pragma unroll
       for (int t = 0; t < TT; t++) {
         char* p = amp + (ctx0 | (t ? pairq : 0)) * sizeof(V) + gs;
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
+        for (int j = 0; j < NS; j++) {
           uint64_t o = 0;
-          if (j & 1) o += a.sgb[8];
-          if (j & 2) o += a.sgb[9];
-          if (j & 4) o += a.sgb[10];
-          if (j & 8) o += a.sgb[11];
+#pragma unroll
+          for (int k = 0; k < NR; k++)
+            if (j & (1 << k)) o += a.sgb[5 + NW + k];
           st_amp<R>(reinterpret_cast<V*>(p + o), x[t][j]);
         }
       }
@@ -768,19 +779,23 @@ __global__ void k_grad_reduce(const double* gpart, int nctas, int nslots, double
   out[s] = acc;
 }
 
-template <typename R, bool GRAD, int TT>
+// Resident CTAs per SM for a register-bit count: 5 -> two CTAs of 128 threads
+// (255 registers each), 4 -> one CTA of 256 threads.
+constexpr int ctas_per_sm(int nreg) { return nreg == 5 ? 2 : 1; }
+
+template <typename R, bool GRAD, int TT, int NR>
 cudaError_t launch_tt(const Pass2Args& a, cudaStream_t s) {
-  const int NT = 256;
+  constexpr int NT = 32 << (7 - NR);
   static bool init = false;
   if (!init) {
-    cudaFuncSetAttribute(k_fused2<R, NT, GRAD, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_fused2<R, GRAD, TT, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024);
     init = true;
   }
   const size_t tb = sizeof(cpx<R>) << KET_T2_BITS;
   const size_t smem = TT * tb + (GRAD ? sizeof(double) * 8 * (size_t)a.nslots : 0);
   const uint64_t ngroups = (uint64_t(1) << (a.n - KET_T2_BITS)) / TT;
-  const unsigned blocks = (unsigned)std::min<uint64_t>(ngroups, (uint64_t)fused2_grid());
-  k_fused2<R, NT, GRAD, TT><<<blocks, NT, smem, s>>>(a);
+  const unsigned blocks = (unsigned)std::min<uint64_t>(ngroups, (uint64_t)fused2_grid(NR));
+  k_fused2<R, GRAD, TT, NR><<<blocks, NT, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -788,11 +803,11 @@ template <typename R, bool GRAD>
 cudaError_t launch_t(const Pass2Args& in, cudaStream_t s) {
   static bool init = false;
   if (!init) {
-    uint16_t sm[16];
-    for (int c = 0; c < 16; c++) {
-      uint16_t v = 0;
-      for (int j = 0; j < 16; j++)
-        if ((j & c) == c) v |= (uint16_t)(1u << j);
+    uint32_t sm[32];
+    for (int c = 0; c < 32; c++) {
+      uint32_t v = 0;
+      for (int j = 0; j < 32; j++)
+        if ((j & c) == c) v |= 1u << j;
       sm[c] = v;
     }
     cudaMemcpyToSymbol(c_slotmask, sm, sizeof(sm));
@@ -809,15 +824,17 @@ cudaError_t launch_t(const Pass2Args& in, cudaStream_t s) {
     a.sgb[r] = gbit(a.store_pos[r]);
     a.lbx[r] = exch_offset(1u << a.load_pos[r], sizeof(R) == 4);
   }
-  if constexpr (!GRAD) {
-    if (a.pairbit >= 0 && a.nctx > 0) return launch_tt<R, GRAD, 2>(a, s);
+  if constexpr (GRAD) {
+    return launch_tt<R, true, 1, 4>(a, s);  // probes: 16 slots, ancilla on register bit 3
+  } else {
+    if (a.nreg == 5) return launch_tt<R, false, 1, 5>(a, s);
+    return launch_tt<R, false, 1, 4>(a, s);
   }
-  return launch_tt<R, GRAD, 1>(a, s);
 }
 
 }  // namespace
 
-int fused2_grid() { return num_sms() * KET_FUSED_CTAS_PER_SM; }
+int fused2_grid(int nreg) { return num_sms() * ctas_per_sm(nreg); }
 
 int choose_pairbit(const std::vector<FOp>& prog, const Pass2Args& a) {
   uint64_t used = 0;  // (a phase fan's out-of-tile terms are evaluated per tile: not counted)

@@ -35,10 +35,16 @@ struct PassArgs {
 };
 
 // ---------------------------------------------------------------- register-tiled pass
-// The tile's 12 bits are split into roles: 5 lane bits, 3 warp bits, 4 register
-// bits (each thread holds 16 amplitudes).  A layout lists, for lane bits 0..4,
-// warp bits 0..2 and register bits 0..3, which tile bit plays that role.
+// The tile's 12 bits are split into roles: 5 lane bits, NW warp bits and NR
+// register bits (NW + NR = 7; each thread holds 2^NR amplitudes).  Role r < 5
+// is lane bit r, 5 <= r < 5 + NW is warp bit r - 5 (thread-id bit r), and r >=
+// 5 + NW is register bit r - 5 - NW.  A layout lists which tile bit plays
+// each role.  Ordinary passes use NR = 5 (128 threads per CTA, two CTAs per
+// SM); adjoint passes use NR = 4 (256 threads).
 #define KET_T2_BITS 12
+#define KET_NR_MAX 5
+// Register bits of ordinary (non-adjoint) passes.
+#define KET_FUSED_NREG 5
 enum FOpType : uint8_t {
   FO_EXCH = 0,    // re-layout the tile through shared memory
   FO_MAT1R = 1,   // 2x2 on register bit a
@@ -70,24 +76,24 @@ enum FOpType : uint8_t {
 // bit, the matrix form and a register control are folded in by the host).
 enum FOpCode : uint8_t {
   OC_EXCH = 0,
-  OC_MAT1R = 1,       // + 3 * A + form (form 0 general, 1 real, 2 Rx-like): 1..12
-  OC_MAT1L = 13,      // + form: 13..15
-  OC_X1R = 16,        // + A: 16..19 (no register control)
-  OC_X1RC = 20,       // + 4 * A + C: 20..35, X on register bit A controlled by register bit C only
-  OC_X1L = 36,
-  OC_DIAGR = 37,      // + A: 37..40 (general diag)
-  OC_DIAGR1 = 41,     // + A: 41..44 (m0 == 1)
-  OC_DIAGR1C = 45,    // + 4 * A + C: 45..60 (m0 == 1, controlled by register bit C only)
-  OC_DIAGT = 61,
-  OC_DIAGX = 62,
-  OC_DIAG = 63,
-  OC_SWAPS = 64,
-  OC_MAT2S = 65,
-  OC_GRADM = 66,      // + A: 66..68
-  OC_GRADD = 69,
-  OC_GRADM2 = 70,
-  OC_X1S = 71,        // X on tile bit b with controls ctile, through shared memory (multi-controlled X)
-  OC_CPHASE = 72,     // + A: 72..75, phase fan on register bit A
+  OC_MAT1R = 1,       // + 3 * A + form (form 0 general, 1 real, 2 Rx-like): 1..15
+  OC_MAT1L = 16,      // + form: 16..18
+  OC_X1R = 19,        // + A: 19..23 (no register control)
+  OC_X1RC = 24,       // + 5 * A + C: 24..48, X on register bit A controlled by register bit C only
+  OC_X1L = 49,
+  OC_DIAGR = 50,      // + A: 50..54 (general diag)
+  OC_DIAGR1 = 55,     // + A: 55..59 (m0 == 1)
+  OC_DIAGR1C = 60,    // + 5 * A + C: 60..84 (m0 == 1, controlled by register bit C only)
+  OC_DIAGT = 85,
+  OC_DIAGX = 86,
+  OC_DIAG = 87,
+  OC_SWAPS = 88,
+  OC_MAT2S = 89,
+  OC_GRADM = 90,      // + A: 90..93
+  OC_GRADD = 94,
+  OC_GRADM2 = 95,
+  OC_X1S = 96,        // X on tile bit b with controls ctile, through shared memory (multi-controlled X)
+  OC_CPHASE = 97,     // + A: 97..101, phase fan on register bit A
   OC_NOP = 0xFF       // continuation record: dispatched as an op that does nothing
 };
 
@@ -95,25 +101,24 @@ enum FOpCode : uint8_t {
 // bit A), each with at most one control, merged into one op.  Every amplitude
 // whose bit A is 1 is multiplied by
 //   T[k] * prod_{thread-id bits s set} H[s] * exp(i * sum_{terms: ctx & mask} angle)
-// where k is the slot index with bit A removed.  m[0..15] hold T[0..7]
-// (constant and register-bit controls), m[16..31] hold H[0..7] (lane bits
-// 0-4, warp bits 5-7).  The out-of-tile controls are (angle, global qubit
-// mask) pairs stored as double2 in the continuation records (FO_CONT) that
-// follow the op: each record has a 16-byte header that makes it a no-op
-// (OC_NOP, no controls) and 19 pairs after it; the op's `lmask` field holds the
-// number of pairs and `ctile` the number of records.
+// where k is the slot index with bit A removed.  m holds T[0 .. 2^(NR-1)-1]
+// (constant and register-bit controls).  Continuation records (FO_CONT) follow
+// the op; each has a 16-byte header that makes it a no-op (OC_NOP, no
+// controls).  Record 0 holds H[0..7] (lanes, then warps) after its header;
+// records 1.. hold the out-of-tile controls as (angle, global qubit mask)
+// double2 pairs, 19 per record.  The op's `lmask` field holds the number of
+// pairs and `ctile` the number of records.
 enum : int {
   KET_CPHASE_TERMS_PER_RECORD = 19
 };
 
-// Roles in a layout: 0..4 lane bits, 5..7 warp bits, 8..11 register bits.
 struct FOp {
   // bytes 0..15: everything the kernel needs to decide whether and how an op runs
   uint8_t opc;                // FOpCode
   uint8_t a;                  // target: register bit / lane bit / thread-id bit / tile bit (by type)
   uint8_t flags;
   uint8_t creg;               // controls on register bits (bit k = register bit k)
-  uint8_t cthr;               // controls on thread-id bits (lane bits 0-4, warp bits 5-7)
+  uint8_t cthr;               // controls on thread-id bits (lane bits 0-4, then the warp bits)
   int8_t d0, d1;              // FO_DIAG: tile bits of t0 (MSB) and t1, -1 = outside the tile
   uint8_t type;               // FOpType (host-side classification, used by the planner's tests)
   uint64_t cctx;              // controls on global bits outside the tile
@@ -156,6 +161,7 @@ struct Pass2Args {
   int* status;                     // device status word: set to KET_ERR_TIMEOUT if a bounded wait ran out
   double* gpart;                   // adjoint: per-CTA gradient partials [cta][slot][warp]
   int nslots;                      // adjoint: gradient probes in this pass
+  int nreg;                        // register bits of the layouts (4 or 5)
   int pairbit;                     // index into ctxbits of the qubit that tells apart the two tiles a
                                    // thread holds, -1 = one tile per thread (see choose_pairbit)
   // filled by launch_fused2 from the fields above:
@@ -166,13 +172,14 @@ struct Pass2Args {
 
 // Sum the adjoint partials of one pass: out[s] = sum over CTAs and warps (fixed order).
 cudaError_t launch_grad_reduce(const double* gpart, int nctas, int nslots, double* out, cudaStream_t s);
-int fused2_grid();
+// Persistent grid of the register-tiled pass for a register-bit count.
+int fused2_grid(int nreg);
 // A qubit outside the tile (index into a.ctxbits) that no op of the program
 // reads as a control or a diagonal target, or -1.
 int choose_pairbit(const std::vector<FOp>& prog, const Pass2Args& a);
 
 // Lower one fused pass to a register-tiled program (segments + exchanges).
-void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, std::vector<FOp>& prog,
+void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, int nreg, std::vector<FOp>& prog,
                   uint8_t load_pos[KET_T2_BITS], uint8_t store_pos[KET_T2_BITS]);
 cudaError_t launch_fused2(const Pass2Args& a, int precision, cudaStream_t s);
 

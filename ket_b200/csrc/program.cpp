@@ -21,9 +21,14 @@ namespace {
 const int NB = KET_T2_BITS;
 
 struct Lay {
-  int pos[NB];   // role -> tile bit: 0..4 lanes, 5..7 warps, 8..11 registers
+  int pos[NB];   // role -> tile bit: 0..4 lanes, then NW warps, then NR registers
   int role[NB];  // tile bit -> role
 };
+
+thread_local int g_nreg = 4;  // register bits of the program being lowered (4 or 5)
+inline int NRg() { return g_nreg; }
+inline int NWg() { return 7 - g_nreg; }
+inline int REG0() { return 5 + NWg(); }  // role of register bit 0
 
 void fill_roles(Lay& l) {
   for (int r = 0; r < NB; r++) l.role[l.pos[r]] = r;
@@ -35,7 +40,7 @@ bool a0_compatible(const Lay& l) {
   return true;
 }
 
-bool is_reg(const Lay& l, int tb) { return l.role[tb] >= 8; }
+bool is_reg(const Lay& l, int tb) { return l.role[tb] >= REG0(); }
 bool is_lane(const Lay& l, int tb) { return l.role[tb] < 5; }
 
 // Tile-local bit of a global qubit, -1 when outside the tile.
@@ -98,14 +103,14 @@ Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision)
   auto take_reg = [&](int b) { regs.push_back(b); used[b] = true; };
   if (a0) {
     for (int b = 0; b < 5; b++) { lanes.push_back(b); used[b] = true; }
-    for (int b : must) if (!used[b] && (int)regs.size() < 4) take_reg(b);
-    for (int b : order) if (!used[b] && (int)regs.size() < 4 && b >= 5) take_reg(b);
+    for (int b : must) if (!used[b] && (int)regs.size() < NRg()) take_reg(b);
+    for (int b : order) if (!used[b] && (int)regs.size() < NRg() && b >= 5) take_reg(b);
     for (int b : order) if (!used[b]) { warps.push_back(b); used[b] = true; }
   } else {
-    for (int b : must) if (!used[b] && (int)regs.size() < 4) take_reg(b);
+    for (int b : must) if (!used[b] && (int)regs.size() < NRg()) take_reg(b);
     // prefer registers for bits whose first use needs two registers
-    for (int b : order) if (!used[b] && (int)regs.size() < 4 && nreg[b]) take_reg(b);
-    for (int b : order) if (!used[b] && (int)regs.size() < 4) take_reg(b);
+    for (int b : order) if (!used[b] && (int)regs.size() < NRg() && nreg[b]) take_reg(b);
+    for (int b : order) if (!used[b] && (int)regs.size() < NRg()) take_reg(b);
     for (int b : order) if (!used[b] && (int)lanes.size() < 5) { lanes.push_back(b); used[b] = true; }
     for (int b = 0; b < NB; b++) if (!used[b]) { warps.push_back(b); used[b] = true; }
     // Shared-memory bank spread: the swizzle folds tile bits mod 3 (c128) or
@@ -120,14 +125,15 @@ Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision)
     for (int b : ln) out.push_back(b);
     lanes = out;
   }
-  // the adjoint ancilla always occupies register bit 3 (the kernel's probes
-  // address it at compile time)
+  // the adjoint ancilla always occupies the top register bit (the kernel's
+  // probes address it at compile time)
+  const int top = NRg() - 1;
   if (g_anc_tb >= 0)
-    for (int i = 0; i < 3; i++)
-      if (regs[i] == g_anc_tb) std::swap(regs[i], regs[3]);
+    for (int i = 0; i < top; i++)
+      if (regs[i] == g_anc_tb) std::swap(regs[i], regs[top]);
   for (int i = 0; i < 5; i++) l.pos[i] = lanes[i];
-  for (int i = 0; i < 3; i++) l.pos[5 + i] = warps[i];
-  for (int i = 0; i < 4; i++) l.pos[8 + i] = regs[i];
+  for (int i = 0; i < NWg(); i++) l.pos[5 + i] = warps[i];
+  for (int i = 0; i < NRg(); i++) l.pos[REG0() + i] = regs[i];
   fill_roles(l);
   return l;
 }
@@ -154,10 +160,10 @@ void controls(const Gate& g, const Pass& p, const Lay& l, FOp& o) {
     if (t < 0) { o.cctx |= uint64_t(1) << q; continue; }
     o.ctile |= 1u << t;
     int r = l.role[t];
-    if (r >= 8) {
-      o.creg |= (uint8_t)(1u << (r - 8));
+    if (r >= REG0()) {
+      o.creg |= (uint8_t)(1u << (r - REG0()));
     } else {
-      o.cthr |= (uint8_t)(1u << r);  // lanes 0..4 -> tid bits 0..4, warps 5..7 -> tid bits 5..7
+      o.cthr |= (uint8_t)(1u << r);  // lanes 0..4 -> tid bits 0..4, warps -> the tid bits above
       if (r < 5) {
         uint32_t lanes = 0;
         for (int ln = 0; ln < 32; ln++)
@@ -179,7 +185,7 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
     case G_MAT1: case G_X1: {
       bool reg = is_reg(l, t0);
       o.type = g.type == G_MAT1 ? (reg ? FO_MAT1R : FO_MAT1L) : (reg ? FO_X1R : FO_X1L);
-      o.a = (uint8_t)(reg ? l.role[t0] - 8 : l.role[t0]);
+      o.a = (uint8_t)(reg ? l.role[t0] - REG0() : l.role[t0]);
       o.b = (uint8_t)t0;  // tile bit (the shared-memory form of a multi-controlled X)
       bool real = true;
       for (int k = 0; k < 4; k++) {
@@ -214,18 +220,18 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
         o.dg0 = uint64_t(1) << g.t0;
       } else if (is_reg(l, t0)) {
         o.type = FO_DIAGR;
-        o.a = (uint8_t)(l.role[t0] - 8);
+        o.a = (uint8_t)(l.role[t0] - REG0());
       } else {
         o.type = FO_DIAGT;
-        o.a = (uint8_t)l.role[t0];  // lanes 0..4 -> tid bits 0..4, warps 5..7 -> tid bits 5..7
+        o.a = (uint8_t)l.role[t0];  // lanes 0..4 -> tid bits 0..4, warps -> the tid bits above
       }
       break;
     }
     case G_GRADM: {
       o.type = FO_GRADM;
       o.flags = 0;
-      o.a = (uint8_t)(l.role[t0] - 8);
-      o.b = (uint8_t)(l.role[g_anc_tb] - 8);
+      o.a = (uint8_t)(l.role[t0] - REG0());
+      o.b = (uint8_t)(l.role[g_anc_tb] - REG0());
       o.slot = (int16_t)g.slot;
       for (int k = 0; k < 4; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
       break;
@@ -233,10 +239,10 @@ FOp make_op(const Gate& g, const Pass& p, const Lay& l, bool prune) {
     case G_GRADD: {
       o.type = FO_GRADD;
       o.flags = 0;
-      o.b = (uint8_t)(l.role[g_anc_tb] - 8);
+      o.b = (uint8_t)(l.role[g_anc_tb] - REG0());
       o.slot = (int16_t)g.slot;
       if (t0 < 0) { o.flags |= FOF_TGT_CTX; o.dg0 = uint64_t(1) << g.t0; }
-      else if (is_reg(l, t0)) o.a = (uint8_t)(l.role[t0] - 8);
+      else if (is_reg(l, t0)) o.a = (uint8_t)(l.role[t0] - REG0());
       else { o.flags |= FOF_TGT_THR; o.a = (uint8_t)l.role[t0]; }
       for (int k = 0; k < 2; k++) { o.m[2 * k] = g.m[k].re; o.m[2 * k + 1] = g.m[k].im; }
       break;
@@ -290,8 +296,10 @@ void merge_phase_fans(std::vector<FOp>& prog) {
       continue;
     }
     const int A = prog[i].a;
-    cd T[8], H[8];
-    for (int k = 0; k < 8; k++) { T[k] = cd{1, 0}; H[k] = cd{1, 0}; }
+    const int nt = 1 << (NRg() - 1);  // slots with bit A set
+    cd T[16], H[8];
+    for (int k = 0; k < 16; k++) T[k] = cd{1, 0};
+    for (int k = 0; k < 8; k++) H[k] = cd{1, 0};
     std::vector<std::pair<uint64_t, double>> terms;  // (mask, angle)
     auto mul = [](cd a, cd b) { return cd{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; };
     for (size_t g = i; g < j; g++) {
@@ -307,7 +315,7 @@ void merge_phase_fans(std::vector<FOp>& prog) {
         for (int sb = 0; sb < 8; sb++)
           if (o.cthr == (1u << sb)) H[sb] = mul(H[sb], ph);
       } else {
-        for (int k = 0; k < 8; k++) {
+        for (int k = 0; k < nt; k++) {
           const int slot = ((k >> A) << (A + 1)) | (1 << A) | (k & ((1 << A) - 1));
           if ((slot & o.creg) == o.creg) T[k] = mul(T[k], ph);
         }
@@ -318,11 +326,8 @@ void merge_phase_fans(std::vector<FOp>& prog) {
     f.type = FO_CPHASE;
     f.a = (uint8_t)A;
     f.d0 = f.d1 = -2;
-    for (int k = 0; k < 8; k++) {
-      f.m[2 * k] = T[k].re; f.m[2 * k + 1] = T[k].im;
-      f.m[16 + 2 * k] = H[k].re; f.m[16 + 2 * k + 1] = H[k].im;
-    }
-    const size_t nrec = (terms.size() + KET_CPHASE_TERMS_PER_RECORD - 1) / KET_CPHASE_TERMS_PER_RECORD;
+    for (int k = 0; k < nt; k++) { f.m[2 * k] = T[k].re; f.m[2 * k + 1] = T[k].im; }
+    const size_t nrec = 1 + (terms.size() + KET_CPHASE_TERMS_PER_RECORD - 1) / KET_CPHASE_TERMS_PER_RECORD;
     f.lmask = (uint32_t)terms.size();
     f.ctile = (uint32_t)nrec;
     out.push_back(f);
@@ -333,11 +338,15 @@ void merge_phase_fans(std::vector<FOp>& prog) {
       c.type = FO_CONT;
       c.d0 = c.d1 = -2;
       double* d = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(&c) + 16);
-      for (size_t t = 0; t < KET_CPHASE_TERMS_PER_RECORD; t++) {
-        const size_t ti = r * KET_CPHASE_TERMS_PER_RECORD + t;
-        if (ti >= terms.size()) break;
-        d[2 * t] = terms[ti].second;
-        memcpy(&d[2 * t + 1], &terms[ti].first, 8);
+      if (r == 0) {
+        for (int k = 0; k < 8; k++) { d[2 * k] = H[k].re; d[2 * k + 1] = H[k].im; }
+      } else {
+        for (size_t t = 0; t < KET_CPHASE_TERMS_PER_RECORD; t++) {
+          const size_t ti = (r - 1) * KET_CPHASE_TERMS_PER_RECORD + t;
+          if (ti >= terms.size()) break;
+          d[2 * t] = terms[ti].second;
+          memcpy(&d[2 * t + 1], &terms[ti].first, 8);
+        }
       }
       out.push_back(c);
     }
@@ -353,7 +362,7 @@ void assign_opcode(FOp& o) {
   // a single control on a register bit (and none elsewhere) gets a compile-time variant
   int c1 = -1;
   if (o.creg && !(o.creg & (o.creg - 1)) && !o.cthr && !o.cctx)
-    for (int k = 0; k < 4; k++)
+    for (int k = 0; k < KET_NR_MAX; k++)
       if (o.creg == (1u << k)) c1 = k;
   switch (o.type) {
     case FO_EXCH: o.opc = OC_EXCH; break;
@@ -361,12 +370,12 @@ void assign_opcode(FOp& o) {
     case FO_MAT1L: o.opc = (uint8_t)(OC_MAT1L + (real ? 1 : rx ? 2 : 0)); break;
     case FO_X1R:
       if (!o.creg) o.opc = (uint8_t)(OC_X1R + o.a);
-      else if (c1 >= 0) o.opc = (uint8_t)(OC_X1RC + 4 * o.a + c1);
+      else if (c1 >= 0) o.opc = (uint8_t)(OC_X1RC + 5 * o.a + c1);
       else o.opc = OC_X1S;  // several controls, some on register bits: rare
       break;
     case FO_X1L: o.opc = OC_X1L; break;
     case FO_DIAGR:
-      if (d0one) o.opc = c1 >= 0 ? (uint8_t)(OC_DIAGR1C + 4 * o.a + c1) : (uint8_t)(OC_DIAGR1 + o.a);
+      if (d0one) o.opc = c1 >= 0 ? (uint8_t)(OC_DIAGR1C + 5 * o.a + c1) : (uint8_t)(OC_DIAGR1 + o.a);
       else o.opc = (uint8_t)(OC_DIAGR + o.a);
       break;
     case FO_DIAGT: o.opc = OC_DIAGT; break;
@@ -383,9 +392,10 @@ void assign_opcode(FOp& o) {
   }
 }
 
-void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, std::vector<FOp>& prog,
+void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, int nreg, std::vector<FOp>& prog,
                   uint8_t load_pos[KET_T2_BITS], uint8_t store_pos[KET_T2_BITS]) {
   prog.clear();
+  g_nreg = nreg;
   g_anc_tb = plan.anc >= 0 ? tpos(p, plan.anc) : -1;
   Lay cur = choose(plan, p, 0, true, precision);
   for (int i = 0; i < NB; i++) load_pos[i] = (uint8_t)cur.pos[i];

@@ -21,27 +21,31 @@ typedef std::complex<double> cx;
 
 namespace {
 
+// Thread/slot shape of the layouts being emulated: NR register bits, NW warp bits.
+int NR = KET_FUSED_NREG, NW = 7 - KET_FUSED_NREG, NTH = 32 << (7 - KET_FUSED_NREG), NS = 1 << KET_FUSED_NREG;
+
 struct Lay {
-  uint32_t tbase[256];
-  uint32_t rp[4];
+  std::vector<uint32_t> tbase;  // per thread
+  uint32_t rp[KET_NR_MAX];
 };
 
 Lay make_lay(const uint8_t* pos) {
   Lay L;
-  for (int t = 0; t < 256; t++) {
+  L.tbase.assign(NTH, 0);
+  for (int t = 0; t < NTH; t++) {
     int lane = t & 31, warp = t >> 5;
     uint32_t v = 0;
     for (int l = 0; l < 5; l++) v |= (uint32_t)((lane >> l) & 1) << pos[l];
-    for (int w = 0; w < 3; w++) v |= (uint32_t)((warp >> w) & 1) << pos[5 + w];
+    for (int w = 0; w < NW; w++) v |= (uint32_t)((warp >> w) & 1) << pos[5 + w];
     L.tbase[t] = v;
   }
-  for (int k = 0; k < 4; k++) L.rp[k] = 1u << pos[8 + k];
+  for (int k = 0; k < NR; k++) L.rp[k] = 1u << pos[5 + NW + k];
   return L;
 }
 
 uint32_t rofs(const Lay& L, int j) {
   uint32_t o = 0;
-  for (int k = 0; k < 4; k++)
+  for (int k = 0; k < NR; k++)
     if ((j >> k) & 1) o |= L.rp[k];
   return o;
 }
@@ -51,17 +55,21 @@ void prune(cx& a) {
   if (n2 < 1e-14) a = 0.0;
 }
 
-uint16_t slotmask(uint32_t creg) {
-  uint16_t v = 0;
-  for (int j = 0; j < 16; j++)
-    if (((uint32_t)j & creg) == creg) v |= (uint16_t)(1u << j);
+uint32_t slotmask(uint32_t creg) {
+  uint32_t v = 0;
+  for (int j = 0; j < NS; j++)
+    if (((uint32_t)j & creg) == creg) v |= 1u << j;
   return v;
+}
+
+const double* record_data(const std::vector<FOp>& prog, size_t k) {
+  return reinterpret_cast<const double*>(reinterpret_cast<const unsigned char*>(&prog[k]) + 16);
 }
 
 void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
   std::vector<FOp> prog;
   uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
-  plan_program(plan, p, KET_C128, prunef, prog, lp, sp);
+  plan_program(plan, p, KET_C128, prunef, NR, prog, lp, sp);
   const int L = p.L;
   auto gq = [&](int tb) { return tb < L ? tb : p.hbits[tb - L]; };
   uint64_t S = (uint64_t(1) << L) - 1;
@@ -70,7 +78,7 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
   for (int q = 0; q < n; q++)
     if (!((S >> q) & 1)) ctxbits.push_back(q);
   const uint64_t ntiles = uint64_t(1) << (n - KET_T2_BITS);
-  std::vector<cx> x(256 * 16), sm(4096);
+  std::vector<cx> x(NTH * NS), sm(4096);
   auto gaddr = [&](uint64_t ctx, uint32_t tidx) {
     uint64_t g = ctx;
     for (int b = 0; b < KET_T2_BITS; b++)
@@ -82,54 +90,55 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
     for (size_t j = 0; j < ctxbits.size(); j++)
       if ((tile >> j) & 1) ctx |= uint64_t(1) << ctxbits[j];
     Lay Lc = make_lay(lp);
-    for (int t = 0; t < 256; t++)
-      for (int j = 0; j < 16; j++) x[t * 16 + j] = amp[gaddr(ctx, Lc.tbase[t] | rofs(Lc, j))];
+    for (int t = 0; t < NTH; t++)
+      for (int j = 0; j < NS; j++) x[t * NS + j] = amp[gaddr(ctx, Lc.tbase[t] | rofs(Lc, j))];
     for (size_t oi = 0; oi < prog.size(); oi++) {
       const FOp& op = prog[oi];
       if (op.type == FO_CPHASE) {
         // phase fan on register bit a: T[k] * prod H[thread bits] * exp(i sum ctx angles)
+        const double* H = record_data(prog, oi + 1);
         double th = 0.0;
         for (uint32_t t = 0; t < op.lmask; t++) {
           const size_t rec = t / KET_CPHASE_TERMS_PER_RECORD, w = t % KET_CPHASE_TERMS_PER_RECORD;
-          const double* rd = reinterpret_cast<const double*>(reinterpret_cast<const unsigned char*>(&prog[oi + 1 + rec]) + 16);
+          const double* rd = record_data(prog, oi + 2 + rec);
           uint64_t mk;
           memcpy(&mk, &rd[2 * w + 1], 8);
           if (ctx & mk) th += rd[2 * w];
         }
         const cx E = std::polar(1.0, th);
-        for (int t = 0; t < 256; t++) {
+        for (int t = 0; t < NTH; t++) {
           cx F = E;
           for (int sb = 0; sb < 8; sb++)
-            if ((t >> sb) & 1) F *= cx(op.m[16 + 2 * sb], op.m[17 + 2 * sb]);
-          for (int j = 0; j < 16; j++) {
+            if ((t >> sb) & 1) F *= cx(H[2 * sb], H[2 * sb + 1]);
+          for (int j = 0; j < NS; j++) {
             if (!((j >> op.a) & 1)) continue;
             const int k = ((j >> (op.a + 1)) << op.a) | (j & ((1 << op.a) - 1));
-            x[t * 16 + j] *= cx(op.m[2 * k], op.m[2 * k + 1]) * F;
+            x[t * NS + j] *= cx(op.m[2 * k], op.m[2 * k + 1]) * F;
           }
         }
         oi += op.ctile;
         continue;
       }
       if (op.type == FO_EXCH) {
-        for (int t = 0; t < 256; t++)
-          for (int j = 0; j < 16; j++) sm[Lc.tbase[t] | rofs(Lc, j)] = x[t * 16 + j];
+        for (int t = 0; t < NTH; t++)
+          for (int j = 0; j < NS; j++) sm[Lc.tbase[t] | rofs(Lc, j)] = x[t * NS + j];
         Lc = make_lay(op.pos);
-        for (int t = 0; t < 256; t++)
-          for (int j = 0; j < 16; j++) x[t * 16 + j] = sm[Lc.tbase[t] | rofs(Lc, j)];
+        for (int t = 0; t < NTH; t++)
+          for (int j = 0; j < NS; j++) x[t * NS + j] = sm[Lc.tbase[t] | rofs(Lc, j)];
         continue;
       }
       if ((ctx & op.cctx) != op.cctx) continue;
       const bool pr = op.flags & FOF_PRUNE;
       const cx m0(op.m[0], op.m[1]), m1(op.m[2], op.m[3]), m2(op.m[4], op.m[5]), m3(op.m[6], op.m[7]);
       std::vector<cx> nx = x;
-      for (int t = 0; t < 256; t++) {
-        const uint32_t sm_ = ((uint32_t)(t & op.cthr) == op.cthr) ? slotmask(op.creg & 15) : 0;
-        cx* xt = &x[t * 16];
-        cx* nt = &nx[t * 16];
+      for (int t = 0; t < NTH; t++) {
+        const uint32_t sm_ = ((uint32_t)(t & op.cthr) == op.cthr) ? slotmask(op.creg) : 0;
+        cx* xt = &x[t * NS];
+        cx* nt = &nx[t * NS];
         const int lane = t & 31;
         switch (op.type) {
           case FO_MAT1R: case FO_X1R:
-            for (int j = 0; j < 16; j++) {
+            for (int j = 0; j < NS; j++) {
               if ((j >> op.a) & 1) continue;
               int j1 = j | (1 << op.a);
               if (!((sm_ >> j) & 1)) continue;
@@ -140,8 +149,8 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
             break;
           case FO_MAT1L: case FO_X1L: {
             int bitv = (lane >> op.a) & 1;
-            const cx* pt = &x[(t ^ (1 << op.a)) * 16];
-            for (int j = 0; j < 16; j++) {
+            const cx* pt = &x[(t ^ (1 << op.a)) * NS];
+            for (int j = 0; j < NS; j++) {
               if (!((sm_ >> j) & 1)) continue;
               if (op.type == FO_X1L) { nt[j] = pt[j]; continue; }
               nt[j] = bitv ? (m2 * pt[j] + m3 * xt[j]) : (m0 * xt[j] + m1 * pt[j]);
@@ -149,18 +158,18 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
             break;
           }
           case FO_DIAGR:
-            for (int j = 0; j < 16; j++)
+            for (int j = 0; j < NS; j++)
               if ((sm_ >> j) & 1) nt[j] = ((j >> op.a) & 1 ? m1 : m0) * xt[j];
             break;
           case FO_DIAGT: case FO_DIAGX: {
             bool one = op.type == FO_DIAGT ? ((t >> op.a) & 1) : ((ctx & op.dg0) != 0);
-            for (int j = 0; j < 16; j++)
+            for (int j = 0; j < NS; j++)
               if ((sm_ >> j) & 1) nt[j] = (one ? m1 : m0) * xt[j];
             break;
           }
           case FO_DIAG: {
             // d0, d1: tile bits, -1 = outside the tile; controls as a tile-bit mask
-            for (int j = 0; j < 16; j++) {
+            for (int j = 0; j < NS; j++) {
               uint32_t idx = Lc.tbase[t] | rofs(Lc, j);
               if ((idx & op.ctile) != op.ctile) continue;
               int k0 = op.d0 >= 0 ? (int)((idx >> op.d0) & 1) : (int)((ctx & op.dg0) != 0);
@@ -174,8 +183,8 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
         }
       }
       if (op.type == FO_SWAPS || op.type == FO_MAT2S) {
-        for (int t = 0; t < 256; t++)
-          for (int j = 0; j < 16; j++) sm[Lc.tbase[t] | rofs(Lc, j)] = x[t * 16 + j];
+        for (int t = 0; t < NTH; t++)
+          for (int j = 0; j < NS; j++) sm[Lc.tbase[t] | rofs(Lc, j)] = x[t * NS + j];
         const int ta = op.a, tb = op.b, lo = ta < tb ? ta : tb, hi = ta < tb ? tb : ta;
         for (uint32_t g = 0; g < 1024; g++) {
           uint32_t lo_m = (1u << lo) - 1;
@@ -193,8 +202,8 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
             sm[idx[r]] = y;
           }
         }
-        for (int t = 0; t < 256; t++)
-          for (int j = 0; j < 16; j++) nx[t * 16 + j] = sm[Lc.tbase[t] | rofs(Lc, j)];
+        for (int t = 0; t < NTH; t++)
+          for (int j = 0; j < NS; j++) nx[t * NS + j] = sm[Lc.tbase[t] | rofs(Lc, j)];
         x = nx;
         continue;
       }
@@ -203,8 +212,8 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
       x = nx;
     }
     Lay Ls = make_lay(sp);
-    for (int t = 0; t < 256; t++)
-      for (int j = 0; j < 16; j++) amp[gaddr(ctx, Ls.tbase[t] | rofs(Ls, j))] = x[t * 16 + j];
+    for (int t = 0; t < NTH; t++)
+      for (int j = 0; j < NS; j++) amp[gaddr(ctx, Ls.tbase[t] | rofs(Ls, j))] = x[t * NS + j];
   }
 }
 
@@ -215,8 +224,12 @@ extern "C" {
 // Apply ops to the n-qubit state re_im (interleaved) through the planner's
 // fused programs, emulated.  Returns 0, or the lowering status; passes[0] =
 // emulated register-tiled passes, passes[1] = other passes (not emulated: -1).
-int emu_apply(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int prune, int fusion,
-              double* re_im, int64_t* passes) {
+int emu_apply_nreg(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int prune, int fusion,
+                   double* re_im, int64_t* passes, int nreg) {
+  NR = nreg;
+  NW = 7 - nreg;
+  NTH = 32 << NW;
+  NS = 1 << NR;
   Plan plan;
   std::string err;
   int rc = lower_ops(n, ops, nops, mats, nmat, prune != 0, plan.gates, err);
@@ -231,5 +244,10 @@ int emu_apply(int n, const ket_op* ops, size_t nops, const double* mats, size_t 
     passes[0]++;
   }
   return 0;
+}
+
+int emu_apply(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int prune, int fusion,
+              double* re_im, int64_t* passes) {
+  return emu_apply_nreg(n, ops, nops, mats, nmat, prune, fusion, re_im, passes, KET_FUSED_NREG);
 }
 }

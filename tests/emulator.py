@@ -26,19 +26,20 @@ def lib():
                         "-o", OUT, *SRCS], check=True)
     L = C.CDLL(OUT)
     from ket_b200._lib import ket_op
-    L.emu_apply.restype = C.c_int
-    L.emu_apply.argtypes = [C.c_int, C.POINTER(ket_op), C.c_size_t, C.POINTER(C.c_double), C.c_size_t, C.c_int,
-                            C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    L.emu_apply_nreg.restype = C.c_int
+    L.emu_apply_nreg.argtypes = [C.c_int, C.POINTER(ket_op), C.c_size_t, C.POINTER(C.c_double), C.c_size_t, C.c_int,
+                                 C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
     _lib = L
     return L
 
 
-def emu_apply(n, ops, init_state, prune=True, fusion=-1):
+def emu_apply(n, ops, init_state, prune=True, fusion=-1, nreg=5):
+    """nreg: register bits of the emulated layouts (5: ordinary passes, 4: adjoint passes)."""
     from ket_b200.circuit import ops_to_abi
     arr, m, k = ops_to_abi(ops)
     st = np.ascontiguousarray(init_state, dtype=np.complex128).copy()
     passes = (C.c_int64 * 2)()
     mv = np.ascontiguousarray(m).view(np.float64)
-    rc = lib().emu_apply(n, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, 1 if prune else 0, fusion,
-                         st.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)), passes)
+    rc = lib().emu_apply_nreg(n, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, 1 if prune else 0, fusion,
+                              st.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)), passes, nreg)
     return rc, st, list(passes)

@@ -12,7 +12,8 @@ from test_gpu_parity import build_both, random_gates
 
 @pytest.mark.parametrize("n,seed", [(12, 1), (13, 2), (14, 3), (15, 4), (16, 5)])
 @pytest.mark.parametrize("prune", [False, True])
-def test_emulated_programs_match_oracle(n, seed, prune):
+@pytest.mark.parametrize("nreg", [5, 4])
+def test_emulated_programs_match_oracle(n, seed, prune, nreg):
     from oracle import oracle as O
     gates = random_gates(n, 90, seed, unitary=False)
     kc, oc = build_both(n, gates)
@@ -20,21 +21,22 @@ def test_emulated_programs_match_oracle(n, seed, prune):
     st0 = np.zeros(1 << n, complex)
     st0[init] = 1
     from ket_b200.circuit import flatten_ops
-    rc, got, passes = emu_apply(n, flatten_ops(kc.ops), st0, prune=prune)
+    rc, got, passes = emu_apply(n, flatten_ops(kc.ops), st0, prune=prune, nreg=nreg)
     assert rc == 0 and passes[0] > 0
     want = oc.simulate(init=init, mode=O.DENSE_PRUNE if prune else O.DENSE).dense()
     assert np.max(np.abs(got - want)) < 1e-12
 
 
 @pytest.mark.parametrize("n", [14, 16])
-def test_emulated_brickwork_qft(n):
+@pytest.mark.parametrize("nreg", [5, 4])
+def test_emulated_brickwork_qft(n, nreg):
     from ket_b200 import workloads as W
     from ket_b200.circuit import flatten_ops
     from oracle import oracle as O
     c, _ = W.brickwork_qft(n, 8, 42)
     st0 = np.zeros(1 << n, complex)
     st0[0] = 1
-    rc, got, passes = emu_apply(n, flatten_ops(c.ops), st0, prune=False)
+    rc, got, passes = emu_apply(n, flatten_ops(c.ops), st0, prune=False, nreg=nreg)
     oc, _ = O.brickwork(n, 8, 42, with_qft=True)
     assert rc == 0
     assert np.max(np.abs(got - oc.simulate(mode=O.DENSE).dense())) < 1e-12
