@@ -260,6 +260,12 @@ KET_API int ket_shift_gradient(ket_ctx* ctx, int nqubits, uint64_t init, const k
  * sum_edges (1 - <Z_u Z_v>)/2 in FP64.  This equals vqe(qaoa(n, E, -2*gamma, beta),
  * maxCutHamiltonian(n, E)) of algorithms.ts:231-276.  All instances run in one
  * persistent launch (captured in a CUDA graph and replayed when use_graph = 1). */
+/* Launch shape of ket_batch_qaoa on this context: block_threads in {128, 256,
+ * 512} threads per CTA and tile_bits in {11, 12} (instances up to tile_bits
+ * qubits run whole in shared memory; wider ones, up to 2 * tile_bits qubits,
+ * as tiled passes).  0 selects the default (256, 12).  The autotuner in
+ * ket_b200/autotune.py picks them per workload.  No counterpart in the reference. */
+KET_API int ket_batch_config(ket_ctx* ctx, int block_threads, int tile_bits);
 KET_API int ket_batch_qaoa(ket_ctx* ctx, int ninst, const int* n, const int* ne, const int64_t* eoff, const int* edges,
                    int p, const double* gamma, const double* beta, int use_graph, double* out);
 

@@ -72,6 +72,7 @@ def lib():
             "ket_exec_opts_default": (None, [P(ket_exec_opts)]),
             "ket_debug_fail_alloc": (i32, [i32]),
             "ket_debug_batch_hook": (i32, [i32, C.c_uint32]),
+            "ket_batch_config": (i32, [vp, i32, i32]),
             "ket_ctx_create": (i32, [i32, P(vp)]),
             "ket_ctx_destroy": (i32, [vp]),
             "ket_ctx_scratch_bytes": (i32, [vp, P(u64)]),

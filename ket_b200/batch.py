@@ -18,10 +18,20 @@ from ._lib import check, default_ctx, lib
 
 
 def batch_qaoa(instances: Sequence[Tuple[int, Sequence[Tuple[int, int]], Sequence[float], Sequence[float]]],
-               use_graph: bool = True) -> np.ndarray:
-    """Expected cut <C> of every instance (n, edges, gamma, beta)."""
+               use_graph: bool = True, tune: bool = False) -> np.ndarray:
+    """Expected cut <C> of every instance (n, edges, gamma, beta).  tune: pick
+    the launch shape with the autotuner (ket_b200/autotune.py), timing the
+    candidates on this batch the first time a batch of its shape is seen."""
     if not instances:
         return np.zeros(0)
+    if tune:
+        from . import autotune
+        cfg = autotune.cached_batch_config(instances) or autotune.tune_batch_qaoa(instances)
+        autotune.set_batch_config(cfg["block_threads"], cfg["tile_bits"])
+    return _run(instances, use_graph)
+
+
+def _run(instances, use_graph: bool) -> np.ndarray:
     p = len(instances[0][2])
     ns, nes, eoff, edges, gam, bet = [], [], [], [], [], []
     for n, e, g, b in instances:

@@ -243,6 +243,54 @@ uint32_t g_spin_limit = 1u << 24;
 
 using namespace ket;
 
+// Launch the persistent batch kernel with NT threads per CTA (every CTA
+// resident at once) and its fixed-order reduction, captured in a CUDA graph
+// when use_graph is set.
+template <int NT>
+static cudaError_t run_batch(ket_ctx* c, const QArgs& a, size_t smem, int ninst, double* dout, int use_graph) {
+  static bool attr = false;
+  if (!attr) {
+    const size_t smax = (16u << 12) + 16 * (KQ_MAX_EDGES + 1) + 8 * KQ_MAX_EDGES + 8 * 32;
+    cudaFuncSetAttribute(k_batch_qaoa<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+    attr = true;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_qaoa<NT>, NT, smem);
+  per_sm = std::max(1, per_sm);
+  const int grid = num_sms() * per_sm;
+  auto record = [&]() -> cudaError_t {
+    cudaMemsetAsync(a.next, 0, 4 * ((size_t)ninst + 2), c->stream);
+    k_batch_qaoa<NT><<<grid, NT, smem, c->stream>>>(a);
+    k_qaoa_reduce<<<(ninst + 127) / 128, 128, 0, c->stream>>>(a.inst, ninst, a.part, dout);
+    return cudaGetLastError();
+  };
+  if (!use_graph) return record();
+  cudaGraph_t graph;
+  cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  e = record();
+  cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+  if (e != cudaSuccess) return e;
+  if (e2 != cudaSuccess) return e2;
+  if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+  e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return e;
+  return cudaGraphLaunch(c->graph_exec, c->stream);
+}
+
+extern "C" int ket_batch_config(ket_ctx* c, int block_threads, int tile_bits) {
+  if (!c) return fail(KET_ERR_TYPE, "null context");
+  if (block_threads == 0) block_threads = 256;
+  if (tile_bits == 0) tile_bits = 12;
+  if (block_threads != 128 && block_threads != 256 && block_threads != 512)
+    return fail(KET_ERR_TYPE, "block_threads must be 128, 256 or 512");
+  if (tile_bits != 11 && tile_bits != 12) return fail(KET_ERR_TYPE, "tile_bits must be 11 or 12");
+  c->batch_threads = block_threads;
+  c->batch_tile = tile_bits;
+  return KET_OK;
+}
+
 extern "C" int ket_debug_batch_hook(int drop_item, uint32_t spin_limit) {
   g_drop_item = drop_item;
   g_spin_limit = spin_limit ? spin_limit : (1u << 24);
@@ -257,14 +305,15 @@ extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne
   if (ninst < 0 || p < 0 || p > KQ_MAX_P) return fail(KET_ERR_TYPE, "bad instance count or layer count");
   if (ninst == 0) return KET_OK;
   cudaSetDevice(c->device);
-  const int T = 12, NT = 256;
+  const int T = c->batch_tile;
   std::vector<QInst> inst(ninst);
   std::vector<uint64_t> masks;
   int64_t work = 0, parts = 0, nedges = 0;
   for (int i = 0; i < ninst; i++) {
     if (n[i] < 1 || n[i] > 30) return fail(KET_ERR_RANGE, "instance qubit count out of range (1..30)");
     if (ne[i] < 0 || ne[i] > KQ_MAX_EDGES) return fail(KET_ERR_TYPE, "instance edge count out of range (0..64)");
-    if (n[i] > T && n[i] - T > T) return fail(KET_ERR_UNSUPPORTED, "instances wider than 24 qubits");
+    if (n[i] > T && n[i] - T > T)
+      return fail(KET_ERR_UNSUPPORTED, "instance wider than twice the tile width (" + std::to_string(2 * T) + " qubits)");
     QInst& I = inst[i];
     I.n = n[i];
     I.ne = ne[i];
@@ -345,39 +394,13 @@ extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne
   a.nitems = (int)items.size();
   a.tile = T;
   const size_t smem = (16u << T) + 16 * (KQ_MAX_EDGES + 1) + 8 * KQ_MAX_EDGES + 8 * 32;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_batch_qaoa<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_qaoa<NT>, NT, smem);
-  per_sm = std::max(1, per_sm);
-  const int grid = num_sms() * per_sm;  // persistent: every CTA resident at once
   double* dout = (double*)(base + off_out);
-  auto record = [&]() -> cudaError_t {
-    cudaMemsetAsync(a.next, 0, 4 * ((size_t)ninst + 2), c->stream);
-    k_batch_qaoa<NT><<<grid, NT, smem, c->stream>>>(a);
-    k_qaoa_reduce<<<(ninst + 127) / 128, 128, 0, c->stream>>>(a.inst, ninst, a.part, dout);
-    return cudaGetLastError();
-  };
-  cudaError_t e;
   prof_begin(c);
-  if (use_graph) {
-    cudaGraph_t graph;
-    e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
-    e = record();
-    cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
-    if (e != cudaSuccess) return cuda_fail(e, "batch capture");
-    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
-    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
-    e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
-    e = cudaGraphLaunch(c->graph_exec, c->stream);
-  } else {
-    e = record();
+  cudaError_t e;
+  switch (c->batch_threads) {
+    case 128: e = run_batch<128>(c, a, smem, ninst, dout, use_graph); break;
+    case 512: e = run_batch<512>(c, a, smem, ninst, dout, use_graph); break;
+    default: e = run_batch<256>(c, a, smem, ninst, dout, use_graph); break;
   }
   prof_end(c, PK_BATCH);
   c->launches += 1;  // the reduction (prof_end counted the batch kernel)

@@ -29,6 +29,8 @@ struct ket_ctx {
   std::vector<cudaEvent_t> ev_pool;
   std::vector<int> prof_kind;     // kind of each timed launch
   size_t prof_next = 0;           // next free event pair
+  int batch_threads = 256;        // ket_batch_qaoa: threads per CTA (set by ket_batch_config)
+  int batch_tile = 12;            // ket_batch_qaoa: tile width in qubits
 };
 
 struct ket_state {

@@ -53,3 +53,29 @@ def test_batch_qaoa_wide_instances():
     got = batch_qaoa(inst)
     for (n, e, g, b), v in zip(inst, got):
         assert abs(v - oracle_cut(n, e, g, b)) < 1e-10
+
+
+def test_every_launch_shape_gives_the_same_cuts(tmp_path, monkeypatch):
+    """The autotuner's candidates (threads per CTA x tile width) change how the
+    work is cut, not the result; the tuner caches its pick per batch shape."""
+    from ket_b200 import autotune, workloads as W
+    from ket_b200.batch import batch_qaoa
+    monkeypatch.setenv("KET_B200_CACHE", str(tmp_path))
+    inst = W.qaoa_batch(48, p=2, seed=5, sizes=(10, 12, 14, 16, 18))
+    try:
+        ref = None
+        for nt, tb in autotune.CANDIDATES:
+            autotune.set_batch_config(nt, tb)
+            got = batch_qaoa(inst, use_graph=True)
+            if ref is None:
+                ref = got
+            assert np.max(np.abs(got - ref)) < 1e-11, (nt, tb)
+        for (n, e, g, b), v in list(zip(inst, ref))[:6]:
+            assert abs(v - oracle_cut(n, e, g, b)) < 1e-11
+        res = autotune.tune_batch_qaoa(inst, repeats=1)
+        assert (res["block_threads"], res["tile_bits"]) in autotune.CANDIDATES
+        assert autotune.cached_batch_config(inst)["block_threads"] == res["block_threads"]
+        tuned = batch_qaoa(inst, tune=True)
+        assert np.max(np.abs(tuned - ref)) < 1e-11
+    finally:
+        autotune.set_batch_config(0, 0)
