@@ -54,8 +54,9 @@ typedef enum ket_status {
 
 typedef enum ket_precision { KET_C128 = 0, KET_C64 = 1 } ket_precision;
 
-/* Op kinds: the FlatOp union of src/circuit.ts:20-47 (measure/reset/if are
- * rejected: the pure path never sees them, src/circuit.ts:1432-1438). */
+/* Op kinds: the FlatOp union of src/circuit.ts:20-47.  measure / reset / if
+ * are accepted only by ket_run_shots (the pure path never sees them,
+ * src/circuit.ts:1432-1438). */
 typedef enum ket_op_kind {
   KET_OP_SINGLE = 0,      /* q[0];            2x2 matrix   (applySingle, statevector.ts:47)      */
   KET_OP_CNOT = 1,        /* q = {c, t}                    (applyCNOT, :70)                      */
@@ -66,7 +67,12 @@ typedef enum ket_op_kind {
   KET_OP_CSWAP = 6,       /* q = {c, a, b}                 (applyCSwap, :153)                    */
   KET_OP_CSRSWAP = 7,     /* q = {c, a, b}                 (applyCsrSwap, :177)                  */
   KET_OP_UNITARY = 8,     /* q[0..nq-1], q[0] = MSB; 2^nq x 2^nq (applyUnitary, :240)           */
-  KET_OP_BARRIER = 9      /* no effect on the state                                               */
+  KET_OP_BARRIER = 9,     /* no effect on the state                                               */
+  KET_OP_MEASURE = 10,    /* q = {qubit, classical bit or -1 (not recorded)} (applyOps, circuit.ts:184-190) */
+  KET_OP_RESET = 11,      /* q = {qubit}                   (circuit.ts:191-196)                  */
+  KET_OP_IF = 12          /* q = {first classical bit, register size (<= 31), value, body length};
+                             the body is the next `body length` ops, nested ifs included
+                             (circuit.ts:197-199)                                                 */
 } ket_op_kind;
 
 #define KET_MAX_OP_QUBITS 10
@@ -87,6 +93,12 @@ typedef struct ket_exec_opts {
                           |a|^2 < 1e-14 is flushed to zero (statevector.ts:19-27); 0 = plain dense */
   int32_t reserved[6];
 } ket_exec_opts;
+
+/* NoiseParams (circuit.ts:213-221): depolarizing probability per single-qubit
+ * gate, per two-qubit gate, and the readout flip probability. */
+typedef struct ket_noise {
+  double p1, p2, pmeas;
+} ket_noise;
 
 typedef struct ket_ctx ket_ctx;
 typedef struct ket_state ket_state;
@@ -203,6 +215,23 @@ KET_API int ket_norm2(const ket_state* st, double* out);
  * (the last such entry's running sum is taken as 1.0).  For 2^n <= 2^22 the running
  * sum is accumulated in ascending index order, exactly as the reference does. */
 KET_API int ket_sample(const ket_state* st, const double* r, size_t shots, double threshold, uint64_t* out_idx);
+/* run()'s per-shot path (circuit.ts:3455-3481 over applyOps, :169-207): one
+ * trajectory per shot from |init>, using st as the device workspace (its
+ * qubit count and precision; its contents are overwritten).  ops may hold
+ * measure / reset / if (KET_OP_MEASURE...).  noise (NULL = none) adds the
+ * depolarizing Paulis of dep1 / dep2 (:289-304) after single-qubit gates and
+ * after cnot / controlled / swap / two, and the readout flips.  All shots
+ * share one xorshift32 stream whose state is *prng_state (makePrng,
+ * :813-819; 0 reads as 1), drawn in the reference's order; on return it holds
+ * the state after the last draw.  ncbits = classical bits of all registers,
+ * numbered consecutively.  Outputs per shot s: out_idx[s] = the sampled basis
+ * index after readout flips (sampleSV, :75-83), out_bits[s * ncbits + b] =
+ * classical bit b at the end of the shot.  P(q=1) is summed in a fixed device
+ * order where the reference sums in its Map's insertion order: the two agree
+ * up to rounding. */
+KET_API int ket_run_shots(ket_state* st, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
+                          const ket_noise* noise, uint64_t init, size_t shots, uint32_t* prng_state, int ncbits,
+                          uint64_t* out_idx, uint8_t* out_bits);
 /* Circuit.expectation(pauli) (circuit.ts:3728-3753): pauli[q] in "IXYZ" acts on qubit q. */
 KET_API int ket_expect_pauli(const ket_state* st, const char* pauli, double* out);
 /* vqe() energy (algorithms.ts:301-336): sum_t coeffs[t] <P_t>.  ops holds nterms

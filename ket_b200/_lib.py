@@ -18,6 +18,7 @@ KET_OK, KET_ERR_RANGE, KET_ERR_TYPE, KET_ERR_OOM, KET_ERR_CUDA, KET_ERR_TIMEOUT,
 KET_C128, KET_C64 = 0, 1
 
 OP_SINGLE, OP_CNOT, OP_SWAP, OP_TWO, OP_CONTROLLED, OP_TOFFOLI, OP_CSWAP, OP_CSRSWAP, OP_UNITARY, OP_BARRIER = range(10)
+OP_MEASURE, OP_RESET, OP_IF = 10, 11, 12  # ket_run_shots only
 MAX_OP_QUBITS = 10
 
 PG = {"rx": 0, "ry": 1, "rz": 2, "vz": 2, "u1": 3, "p": 3, "gpi": 4, "gpi2": 5, "crx": 6, "cry": 7, "crz": 8,
@@ -39,6 +40,10 @@ class KetError(RuntimeError):
 
 class ket_op(C.Structure):
     _fields_ = [("kind", C.c_int32), ("nq", C.c_int32), ("q", C.c_int32 * MAX_OP_QUBITS), ("mat", C.c_int64)]
+
+
+class ket_noise(C.Structure):
+    _fields_ = [("p1", C.c_double), ("p2", C.c_double), ("pmeas", C.c_double)]
 
 
 class ket_exec_opts(C.Structure):
@@ -101,6 +106,8 @@ def lib():
             "ket_marginal_dist": (i32, [vp, P(i32), i32, P(dbl)]),
             "ket_norm2": (i32, [vp, P(dbl)]),
             "ket_sample": (i32, [vp, P(dbl), sz, dbl, P(u64)]),
+            "ket_run_shots": (i32, [vp, P(ket_op), sz, P(dbl), sz, P(ket_noise), u64, sz, P(C.c_uint32), i32,
+                                    P(u64), P(C.c_uint8)]),
             "ket_expect_pauli": (i32, [vp, C.c_char_p, P(dbl)]),
             "ket_expect_pauli_sum": (i32, [vp, i32, P(dbl), C.c_char_p, P(dbl)]),
             "ket_adjoint_gradient": (i32, [vp, i32, u64, P(ket_op), sz, P(dbl), sz, P(ket_param_binding), sz,

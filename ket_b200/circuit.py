@@ -23,13 +23,39 @@ from typing import Callable, Dict, Iterable, List, NamedTuple, Optional, Sequenc
 import numpy as np
 
 from . import gates as G
-from ._lib import (KET_C128, KET_C64, OP_BARRIER, OP_CNOT, OP_CONTROLLED, OP_CSRSWAP, OP_CSWAP, OP_SINGLE, OP_SWAP,
-                   OP_TOFFOLI, OP_TWO, OP_UNITARY, RangeError, check, default_ctx, exec_opts, ket_op, lib)
+from ._lib import (KET_C128, KET_C64, OP_BARRIER, OP_CNOT, OP_CONTROLLED, OP_CSRSWAP, OP_CSWAP, OP_IF, OP_MEASURE,
+                   OP_RESET, OP_SINGLE, OP_SWAP, OP_TOFFOLI, OP_TWO, OP_UNITARY, RangeError, check, default_ctx,
+                   exec_opts, ket_noise, ket_op, lib)
 
 Number = Union[int, float]
 Param = Union[int, float, str]
 
 PRUNE = 1e-14  # statevector.ts:277 / complex.ts:24
+
+# Published device noise profiles (DEVICES, circuit.ts:228-245): p1, p2, pMeas.
+DEVICES = {
+    "aria-1": {"qubits": 25, "nativeGates": ("gpi", "gpi2", "ms", "vz"), "noise": {"p1": 0.0003, "p2": 0.005, "pMeas": 0.004}},
+    "forte-1": {"qubits": 36, "nativeGates": ("gpi", "gpi2", "ms", "vz", "zz"),
+                "noise": {"p1": 0.0001, "p2": 0.002, "pMeas": 0.002}},
+    "harmony": {"qubits": 11, "nativeGates": ("gpi", "gpi2", "ms", "vz"), "noise": {"p1": 0.001, "p2": 0.015, "pMeas": 0.01}},
+    "ibm_sherbrooke": {"qubits": 127, "noise": {"p1": 2.4e-4, "p2": 7.4e-3, "pMeas": 1.35e-2}},
+    "ibm_brisbane": {"qubits": 127, "noise": {"p1": 2.4e-4, "p2": 7.6e-3, "pMeas": 1.35e-2}},
+    "ibm_torino": {"qubits": 133, "noise": {"p1": 2.0e-4, "p2": 3.0e-3, "pMeas": 1.0e-2}},
+    "h1-1": {"qubits": 20, "noise": {"p1": 1.8e-5, "p2": 9.7e-4, "pMeas": 2.3e-3}},
+    "h2-1": {"qubits": 56, "noise": {"p1": 1.9e-5, "p2": 1.1e-3, "pMeas": 1.0e-3}},
+}
+
+
+def resolve_noise(noise):
+    """run()'s noise option (circuit.ts:3411-3418): None, a device name, or a
+    NoiseParams mapping {p1, p2, pMeas} -> (p1, p2, pMeas), or None."""
+    if noise is None:
+        return None
+    if isinstance(noise, str):
+        if noise not in DEVICES:
+            raise TypeError(f"Unknown device profile '{noise}'. Known: {', '.join(DEVICES)}")
+        noise = DEVICES[noise]["noise"]
+    return (float(noise.get("p1") or 0), float(noise.get("p2") or 0), float(noise.get("pMeas") or 0))
 
 
 class Op(NamedTuple):
@@ -382,8 +408,8 @@ class Circuit:
         return self._with(self._node, cregs=cr)
 
     def measure(self, q: int, creg: str, bit: int):
-        if q < 0 or q >= self.qubits:
-            raise RangeError(f"qubit index {q} is out of range for a {self.qubits}-qubit circuit")
+        # the reference's measure() does not check q (circuit.ts:1607-1615):
+        # a qubit outside the state reads 0
         cr = dict(self._cregs)
         cr[creg] = max(cr.get(creg, 0), bit + 1)
         return self._with(_Node(self._node, Op("measure", (q,), None, "measure", (), (creg, bit))), cregs=cr)
@@ -541,16 +567,40 @@ class Circuit:
             initialState: Optional[str] = None) -> Distribution:
         """run() pure fast path (circuit.ts:3406-3453): simulate once, sample shots
         by a lower-bound search of the ascending-index FP64 CDF."""
-        rng_draws = prng_draws(seed, shots)
+        nz = resolve_noise(noise)
         if initialState is not None:
             bitstring_to_index(initialState, self.qubits)
-        if noise is not None or any(op.kind in ("measure", "reset", "if") for op in self.ops):
-            raise NotImplementedError("the per-shot executor (noise, measure/reset/if) is not part of this engine")
+        if nz is not None or any(op.kind in ("measure", "reset", "if") for op in self.ops):
+            return self._run_pershot(shots, seed, nz, initialState)
+        rng_draws = prng_draws(seed, shots)
         idx = self._state(initialState).sample(rng_draws)
         counts: Dict[int, int] = {}
         for i in idx.tolist():
             counts[i] = counts.get(i, 0) + 1
         return Distribution(self.qubits, shots, counts, {name: [0.0] * size for name, size in self._cregs.items()})
+
+    def _run_pershot(self, shots: int, seed: Optional[int], nz, initialState: Optional[str]) -> Distribution:
+        """run()'s per-shot path (circuit.ts:3455-3481): one device trajectory
+        per shot through ket_run_shots, all shots drawing one makePrng stream."""
+        init = bitstring_to_index(initialState, self.qubits) if initialState is not None else 0
+        arr, m, k, ncbits, layout = shots_to_abi(self.ops, self._cregs)
+        st = DeviceState(self.qubits)
+        noise = ket_noise(*(nz if nz is not None else (0.0, 0.0, 0.0)))
+        state = C.c_uint32(make_prng(seed).state[0])
+        out_idx = np.zeros(max(shots, 1), dtype=np.uint64)
+        out_bits = np.zeros(max(shots * ncbits, 1), dtype=np.uint8)
+        mv = np.ascontiguousarray(m).view(np.float64)
+        check(lib().ket_run_shots(st.h, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size,
+                                  C.byref(noise) if nz is not None else None, init, shots, C.byref(state), ncbits,
+                                  out_idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                  out_bits.ctypes.data_as(C.POINTER(C.c_uint8))))
+        counts: Dict[int, int] = {}
+        for i in out_idx[:shots].tolist():
+            counts[i] = counts.get(i, 0) + 1
+        bits = out_bits[: shots * ncbits].reshape(shots, ncbits) if shots else np.zeros((0, ncbits), np.uint8)
+        cregs = {name: [float(bits[:, off + j].sum()) / shots if shots else 0.0 for j in range(size)]
+                 for name, (off, size) in layout.items()}
+        return Distribution(self.qubits, shots, counts, cregs)
 
     # ------------------------------------------------------------------ lowering to the C ABI
     def to_abi(self):
@@ -622,6 +672,25 @@ def _remap(op: Op, qmap) -> Op:
     return op._replace(qubits=tuple(qmap[i] for i in op.qubits))
 
 
+def _fill_gate(o, op: Op, mats: List[complex]):
+    o.kind = _KIND_CODE[op.kind]
+    qs = op.qubits
+    if len(qs) > 10:
+        if op.kind == "barrier":
+            qs = qs[:1]
+        else:
+            raise TypeError("op with more than 10 qubits is not supported")
+    o.nq = len(qs)
+    for j, qq in enumerate(qs):
+        o.q[j] = int(qq)
+    if op.gate is not None:
+        o.mat = len(mats)
+        for row in op.gate:
+            mats.extend(row)
+    else:
+        o.mat = -1
+
+
 def ops_to_abi(ops):
     """Lower flat ops to (ket_op array, matrix buffer, count)."""
     arr = (ket_op * max(1, len(ops)))()
@@ -630,27 +699,63 @@ def ops_to_abi(ops):
     for op in ops:
         if op.kind in ("measure", "reset", "if"):
             raise TypeError("pure path got a measure/reset/if op")
-        code = _KIND_CODE[op.kind]
-        o = arr[k]
-        o.kind = code
-        qs = op.qubits
-        if len(qs) > 10:
-            if op.kind == "barrier":
-                qs = qs[:1]
-            else:
-                raise TypeError("op with more than 10 qubits is not supported")
-        o.nq = len(qs)
-        for j, qq in enumerate(qs):
-            o.q[j] = int(qq)
-        if op.gate is not None:
-            o.mat = len(mats)
-            for row in op.gate:
-                mats.extend(row)
-        else:
-            o.mat = -1
+        _fill_gate(arr[k], op, mats)
         k += 1
     m = np.asarray(mats, dtype=np.complex128) if mats else np.zeros(1, dtype=np.complex128)
     return arr, m, k
+
+
+def shots_to_abi(ops, cregs: Dict[str, int]):
+    """Lower ops with measure / reset / if to ket_run_shots' encoding:
+    (ket_op array, matrix buffer, count, classical bits, {register: (first
+    bit, size)}).  Registers take consecutive bits in declaration order (the
+    Map order of the reference's #cregs).  An if-body follows its if op;
+    bodies are flattened as applyOps does when it runs them.  A measure into a
+    register the circuit does not hold -- one declared only inside an if body,
+    whose builder circuit the reference discards -- is not recorded."""
+    layout, nb = {}, 0
+    for name, size in cregs.items():
+        layout[name] = (nb, int(size))
+        nb += int(size)
+    entries = []
+
+    def lower(seq):
+        for op in flatten_ops(seq):
+            if op.kind == "measure":
+                creg, bit = op.extra
+                reg = layout.get(creg)
+                cb = reg[0] + bit if reg is not None and 0 <= bit < reg[1] else -1
+                entries.append((OP_MEASURE, (int(op.qubits[0]), cb)))
+            elif op.kind == "reset":
+                entries.append((OP_RESET, (int(op.qubits[0]),)))
+            elif op.kind == "if":
+                creg, value, body = op.extra
+                first, size = layout.get(creg, (0, 0))
+                if size > 31:
+                    raise NotImplementedError("if() on a register of more than 31 bits")
+                v = int(value) if float(value).is_integer() and -(1 << 31) <= value < (1 << 31) else -1
+                pos = len(entries)
+                entries.append(None)
+                lower(body)
+                entries[pos] = (OP_IF, (first, size, v, len(entries) - pos - 1))
+            else:
+                entries.append(op)
+
+    lower(ops)
+    arr = (ket_op * max(1, len(entries)))()
+    mats: List[complex] = []
+    for i, e in enumerate(entries):
+        if isinstance(e, Op):
+            _fill_gate(arr[i], e, mats)
+        else:
+            code, qs = e
+            arr[i].kind = code
+            arr[i].nq = len(qs)
+            for j, v in enumerate(qs):
+                arr[i].q[j] = v
+            arr[i].mat = -1
+    m = np.asarray(mats, dtype=np.complex128) if mats else np.zeros(1, dtype=np.complex128)
+    return arr, m, len(entries), nb, layout
 
 
 class DeviceState:

@@ -178,22 +178,31 @@ int ket_marginal_dist(const ket_state* s, const int* qubits, int m, double* out)
 }
 
 int ket_sample(const ket_state* s, const double* r, size_t shots, double thr, uint64_t* out) {
+  return ket::sample_indices(s, r, shots, thr, KET_SEQ_CDF_QUBITS, out);
+}
+
+}  // extern "C"
+
+namespace ket {
+
+int sample_indices(const ket_state* s, const double* r, size_t shots, double thr, int seq_qubits, uint64_t* out) {
   TRY(check_state(s));
   if (shots && (!r || !out)) return fail(KET_ERR_TYPE, "null argument");
   if (!shots) return KET_OK;
-  size_t need = sample_scratch(s->n) + 16 * shots + 1024;
+  size_t need = sample_scratch(s->n, seq_qubits) + 16 * shots + 1024;
   void* scr;
   TRY(ctx_scratch(s->ctx, need, &scr));
   double* dr = (double*)scr;
   uint64_t* dout = (uint64_t*)align_up((char*)(dr + shots), 256);
   void* work = align_up((char*)(dout + shots), 256);
   TRY(h2d(s->ctx, dr, r, 8 * shots));
-  TRY(LAUNCH_READ(s->ctx, launch_sample(s->amp, s->n, s->precision, thr, dr, shots, work, dout, s->ctx->stream)));
+  TRY(LAUNCH_READ(s->ctx, launch_sample(s->amp, s->n, s->precision, thr, seq_qubits, dr, shots, work, dout,
+                                         s->ctx->stream)));
   TRY(d2h(s->ctx, out, dout, 8 * shots));
   return ctx_wait(s->ctx);
 }
 
-}  // extern "C"
+}  // namespace ket
 
 namespace {
 

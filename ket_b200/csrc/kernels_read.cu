@@ -466,11 +466,11 @@ cudaError_t launch_marginal_dist(const void* amp, int n, int prec, const Margina
 }
 
 template <typename R>
-static cudaError_t sample_t(const void* amp, int n, double thr, const double* r, uint64_t shots, void* scratch,
-                            uint64_t* out, cudaStream_t s) {
+static cudaError_t sample_t(const void* amp, int n, double thr, int seq_qubits, const double* r, uint64_t shots,
+                            void* scratch, uint64_t* out, cudaStream_t s) {
   const typename Vec2<R>::T* a = (const typename Vec2<R>::T*)amp;
   const uint64_t N = uint64_t(1) << n;
-  if (n <= KET_SEQ_CDF_QUBITS) {
+  if (n <= seq_qubits || n < 10) {
     double* cum = (double*)scratch;
     uint64_t* last = (uint64_t*)(cum + N);
     k_cdf_sequential<R><<<1, 32, 0, s>>>(a, N, thr, cum, last);
@@ -491,16 +491,16 @@ static cudaError_t sample_t(const void* amp, int n, double thr, const double* r,
   }
   return cudaGetLastError();
 }
-size_t sample_scratch(int n) {
+size_t sample_scratch(int n, int seq_qubits) {
   uint64_t N = uint64_t(1) << n;
-  if (n <= KET_SEQ_CDF_QUBITS) return 8 * N + 64;
+  if (n <= seq_qubits || n < 10) return 8 * N + 64;
   uint64_t nc = N / 1024;
   return 8 * (3 * nc + 8);
 }
-cudaError_t launch_sample(const void* amp, int n, int prec, double thr, const double* r, uint64_t shots, void* scratch,
-                          uint64_t* out, cudaStream_t s) {
-  return prec == KET_C64 ? sample_t<float>(amp, n, thr, r, shots, scratch, out, s)
-                         : sample_t<double>(amp, n, thr, r, shots, scratch, out, s);
+cudaError_t launch_sample(const void* amp, int n, int prec, double thr, int seq_qubits, const double* r, uint64_t shots,
+                          void* scratch, uint64_t* out, cudaStream_t s) {
+  return prec == KET_C64 ? sample_t<float>(amp, n, thr, seq_qubits, r, shots, scratch, out, s)
+                         : sample_t<double>(amp, n, thr, seq_qubits, r, shots, scratch, out, s);
 }
 
 cudaError_t launch_gather(const void* amp, int prec, const uint64_t* idx, uint64_t k, double* out, cudaStream_t s) {

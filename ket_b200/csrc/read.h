@@ -43,8 +43,11 @@ cudaError_t launch_marginals(const void* amp, int n, int prec, double* partial, 
 int mdist_chunk_bits(int n, int m);
 cudaError_t launch_marginal_dist(const void* amp, int n, int prec, const MarginalSpec& spec, double* partial,
                                  double* out, cudaStream_t s);
-size_t sample_scratch(int n);
-cudaError_t launch_sample(const void* amp, int n, int prec, double thr, const double* r, uint64_t shots, void* scratch,
+// Sampling: a sequential FP64 CDF in index order (the reference's order) for
+// n <= seq_qubits, chunk sums and a per-draw walk inside one chunk above
+// that (seq_qubits >= 10: a chunk is 1024 amplitudes).
+size_t sample_scratch(int n, int seq_qubits);
+cudaError_t launch_sample(const void* amp, int n, int prec, double thr, int seq_qubits, const double* r, uint64_t shots, void* scratch,
                           uint64_t* out, cudaStream_t s);
 cudaError_t launch_gather(const void* amp, int prec, const uint64_t* idx, uint64_t k, double* out, cudaStream_t s);
 cudaError_t launch_pauli_group(const void* amp, int n, int prec, const PauliGroup& g, double* partial, double* out,

@@ -14,6 +14,9 @@
 //   src/circuit.ts:113-161        flattenOps / svFromBitstring / simulatePure
 //   src/circuit.ts:813-819        makePrng (xorshift32)
 //   src/circuit.ts:3406-3453      run() pure fast path (sort, CDF, lower bound)
+//   src/circuit.ts:55-81, :169-207, :289-304, :3455-3481
+//                                 the per-shot path: collapseQubit, sampleSV,
+//                                 applyOps (measure / reset / if), dep1 / dep2
 //   src/circuit.ts:1491-1518      amplitude / probability / marginals
 //   src/circuit.ts:3700-3753      exactProbs / expectation
 //   src/circuit.ts:1108-1146      #checkOp validation (RangeError / TypeError)
@@ -135,13 +138,18 @@ static Mat gMs(double p0, double p1) {
 }
 
 // ---------------------------------------------------------------- Op IR (circuit.ts:20-47)
-enum Kind { K_SINGLE, K_CNOT, K_SWAP, K_TWO, K_CONTROLLED, K_TOFFOLI, K_CSWAP, K_CSRSWAP, K_UNITARY, K_BARRIER };
+enum Kind { K_SINGLE, K_CNOT, K_SWAP, K_TWO, K_CONTROLLED, K_TOFFOLI, K_CSWAP, K_CSRSWAP, K_UNITARY, K_BARRIER,
+            K_MEASURE, K_RESET, K_IF };
 
 struct Op {
   Kind kind;
   std::vector<int> q;   // single:[q] cnot:[c,t] swap:[a,b] two:[a,b] controlled:[c,t]
                         // toffoli:[c1,c2,t] cswap/csrswap:[c,a,b] unitary: qs (qs[0]=MSB)
+                        // measure / reset: [q]
   Mat m;
+  int cbit = 0;                       // measure: classical bit (registers numbered consecutively)
+  int reg0 = 0, regn = 0, value = 0;  // if: the register's first bit and size, the compared value
+  std::vector<Op> body;               // if: the conditional ops
 };
 
 struct Circuit {
@@ -527,7 +535,7 @@ static void dense_apply(Dense& d, const Op& op) {
       }
       break;
     }
-    case K_BARRIER: break;
+    case K_BARRIER: case K_MEASURE: case K_RESET: case K_IF: break;
   }
 }
 
@@ -557,7 +565,7 @@ static State* simulate(const Circuit& c, uint64_t init, int mode) {
         case K_CSRSWAP: s->sv = applyCsrSwap(s->sv, op.q[0], op.q[1], op.q[2], s->ps); break;
         case K_TWO: s->sv = applyTwo(s->sv, op.q[0], op.q[1], op.m, s->ps); break;
         case K_UNITARY: s->sv = applyUnitary(s->sv, op.q, op.m, s->ps); break;
-        case K_BARRIER: break;
+        case K_BARRIER: case K_MEASURE: case K_RESET: case K_IF: break;
       }
     }
   } else {
@@ -620,6 +628,142 @@ static void run_shots(const State* s, int shots, uint32_t seed, uint64_t* out) {
     }
     out[i] = cum.empty() ? 0 : pr[lo].first;
   }
+}
+
+// ---------------------------------------------------------------- the per-shot path
+// Entries of a sparse state in ascending index order.
+static std::vector<std::pair<uint64_t, C>> sorted_entries(const SV& sv) {
+  std::vector<std::pair<uint64_t, C>> e(sv.begin(), sv.end());
+  std::sort(e.begin(), e.end(), [](const std::pair<uint64_t, C>& a, const std::pair<uint64_t, C>& b) {
+    return a.first < b.first;
+  });
+  return e;
+}
+
+// collapseQubit (circuit.ts:55-72).  P(q=1) is summed in ascending index
+// order; the reference sums in its Map's insertion order, which differs from
+// this only in rounding.
+static int collapse(SV& sv, int q, double rand) {
+  const uint64_t mask = (q >= 0 && q < 64) ? (uint64_t(1) << q) : 0;
+  const auto e = sorted_entries(sv);
+  double p1 = 0;
+  for (const auto& kv : e)
+    if (kv.first & mask) p1 += kv.second.re * kv.second.re + kv.second.im * kv.second.im;
+  const int outcome = rand < p1 ? 1 : 0;
+  const double inv = 1 / std::sqrt(outcome == 1 ? p1 : 1 - p1);
+  SV next;
+  next.reserve(e.size());
+  for (const auto& kv : e)
+    if (outcome == 1 ? (kv.first & mask) != 0 : (kv.first & mask) == 0)
+      next.emplace(kv.first, C{kv.second.re * inv, kv.second.im * inv});
+  sv = std::move(next);
+  return outcome;
+}
+
+// sampleSV (circuit.ts:75-83)
+static uint64_t sample_sv(const SV& sv, double rand) {
+  const auto e = sorted_entries(sv);
+  double cum = 0;
+  for (const auto& kv : e) {
+    cum += kv.second.re * kv.second.re + kv.second.im * kv.second.im;
+    if (rand <= cum) return kv.first;
+  }
+  return e.empty() ? 0 : e.back().first;
+}
+
+struct Noise { double p1, p2, pm; };
+
+// dep1 / dep2 (circuit.ts:289-304); TWO_PAULI order (:262-268), 0 = I
+static void dep1(SV& sv, int q, double p, double rand, PruneStats& ps) {
+  if (rand >= p) return;
+  const double r = rand / p;
+  if (r < 1.0 / 3) sv = applySingle(sv, q, gX(), ps);
+  else if (r < 2.0 / 3) sv = applySingle(sv, q, gY(), ps);
+  else sv = applySingle(sv, q, gZ(), ps);
+}
+static void dep2(SV& sv, int a, int b, double p, double rand, PruneStats& ps) {
+  if (rand >= p) return;
+  static const int pairs[15][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 0}, {1, 1}, {1, 2}, {1, 3}, {2, 0},
+                                   {2, 1}, {2, 2}, {2, 3}, {3, 0}, {3, 1}, {3, 2}, {3, 3}};
+  const int k = std::min((int)std::floor(rand / p * 15), 14);
+  Mat (*const pauli[4])() = {nullptr, gX, gY, gZ};
+  if (pairs[k][0]) sv = applySingle(sv, a, pauli[pairs[k][0]](), ps);
+  if (pairs[k][1]) sv = applySingle(sv, b, pauli[pairs[k][1]](), ps);
+}
+
+// applyOps (circuit.ts:169-207)
+static void apply_ops(const std::vector<Op>& ops, SV& sv, std::vector<uint8_t>& bits, Prng& rng, const Noise& nz,
+                      PruneStats& ps) {
+  for (const Op& op : ops) {
+    switch (op.kind) {
+      case K_SINGLE:
+        sv = applySingle(sv, op.q[0], op.m, ps);
+        if (nz.p1 != 0) dep1(sv, op.q[0], nz.p1, rng.next(), ps);
+        break;
+      case K_CNOT:
+        sv = applyCNOT(sv, op.q[0], op.q[1]);
+        if (nz.p2 != 0) dep2(sv, op.q[0], op.q[1], nz.p2, rng.next(), ps);
+        break;
+      case K_CONTROLLED:
+        sv = applyControlled(sv, op.q[0], op.q[1], op.m, ps);
+        if (nz.p2 != 0) dep2(sv, op.q[0], op.q[1], nz.p2, rng.next(), ps);
+        break;
+      case K_SWAP:
+        sv = applySWAP(sv, op.q[0], op.q[1]);
+        if (nz.p2 != 0) dep2(sv, op.q[0], op.q[1], nz.p2, rng.next(), ps);
+        break;
+      case K_TOFFOLI: sv = applyToffoli(sv, op.q[0], op.q[1], op.q[2]); break;
+      case K_CSWAP: sv = applyCSwap(sv, op.q[0], op.q[1], op.q[2]); break;
+      case K_CSRSWAP: sv = applyCsrSwap(sv, op.q[0], op.q[1], op.q[2], ps); break;
+      case K_TWO:
+        sv = applyTwo(sv, op.q[0], op.q[1], op.m, ps);
+        if (nz.p2 != 0) dep2(sv, op.q[0], op.q[1], nz.p2, rng.next(), ps);
+        break;
+      case K_UNITARY: sv = applyUnitary(sv, op.q, op.m, ps); break;
+      case K_MEASURE: {
+        const int outcome = collapse(sv, op.q[0], rng.next());
+        const int reported = (nz.pm != 0 && rng.next() < nz.pm) ? 1 - outcome : outcome;
+        bits[op.cbit] = (uint8_t)reported;
+        break;
+      }
+      case K_RESET:
+        if (collapse(sv, op.q[0], rng.next()) == 1) sv = applySingle(sv, op.q[0], gX(), ps);
+        break;
+      case K_IF: {
+        // cregValue (circuit.ts:164-166): the register as a little-endian integer
+        int v = 0;
+        for (int i = 0; i < op.regn; i++)
+          if (bits[op.reg0 + i]) v |= 1 << i;
+        if (v == op.value) apply_ops(op.body, sv, bits, rng, nz, ps);
+        break;
+      }
+      case K_BARRIER: break;
+    }
+  }
+}
+
+// run() per-shot path (circuit.ts:3455-3481): one trajectory per shot from
+// |init>; out_idx[s] = the sampled index after readout flips, out_bits[s *
+// ncbits + b] = classical bit b at the end of shot s.  Returns the stream's
+// state after the last draw.
+static uint32_t run_pershot(const Circuit& c, uint64_t init, int shots, uint32_t seed, const Noise& nz, int ncbits,
+                            uint64_t* out_idx, uint8_t* out_bits) {
+  Prng rng(seed);
+  PruneStats ps;
+  std::vector<uint8_t> bits(ncbits);
+  for (int i = 0; i < shots; i++) {
+    std::fill(bits.begin(), bits.end(), 0);
+    SV sv;
+    sv.emplace(init, ONE);
+    apply_ops(c.ops, sv, bits, rng, nz, ps);
+    uint64_t idx = sample_sv(sv, rng.next());
+    if (nz.pm != 0)
+      for (int q = 0; q < c.n; q++)
+        if (rng.next() < nz.pm) idx ^= uint64_t(1) << q;
+    out_idx[i] = idx;
+    for (int b = 0; b < ncbits; b++) out_bits[(size_t)i * ncbits + b] = bits[b];
+  }
+  return rng.s;
 }
 
 // ---------------------------------------------------------------- algorithms.ts
@@ -804,6 +948,46 @@ int orc_op_info(void* cp, int i, int* kind, int* qs, int* nq, double* mat, int m
   int m = (int)op.m.size();
   for (int j = 0; j < m && j < mat_cap; j++) { mat[2 * j] = op.m[j].re; mat[2 * j + 1] = op.m[j].im; }
   return m;
+}
+
+// Classical ops (circuit.ts:1598-1642).  measure takes any q, as the
+// reference's builder does not check it (an out-of-range qubit reads 0).
+int orc_add_measure(void* cp, int q, int cbit) {
+  Op op;
+  op.kind = K_MEASURE;
+  op.q = {q};
+  op.cbit = cbit;
+  ((Circuit*)cp)->ops.push_back(std::move(op));
+  return ORC_OK;
+}
+int orc_add_reset(void* cp, int q) {
+  Circuit& c = *(Circuit*)cp;
+  if (q < 0 || q >= c.n) {
+    g_err = "qubit index " + std::to_string(q) + " is out of range for a " + std::to_string(c.n) + "-qubit circuit";
+    return ORC_RANGE;
+  }
+  Op op;
+  op.kind = K_RESET;
+  op.q = {q};
+  c.ops.push_back(std::move(op));
+  return ORC_OK;
+}
+// if: the ops of `body` (a circuit) run when bits [reg0, reg0 + regn) read as
+// a little-endian integer equal value
+int orc_add_if(void* cp, int reg0, int regn, int value, void* body) {
+  Op op;
+  op.kind = K_IF;
+  op.reg0 = reg0;
+  op.regn = regn;
+  op.value = value;
+  op.body = ((Circuit*)body)->ops;
+  ((Circuit*)cp)->ops.push_back(std::move(op));
+  return ORC_OK;
+}
+// run() per-shot path; returns the xorshift32 state after the last draw
+uint32_t orc_run_pershot(void* cp, uint64_t init, int shots, uint32_t seed, double p1, double p2, double pm,
+                         int ncbits, uint64_t* out_idx, uint8_t* out_bits) {
+  return run_pershot(*(Circuit*)cp, init, shots, seed, Noise{p1, p2, pm}, ncbits, out_idx, out_bits);
 }
 
 void* orc_simulate(void* cp, uint64_t init, int mode) { return simulate(*(Circuit*)cp, init, mode); }
@@ -1025,7 +1209,7 @@ uint64_t orc_time_ops(void* cp, uint64_t init, int mode, int first, int count, d
         case K_CSRSWAP: s->sv = applyCsrSwap(s->sv, op.q[0], op.q[1], op.q[2], s->ps); break;
         case K_TWO: s->sv = applyTwo(s->sv, op.q[0], op.q[1], op.m, s->ps); break;
         case K_UNITARY: s->sv = applyUnitary(s->sv, op.q, op.m, s->ps); break;
-        case K_BARRIER: break;
+        case K_BARRIER: case K_MEASURE: case K_RESET: case K_IF: break;
       }
     }
   } else {

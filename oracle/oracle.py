@@ -81,6 +81,10 @@ def lib():
         "orc_regular3": (i32, [i32, P(u32), P(i32)]),
         "orc_prng_next": (u32, [P(u32)]),
         "orc_time_ops": (u64, [vp, u64, i32, i32, i32, P(dbl)]),
+        "orc_add_measure": (i32, [vp, i32, i32]),
+        "orc_add_reset": (i32, [vp, i32]),
+        "orc_add_if": (i32, [vp, i32, i32, i32, vp]),
+        "orc_run_pershot": (u32, [vp, u64, i32, u32, dbl, dbl, dbl, i32, P(u64), P(C.c_uint8)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -163,6 +167,31 @@ class OCircuit:
         m = self._L.orc_op_info(self.h_, i, C.byref(kind), _ip(qs), C.byref(nq), _dp(mat), 4096)
         mm = mat[: 2 * m].view(np.complex128).copy()
         return KIND_NAMES[kind.value], [int(x) for x in qs[: nq.value]], mm
+
+    # classical ops (circuit.ts:1598-1642); classical bits are numbered
+    # consecutively over all registers by the caller
+    def measure(self, q: int, cbit: int) -> "OCircuit":
+        self._raise(self._L.orc_add_measure(self.h_, q, cbit))
+        return self
+
+    def reset(self, q: int) -> "OCircuit":
+        self._raise(self._L.orc_add_reset(self.h_, q))
+        return self
+
+    def if_(self, reg0: int, regn: int, value: int, body: "OCircuit") -> "OCircuit":
+        self._raise(self._L.orc_add_if(self.h_, reg0, regn, value, body.h_))
+        return self
+
+    def run_pershot(self, shots: int, seed_state: int, p1=0.0, p2=0.0, pmeas=0.0, ncbits=0, init: int = 0):
+        """run() per-shot path (circuit.ts:3455-3481): (sampled index per shot,
+        classical bits per shot [shots, ncbits], xorshift32 state after the
+        last draw).  seed_state: the stream's state (makePrng: seed, 0 -> 1)."""
+        idx = np.zeros(max(shots, 1), dtype=np.uint64)
+        bits = np.zeros(max(shots * ncbits, 1), dtype=np.uint8)
+        st = self._L.orc_run_pershot(self.h_, init, shots, seed_state, p1, p2, pmeas, ncbits,
+                                     idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                     bits.ctypes.data_as(C.POINTER(C.c_uint8)))
+        return idx[:shots], bits[: shots * ncbits].reshape(shots, ncbits), int(st)
 
     def simulate(self, init: int = 0, mode: int = SPARSE) -> "OState":
         return OState(self._L.orc_simulate(self.h_, init, mode), self.qubits)

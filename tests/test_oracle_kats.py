@@ -10,7 +10,8 @@ import math
 import numpy as np
 import pytest
 
-from harness import bit_index, init_index, load_kats, oracle_circuit, tol
+from harness import (bit_index, check_pershot, init_index, load_kats, load_pershot_kats, oracle_circuit,
+                     pershot_oracle_raw, summarize, tol)
 from oracle import oracle as O
 
 CASES = load_kats()
@@ -128,3 +129,58 @@ def test_bounds_errors():
         O.OCircuit(2).add("cnot", [1, 1])
     with pytest.raises(O.OracleTypeError):
         O.OCircuit(2).add("crx", [0, 0], [0.5])
+
+
+PERSHOT = load_pershot_kats()
+
+
+def pure_oracle_probs(case):
+    """run()'s pure fast path on the case's gates with the same seed."""
+    c = O.OCircuit(case["n"])
+    for op in case["ops"]:
+        c.add(op[0], op[1], op[2])
+    idx = c.simulate().run(case["run"]["shots"], case["run"]["seed"])
+    probs = {}
+    for i in idx.tolist():
+        k = format(int(i), "b").zfill(case["n"])[::-1]
+        probs[k] = probs.get(k, 0) + 1 / len(idx)
+    return probs
+
+
+@pytest.mark.parametrize("case", PERSHOT, ids=[c["id"] for c in PERSHOT])
+def test_pershot_kat_oracle(case):
+    """run()'s per-shot path (circuit.ts:3455-3481) on the oracle against the
+    reference's measure / reset / if / noise tests."""
+    idx, bits, regs = pershot_oracle_raw(case)
+    probs, cregs = summarize(case["n"], idx, bits, regs)
+    clean = pure_oracle_probs(case) if any(c[0] == "like_clean" for c in case["checks"]) else None
+    check_pershot(case, probs, cregs, clean)
+
+
+def _xorshift(s, k):
+    for _ in range(k):
+        s ^= (s << 13) & 0xFFFFFFFF
+        s ^= s >> 17
+        s ^= (s << 5) & 0xFFFFFFFF
+    return s
+
+
+def test_pershot_draw_order():
+    """Draws per shot follow applyOps: one per measure / reset, one more per
+    measure when pMeas != 0, one per noisy gate, one for sampleSV, then n
+    readout draws when pMeas != 0; an if-body draws only when it runs."""
+    c = O.OCircuit(2).add("h", [0]).add("cnot", [0, 1])
+    c.measure(0, 0)
+    c.reset(1)
+    _, _, st = c.run_pershot(10, 7, 0.0, 0.0, 0.0, 1)
+    assert st == _xorshift(7, 10 * 3)
+    _, _, st = c.run_pershot(10, 7, 0.1, 0.2, 0.3, 1)
+    assert st == _xorshift(7, 10 * (1 + 1 + 1 + 1 + 1 + 1 + 2))
+    # if-body with a noisy gate: x(1) runs only when bit 0 reads 1
+    d = O.OCircuit(2)
+    d.measure(0, 0)
+    d.if_(0, 1, 1, O.OCircuit(2).add("x", [1]))
+    _, _, st = d.run_pershot(5, 9, 0.5, 0.0, 0.0, 1, init=1)  # q0 = 1: always taken
+    assert st == _xorshift(9, 5 * (1 + 1 + 1))
+    _, _, st = d.run_pershot(5, 9, 0.5, 0.0, 0.0, 1, init=0)  # never taken
+    assert st == _xorshift(9, 5 * (1 + 1))
