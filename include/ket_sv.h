@@ -232,6 +232,13 @@ KET_API int ket_sample(const ket_state* st, const double* r, size_t shots, doubl
 KET_API int ket_run_shots(ket_state* st, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
                           const ket_noise* noise, uint64_t init, size_t shots, uint32_t* prng_state, int ncbits,
                           uint64_t* out_idx, uint8_t* out_bits);
+/* Test hook for ket_run_shots: 0 = automatic (states of up to 12 qubits c128
+ * / 13 c64 whose shots draw a fixed number of times run as batched
+ * trajectories, one CTA per shot with the state in shared memory; others
+ * run one trajectory at a time through the fused engine), 1 = always one at
+ * a time, 2 = batched only (KET_ERR_UNSUPPORTED where it does not apply).
+ * No counterpart in the reference. */
+KET_API int ket_debug_pershot_path(int mode);
 /* Circuit.expectation(pauli) (circuit.ts:3728-3753): pauli[q] in "IXYZ" acts on qubit q. */
 KET_API int ket_expect_pauli(const ket_state* st, const char* pauli, double* out);
 /* vqe() energy (algorithms.ts:301-336): sum_t coeffs[t] <P_t>.  ops holds nterms

@@ -108,6 +108,7 @@ def lib():
             "ket_sample": (i32, [vp, P(dbl), sz, dbl, P(u64)]),
             "ket_run_shots": (i32, [vp, P(ket_op), sz, P(dbl), sz, P(ket_noise), u64, sz, P(C.c_uint32), i32,
                                     P(u64), P(C.c_uint8)]),
+            "ket_debug_pershot_path": (i32, [i32]),
             "ket_expect_pauli": (i32, [vp, C.c_char_p, P(dbl)]),
             "ket_expect_pauli_sum": (i32, [vp, i32, P(dbl), C.c_char_p, P(dbl)]),
             "ket_adjoint_gradient": (i32, [vp, i32, u64, P(ket_op), sz, P(dbl), sz, P(ket_param_binding), sz,

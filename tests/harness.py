@@ -93,6 +93,8 @@ def _oracle_ops(c, ops, regs, n):
             _oracle_ops(body, op[3], regs, n)
             first, size = regs.get(op[1], (0, 0))
             c.if_(first, size, op[2], body)
+        elif op[0] == "unitary":
+            c.unitary(unitary_matrix(op[2]), op[1])
         else:
             c.add(op[0], op[1], op[2])
 
@@ -141,6 +143,8 @@ def ket_pershot_circuit(case):
             elif op[0] == "if":
                 body = op[3]
                 c = c.if_(op[1], op[2], lambda b, body=body: build(b, body))
+            elif op[0] == "unitary":
+                c = c.unitary(unitary_matrix(op[2]), *op[1])
             else:
                 c = getattr(c, op[0])(*op[2], *op[1])
         return c

@@ -51,8 +51,19 @@ def test_pershot_kat_engine(case):
     check_pershot(case, r.probs, r.cregs, clean)
 
 
+@pytest.fixture(params=[1, 0], ids=["one_at_a_time", "automatic"])
+def path(request):
+    """ket_run_shots' path: 1 = one trajectory at a time through the fused
+    engine; 0 = automatic (every KAT and the small random circuits below
+    then run as batched trajectories in shared memory)."""
+    from ket_b200 import _lib
+    _lib.check(_lib.lib().ket_debug_pershot_path(request.param))
+    yield request.param
+    _lib.lib().ket_debug_pershot_path(0)
+
+
 @pytest.mark.parametrize("case", CASES, ids=[c["id"] for c in CASES])
-def test_pershot_matches_oracle_shot_by_shot(case):
+def test_pershot_matches_oracle_shot_by_shot(case, path):
     from ket_b200.circuit import make_prng
     c = ket_pershot_circuit(case)
     shots, seed = case["run"]["shots"], case["run"]["seed"]
@@ -71,9 +82,11 @@ def test_pershot_matches_oracle_shot_by_shot(case):
     assert state == ostate
 
 
-def random_case(n, depth, seed, noise):
+def random_case(n, depth, seed, noise, if_draws=True):
     """A seeded circuit with gates of every kind, measurements, resets and a
-    nested if, as a case spec (see tests/golden/make_pershot_kats.py)."""
+    nested if, as a case spec (see tests/golden/make_pershot_kats.py).
+    if_draws=False keeps every draw out of the if-bodies (only noiseless
+    permutation gates there), so that each shot draws a fixed number of times."""
     rng = np.random.default_rng(seed)
     singles = ["h", "x", "y", "z", "s", "t", "v"]
     rots = ["rx", "ry", "rz", "u1"]
@@ -108,15 +121,28 @@ def random_case(n, depth, seed, noise):
     ops = [["creg", "c", 3]] + gates(depth)
     ops += [["measure", 0, "c", 0], ["measure", n - 1, "c", 1]]
     ops += gates(depth // 2)
-    ops += [["if", "c", 1, gates(3) + [["measure", 1, "c", 2], ["if", "c", 5, [["x", [2], []]]]]]]
+    if if_draws:
+        ops += [["if", "c", 1, gates(3) + [["measure", 1, "c", 2], ["if", "c", 5, [["x", [2], []]]]]]]
+    else:
+        ops += [["if", "c", 1, [["ccx", [0, 1, 2], []], ["if", "c", 3, [["cswap", [2, 0, 1], []]]]]]]
+        ops += [["unitary", [1, 3], _random_unitary(rng, 4)], ["csrswap", [0, 2, 3], []]]
     ops += [["reset", n // 2, 0]] + gates(depth // 2) + [["measure", 2, "m", 0]]
     return {"id": f"rand{n}", "n": n, "ops": ops, "run": {"shots": 0, "seed": 0, "noise": noise}, "checks": []}
 
 
-@pytest.mark.parametrize("n,depth,shots,noise", [(10, 40, 200, None), (12, 40, 100, "aria-1"),
-                                                 (16, 24, 12, {"p1": 0.05, "p2": 0.1, "pMeas": 0.02})])
-def test_pershot_random_circuits(n, depth, shots, noise):
-    case = random_case(n, depth, 1000 + n, noise)
+def _random_unitary(rng, d):
+    z = rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))
+    q, r = np.linalg.qr(z)
+    q = q * (np.diag(r) / np.abs(np.diag(r)))
+    return [[float(v) for c in row for v in (c.real, c.imag)] for row in q]
+
+
+@pytest.mark.parametrize("n,depth,shots,noise,if_draws", [
+    (10, 40, 200, None, True), (12, 40, 100, "aria-1", True), (16, 24, 12, {"p1": 0.05, "p2": 0.1, "pMeas": 0.02}, True),
+    (5, 40, 2000, {"p1": 0.05, "p2": 0.1, "pMeas": 0.02}, False), (10, 40, 500, "h1-1", False),
+    (12, 30, 200, {"p1": 0.02, "p2": 0.05, "pMeas": 0.01}, False)])
+def test_pershot_random_circuits(n, depth, shots, noise, if_draws, path):
+    case = random_case(n, depth, 1000 + n, noise, if_draws)
     c = ket_pershot_circuit(case)
     idx, bits, state, layout = engine_raw(c, shots, 77, pershot_noise(case))
     oidx, obits, regs = pershot_oracle_raw(case, shots=shots, seed=77)
