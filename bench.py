@@ -385,7 +385,10 @@ def extras():
       qaoa_batch 4096 QAOA MaxCut instances (3-regular graphs, n in 10..22 even,
                  p = 4) in one persistent launch
       precision  complex64 state against complex128 at 31 qubits (brickwork, 30
-                 layers) and the complex64 33-qubit run of the same family"""
+                 layers) and the complex64 33-qubit run of the same family
+      pershot    run()'s per-shot path: 65536 noisy shots (the aria-1 profile)
+                 of a 12-qubit brickwork with a mid-circuit measure and reset;
+                 shot records checked against the oracle on a sample"""
     import numpy as np
 
     from ket_b200 import KET_C64, workloads as W
@@ -436,7 +439,44 @@ def extras():
     out["precision"] = {"fidelity_31q": abs(ov) ** 2 / (na * nb), "max_abs_amp_err_31q": mx,
                         "norm_c128_31q": na, "norm_c64_31q": nb, "c64_33q_seconds": t33,
                         "c64_33q_gates_per_s": k / t33, "c64_33q_norm": n33}
+    out["pershot"] = pershot_measure()
     return out
+
+
+def pershot_measure(shots: int = 65536, sample: int = 32):
+    """Shots/s of run()'s per-shot path through the public API, and the
+    oracle's per-shot run (the CPU checker) on the first `sample` shots."""
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import DEVICES, flatten_ops, make_prng
+    c = W.midcircuit_brickwork(12, 10, 42)
+    c.run(shots=1024, seed=1, noise="aria-1")
+    t = time.perf_counter()
+    dist = c.run(shots=shots, seed=7, noise="aria-1")
+    tp = time.perf_counter() - t
+    res = {"qubits": 12, "ops": len(c.ops), "shots": shots, "noise": "aria-1", "seconds": tp,
+           "shots_per_s": shots / tp, "distinct_outcomes": len(dist.probs), "unit": "shots/s (wall clock)"}
+    idx, bits, layout, _ = c.run_shots(sample, seed=7, noise="aria-1")
+    try:
+        from oracle import oracle as O
+    except Exception as e:  # the oracle library could not be built here
+        res["oracle"] = f"unavailable: {e}"
+        return res
+    oc = O.OCircuit(12)
+    for op in flatten_ops(c.ops):
+        if op.kind == "measure":
+            oc.measure(op.qubits[0], layout[op.extra[0]][0] + op.extra[1])
+        elif op.kind == "reset":
+            oc.reset(op.qubits[0])
+        else:
+            oc.add(op.name, list(op.qubits), list(op.params))
+    nz = DEVICES["aria-1"]["noise"]
+    t = time.perf_counter()
+    oidx, obits, _ = oc.run_pershot(sample, make_prng(7).state[0], nz["p1"], nz["p2"], nz["pMeas"], bits.shape[1])
+    to = time.perf_counter() - t
+    res["oracle_shots_per_s"] = sample / to
+    res["oracle_sample_shots"] = sample
+    res["sample_matches_oracle"] = bool((idx == oidx).all() and (bits == obits).all())
+    return res
 
 
 def main():

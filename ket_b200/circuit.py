@@ -579,25 +579,35 @@ class Circuit:
             counts[i] = counts.get(i, 0) + 1
         return Distribution(self.qubits, shots, counts, {name: [0.0] * size for name, size in self._cregs.items()})
 
-    def _run_pershot(self, shots: int, seed: Optional[int], nz, initialState: Optional[str]) -> Distribution:
-        """run()'s per-shot path (circuit.ts:3455-3481): one device trajectory
-        per shot through ket_run_shots, all shots drawing one makePrng stream."""
+    def run_shots(self, shots: int = 1024, seed: Optional[int] = None, noise=None,
+                  initialState: Optional[str] = None):
+        """The per-shot records behind run()'s per-shot path (circuit.ts:3455-3481):
+        (sampled index per shot, classical bits [shots, bits], {register: (first
+        bit, size)}, xorshift32 state after the last draw).  One device
+        trajectory per shot through ket_run_shots; all shots draw one makePrng
+        stream in the reference's order."""
+        nz = resolve_noise(noise)
         init = bitstring_to_index(initialState, self.qubits) if initialState is not None else 0
         arr, m, k, ncbits, layout = shots_to_abi(self.ops, self._cregs)
         st = DeviceState(self.qubits)
-        noise = ket_noise(*(nz if nz is not None else (0.0, 0.0, 0.0)))
+        noise_s = ket_noise(*(nz if nz is not None else (0.0, 0.0, 0.0)))
         state = C.c_uint32(make_prng(seed).state[0])
         out_idx = np.zeros(max(shots, 1), dtype=np.uint64)
         out_bits = np.zeros(max(shots * ncbits, 1), dtype=np.uint8)
         mv = np.ascontiguousarray(m).view(np.float64)
         check(lib().ket_run_shots(st.h, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size,
-                                  C.byref(noise) if nz is not None else None, init, shots, C.byref(state), ncbits,
+                                  C.byref(noise_s) if nz is not None else None, init, shots, C.byref(state), ncbits,
                                   out_idx.ctypes.data_as(C.POINTER(C.c_uint64)),
                                   out_bits.ctypes.data_as(C.POINTER(C.c_uint8))))
+        bits = out_bits[: shots * ncbits].reshape(shots, ncbits)
+        return out_idx[:shots], bits, layout, int(state.value)
+
+    def _run_pershot(self, shots: int, seed: Optional[int], nz, initialState: Optional[str]) -> Distribution:
+        idx, bits, layout, _ = self.run_shots(shots, seed, None if nz is None else
+                                              {"p1": nz[0], "p2": nz[1], "pMeas": nz[2]}, initialState)
         counts: Dict[int, int] = {}
-        for i in out_idx[:shots].tolist():
+        for i in idx.tolist():
             counts[i] = counts.get(i, 0) + 1
-        bits = out_bits[: shots * ncbits].reshape(shots, ncbits) if shots else np.zeros((0, ncbits), np.uint8)
         cregs = {name: [float(bits[:, off + j].sum()) / shots if shots else 0.0 for j in range(size)]
                  for name, (off, size) in layout.items()}
         return Distribution(self.qubits, shots, counts, cregs)

@@ -14,6 +14,9 @@ with 42, in a fixed draw order:
   gamma = rng()*pi, beta = rng()*pi.
 * tfim_vqe: fields h_i = 0.5 + rng() for i = 0..n-1, then batch parameter
   vectors theta = rng()*2*pi.
+* midcircuit_brickwork(n, layers): brickwork(n, layers), measure q0 into c[0],
+  reset q0, then brickwork(n, layers // 2) on the same stream (run() with
+  noise exercises the per-shot path on it).
 
 oracle/ket_oracle.cpp draws the identical streams for the parity tests.
 """
@@ -62,6 +65,16 @@ def brickwork(n: int, layers: int, rng: Xorshift32, c: Circuit = None) -> Circui
 def brickwork_circuit(n: int, layers: int, seed: int = 42) -> Tuple[Circuit, Xorshift32]:
     rng = Xorshift32(seed)
     return brickwork(n, layers, rng), rng
+
+
+def midcircuit_brickwork(n: int, layers: int, seed: int = 42) -> Circuit:
+    """The per-shot path's workload: brickwork(n, layers) from the seeded
+    stream, then measure q0 into c[0] and reset q0, then brickwork(n,
+    layers // 2) continuing the stream."""
+    rng = Xorshift32(seed)
+    c = brickwork(n, layers, rng)
+    c = c.measure(0, "c", 0).reset(0)
+    return brickwork(n, layers // 2, rng, c)
 
 
 def brickwork_qft(n: int, layers: int, seed: int = 42, n_amps: int = 1024):
