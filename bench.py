@@ -388,7 +388,9 @@ def extras():
                  layers) and the complex64 33-qubit run of the same family
       pershot    run()'s per-shot path: 65536 noisy shots (the aria-1 profile)
                  of a 12-qubit brickwork with a mid-circuit measure and reset;
-                 shot records checked against the oracle on a sample"""
+                 shot records checked against the oracle on a sample
+      json       loading the 30-qubit workload's circuit JSON with the C ABI's
+                 loader and with the Python mirror's Circuit.fromJSON"""
     import numpy as np
 
     from ket_b200 import KET_C64, workloads as W
@@ -440,7 +442,28 @@ def extras():
                         "norm_c128_31q": na, "norm_c64_31q": nb, "c64_33q_seconds": t33,
                         "c64_33q_gates_per_s": k / t33, "c64_33q_norm": n33}
     out["pershot"] = pershot_measure()
+    out["json"] = json_measure()
     return out
+
+
+def json_measure(reps: int = 20):
+    """Loading ket's circuit JSON for the 30-qubit workload (2260 gates):
+    the C ABI's loader against the Python mirror's Circuit.fromJSON."""
+    import ket_b200 as K
+    from ket_b200 import workloads as W
+    from ket_b200.circuit_json import js_stringify, program_from_json
+    c, _ = W.brickwork_qft(30, 40, 42)
+    text = js_stringify(c.toJSON())
+    p = program_from_json(text)
+    t = time.perf_counter()
+    for _ in range(reps):
+        p = program_from_json(text)
+    tc = (time.perf_counter() - t) / reps
+    t = time.perf_counter()
+    K.Circuit.fromJSON(text)
+    tp = time.perf_counter() - t
+    return {"ops": p["count"], "bytes": len(text), "loader_ms": tc * 1e3, "loader_MB_per_s": len(text) / tc / 1e6,
+            "python_mirror_ms": tp * 1e3, "unit": "ms per load (wall clock, host)"}
 
 
 def pershot_measure(shots: int = 65536, sample: int = 32):

@@ -153,6 +153,28 @@ KET_API int ket_state_get_amplitudes(const ket_state* st, uint64_t offset, uint6
 /* Copy src into dst (same size and precision). */
 KET_API int ket_state_copy(ket_state* dst, const ket_state* src);
 
+/* ---------------------------------------------------------------- circuit JSON */
+/* A circuit loaded from ket's JSON (schema "ket": 1, the output of
+ * Circuit.toJSON, circuit.ts:3768-3778), lowered to this ABI's op list. */
+typedef struct ket_program ket_program;
+/* Circuit.fromJSON (circuit.ts:3794-3806, opsFromJSON :532-580): parse the
+ * text, rebuild every gate matrix from its meta name and parameters (:467-529),
+ * inline named sub-circuits (flattenOps, :113-133) and pack measure / reset / if
+ * for ket_run_shots, the registers of "cregs" taking consecutive classical bits
+ * in the file's order.  KET_ERR_TYPE for malformed JSON, another schema
+ * version, an unknown op kind or gate name, or unbound parameters (the
+ * reference's TypeErrors). */
+KET_API int ket_program_from_json(const char* text, size_t len, ket_program** out);
+KET_API int ket_program_free(ket_program* p);
+/* Qubits, ops, complex matrix entries, classical bits, registers, and whether
+ * the op list holds measure / reset / if (then it runs with ket_run_shots). */
+KET_API int ket_program_info(const ket_program* p, int* nqubits, size_t* nops, size_t* nmat, int* ncbits, int* nregs,
+                             int* classical);
+/* Copy out the op list and the matrices (2 * nmat doubles). */
+KET_API int ket_program_ops(const ket_program* p, ket_op* ops, size_t ops_cap, double* mats, size_t mat_cap);
+/* Register i: its name (NUL-terminated, truncated to cap bytes), first classical bit and size. */
+KET_API int ket_program_creg(const ket_program* p, int i, char* name, size_t cap, int* first, int* size);
+
 /* ---------------------------------------------------------------- running circuits */
 /* simulatePure (circuit.ts:143-161): apply ops in order.  mats holds nmat complex
  * entries (2*nmat doubles).  Validation mirrors #checkOp (circuit.ts:1113-1146)

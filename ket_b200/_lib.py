@@ -109,6 +109,11 @@ def lib():
             "ket_run_shots": (i32, [vp, P(ket_op), sz, P(dbl), sz, P(ket_noise), u64, sz, P(C.c_uint32), i32,
                                     P(u64), P(C.c_uint8)]),
             "ket_debug_pershot_path": (i32, [i32]),
+            "ket_program_from_json": (i32, [C.c_char_p, sz, P(vp)]),
+            "ket_program_free": (i32, [vp]),
+            "ket_program_info": (i32, [vp, P(i32), P(sz), P(sz), P(i32), P(i32), P(i32)]),
+            "ket_program_ops": (i32, [vp, P(ket_op), sz, P(dbl), sz]),
+            "ket_program_creg": (i32, [vp, i32, C.c_char_p, sz, P(i32), P(i32)]),
             "ket_expect_pauli": (i32, [vp, C.c_char_p, P(dbl)]),
             "ket_expect_pauli_sum": (i32, [vp, i32, P(dbl), C.c_char_p, P(dbl)]),
             "ket_adjoint_gradient": (i32, [vp, i32, u64, P(ket_op), sz, P(dbl), sz, P(ket_param_binding), sz,

@@ -612,6 +612,18 @@ class Circuit:
                  for name, (off, size) in layout.items()}
         return Distribution(self.qubits, shots, counts, cregs)
 
+    # ------------------------------------------------------------------ JSON (circuit.ts:3768-3806)
+    def toJSON(self) -> dict:
+        """Circuit.toJSON: {ket: 1, qubits, cregs, gates, ops}, gates by meta."""
+        from .circuit_json import to_json
+        return to_json(self)
+
+    @staticmethod
+    def fromJSON(j) -> "Circuit":
+        """Circuit.fromJSON: a CircuitJSON dict or its JSON text."""
+        from .circuit_json import from_json
+        return from_json(j)
+
     # ------------------------------------------------------------------ lowering to the C ABI
     def to_abi(self):
         return ops_to_abi(flatten_ops(self.ops))
