@@ -237,6 +237,18 @@ KET_API int ket_norm2(const ket_state* st, double* out);
  * (the last such entry's running sum is taken as 1.0).  For 2^n <= 2^22 the running
  * sum is accumulated in ascending index order, exactly as the reference does. */
 KET_API int ket_sample(const ket_state* st, const double* r, size_t shots, double threshold, uint64_t* out_idx);
+/* circuitMatrix() (circuit.ts:1462-1485): the 2^n x 2^n matrix of ops on
+ * nqubits <= 12 (KET_ERR_RANGE above, as the reference), out[row * 2^n + col]
+ * as interleaved (re, im), rows and columns indexed with q0 as the MOST
+ * significant bit (the standard convention the reference uses here).  Column
+ * col is the state the ops make from |flip(col)>, with the reference's
+ * per-gate pruning.  Allocates a 2n-qubit device state for the call. */
+KET_API int ket_circuit_matrix(ket_ctx* ctx, int nqubits, const ket_op* ops, size_t nops, const double* mats,
+                               size_t nmat, const ket_exec_opts* opts, double* out);
+/* blochAngles(q) (circuit.ts:4102-4129): out = {rho00, rho11, Re rho01,
+ * Im rho01, theta, phi} of qubit q's reduced density matrix, with
+ * theta = acos(clamp(rho00 - rho11)) and phi = atan2(-2 Im rho01, 2 Re rho01). */
+KET_API int ket_bloch(const ket_state* st, int q, double* out);
 /* run()'s per-shot path (circuit.ts:3455-3481 over applyOps, :169-207): one
  * trajectory per shot from |init>, using st as the device workspace (its
  * qubit count and precision; its contents are overwritten).  ops may hold

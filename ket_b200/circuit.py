@@ -531,6 +531,30 @@ class Circuit:
         self._require_pure("statevector()")
         return list(self._state(initialState).marginals())
 
+    def blochAngles(self, q: int, initialState: Optional[str] = None) -> Dict[str, float]:
+        """blochAngles(q) (circuit.ts:4102-4129): {theta, phi} of qubit q's
+        reduced density matrix."""
+        self._require_pure("blochAngles()")
+        out = np.empty(6, dtype=np.float64)
+        check(lib().ket_bloch(self._state(initialState).h, q, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return {"theta": float(out[4]), "phi": float(out[5])}
+
+    def circuitMatrix(self) -> np.ndarray:
+        """circuitMatrix() (circuit.ts:1462-1485): the 2^n x 2^n matrix,
+        matrix[row][col], rows and columns with q0 as the most significant bit.
+        TypeError for measure/reset/if, RangeError above 12 qubits."""
+        if any(op.kind in ("measure", "reset", "if") for op in self.ops):
+            raise TypeError("circuitMatrix() requires a pure circuit — remove measure/reset/if ops")
+        n = self.qubits
+        if n > 12:
+            raise RangeError(f"circuitMatrix(): circuit too large ({n} qubits = {1 << n}×{1 << n} matrix)")
+        arr, m, k = ops_to_abi(flatten_ops(self.ops))
+        out = np.empty((1 << n, 1 << n), dtype=np.complex128)
+        mv = np.ascontiguousarray(m).view(np.float64)
+        check(lib().ket_circuit_matrix(default_ctx(), n, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size,
+                                       None, out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
     def marginal_dist(self, qubits: Sequence[int], initialState: Optional[str] = None) -> np.ndarray:
         """Joint distribution of `qubits` (bin bit k = qubits[k])."""
         self._require_pure("statevector()")

@@ -18,6 +18,8 @@
 //                                 the per-shot path: collapseQubit, sampleSV,
 //                                 applyOps (measure / reset / if), dep1 / dep2
 //   src/circuit.ts:1491-1518      amplitude / probability / marginals
+//   src/circuit.ts:1462-1485      circuitMatrix
+//   src/circuit.ts:4102-4129      blochAngles
 //   src/circuit.ts:3700-3753      exactProbs / expectation
 //   src/circuit.ts:1108-1146      #checkOp validation (RangeError / TypeError)
 //   src/algorithms.ts:16-38       qft / iqft
@@ -766,6 +768,56 @@ static uint32_t run_pershot(const Circuit& c, uint64_t init, int shots, uint32_t
   return rng.s;
 }
 
+// circuitMatrix (circuit.ts:1462-1485): column col is simulatePure from
+// |flip(col)> (sparse mode); rows and columns use q0 as the most significant bit
+static void circuit_matrix(const Circuit& c, double* out) {
+  const int n = c.n;
+  const uint64_t dim = uint64_t(1) << n;
+  auto flip = [n](uint64_t i) {
+    uint64_t r = 0;
+    for (int b = 0; b < n; b++)
+      if (i & (uint64_t(1) << b)) r |= uint64_t(1) << (n - 1 - b);
+    return r;
+  };
+  std::memset(out, 0, sizeof(double) * 2 * dim * dim);
+  for (uint64_t col = 0; col < dim; col++) {
+    State* s = simulate(c, flip(col), 0);
+    for (auto& kv : s->sv) {
+      const uint64_t at = flip(kv.first) * dim + col;
+      out[2 * at] = kv.second.re;
+      out[2 * at + 1] = kv.second.im;
+    }
+    delete s;
+  }
+}
+
+// blochAngles (circuit.ts:4102-4129) over the entries in ascending index order;
+// out = {rho00, rho11, Re rho01, Im rho01, theta, phi}
+static void bloch(const State* s, int q, double* out) {
+  const uint64_t mask = uint64_t(1) << q;
+  std::vector<std::pair<uint64_t, C>> e;
+  if (s->mode == 0) e = sorted_entries(s->sv);
+  else
+    for (uint64_t i = 0; i < s->d.a.size(); i++)
+      if (s->d.a[i].re != 0 || s->d.a[i].im != 0) e.emplace_back(i, s->d.a[i]);
+  double r00 = 0, r11 = 0, re = 0, im = 0;
+  for (const auto& kv : e) {
+    const C& a = kv.second;
+    const double p = a.re * a.re + a.im * a.im;
+    if (kv.first & mask) { r11 += p; continue; }
+    r00 += p;
+    const C a1 = state_get(s, kv.first | mask);
+    if (a1.re != 0 || a1.im != 0) {
+      re += a.re * a1.re + a.im * a1.im;
+      im += a.im * a1.re - a.re * a1.im;
+    }
+  }
+  const double rz = r00 - r11, rx = 2 * re, ry = -2 * im;
+  out[0] = r00; out[1] = r11; out[2] = re; out[3] = im;
+  out[4] = std::acos(std::max(-1.0, std::min(1.0, rz)));
+  out[5] = std::atan2(ry, rx);
+}
+
 // ---------------------------------------------------------------- algorithms.ts
 static Circuit qft(int n) {                       // algorithms.ts:16-26
   Circuit c{n, {}};
@@ -989,6 +1041,9 @@ uint32_t orc_run_pershot(void* cp, uint64_t init, int shots, uint32_t seed, doub
                          int ncbits, uint64_t* out_idx, uint8_t* out_bits) {
   return run_pershot(*(Circuit*)cp, init, shots, seed, Noise{p1, p2, pm}, ncbits, out_idx, out_bits);
 }
+
+void orc_circuit_matrix(void* cp, double* out) { circuit_matrix(*(Circuit*)cp, out); }
+void orc_bloch(void* sp, int q, double* out) { bloch((State*)sp, q, out); }
 
 void* orc_simulate(void* cp, uint64_t init, int mode) { return simulate(*(Circuit*)cp, init, mode); }
 void orc_state_free(void* s) { delete (State*)s; }

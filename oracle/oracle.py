@@ -81,6 +81,8 @@ def lib():
         "orc_regular3": (i32, [i32, P(u32), P(i32)]),
         "orc_prng_next": (u32, [P(u32)]),
         "orc_time_ops": (u64, [vp, u64, i32, i32, i32, P(dbl)]),
+        "orc_circuit_matrix": (None, [vp, P(dbl)]),
+        "orc_bloch": (None, [vp, i32, P(dbl)]),
         "orc_add_measure": (i32, [vp, i32, i32]),
         "orc_add_reset": (i32, [vp, i32]),
         "orc_add_if": (i32, [vp, i32, i32, i32, vp]),
@@ -193,6 +195,13 @@ class OCircuit:
                                      bits.ctypes.data_as(C.POINTER(C.c_uint8)))
         return idx[:shots], bits[: shots * ncbits].reshape(shots, ncbits), int(st)
 
+    def circuit_matrix(self) -> np.ndarray:
+        """circuitMatrix() (circuit.ts:1462-1485): one sparse simulation per column."""
+        dim = 1 << self.qubits
+        out = np.zeros((dim, dim), dtype=np.complex128)
+        self._L.orc_circuit_matrix(self.h_, out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
     def simulate(self, init: int = 0, mode: int = SPARSE) -> "OState":
         return OState(self._L.orc_simulate(self.h_, init, mode), self.qubits)
 
@@ -263,6 +272,12 @@ class OState:
         out = np.zeros(max(shots, 1), dtype=np.uint64)
         self._L.orc_run(self.h_, shots, seed & 0xFFFFFFFF, out.ctypes.data_as(C.POINTER(C.c_uint64)))
         return out[:shots]
+
+    def bloch(self, q: int):
+        """blochAngles(q) (circuit.ts:4102-4129): (rho00, rho11, Re rho01, Im rho01, theta, phi)."""
+        out = np.zeros(6)
+        self._L.orc_bloch(self.h_, q, _dp(out))
+        return out
 
     def marginals(self) -> np.ndarray:
         out = np.zeros(self.n, dtype=np.float64)

@@ -184,3 +184,51 @@ def test_pershot_draw_order():
     assert st == _xorshift(9, 5 * (1 + 1 + 1))
     _, _, st = d.run_pershot(5, 9, 0.5, 0.0, 0.0, 1, init=0)  # never taken
     assert st == _xorshift(9, 5 * (1 + 1))
+
+
+# circuitMatrix() / blochAngles() (circuit.test.ts:6423-6513, :4745-4786), restated
+S2 = 1 / math.sqrt(2)
+MATRIX_KATS = [
+    ("identity", 2, [], np.eye(4)),
+    ("h", 1, [("h", [0], [])], np.array([[S2, S2], [S2, -S2]])),
+    ("x", 1, [("x", [0], [])], np.array([[0, 1], [1, 0]])),
+    ("s", 1, [("s", [0], [])], np.array([[1, 0], [0, 1j]])),
+    ("cnot_unitary", 2, [("unitary", [0, 1], np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]]))],
+     np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]])),
+    ("h_unitary", 1, [("unitary", [0], np.array([[S2, S2], [S2, -S2]]))], np.array([[S2, S2], [S2, -S2]])),
+]
+BLOCH_KATS = [  # (id, n, gates, theta, theta digits, phi or None, phi digits)
+    ("zero", 1, [], 0.0, 10, None, 0),
+    ("one", 1, [("x", [0], [])], math.pi, 10, None, 0),
+    ("plus", 1, [("h", [0], [])], math.pi / 2, 8, 0.0, 8),
+    ("rx", 1, [("rx", [0], [math.pi / 2])], math.pi / 2, 8, -math.pi / 2, 8),
+    ("ry", 1, [("ry", [0], [math.pi / 3])], math.pi / 3, 8, None, 0),
+    ("bell", 2, [("h", [0], []), ("cnot", [0, 1], [])], math.pi / 2, 8, None, 0),
+]
+
+
+def _ocirc(n, gates):
+    c = O.OCircuit(n)
+    for name, qs, ps in gates:
+        if name == "unitary":
+            c.unitary(ps, qs)
+        else:
+            c.add(name, qs, ps)
+    return c
+
+
+@pytest.mark.parametrize("kat", MATRIX_KATS, ids=[k[0] for k in MATRIX_KATS])
+def test_circuit_matrix_kats_oracle(kat):
+    _, n, gates, want = kat
+    U = _ocirc(n, gates).circuit_matrix()
+    assert np.max(np.abs(U - want)) < tol(10)
+    assert np.max(np.abs(U.conj().T @ U - np.eye(1 << n))) < tol(10)
+
+
+@pytest.mark.parametrize("kat", BLOCH_KATS, ids=[k[0] for k in BLOCH_KATS])
+def test_bloch_kats_oracle(kat):
+    _, n, gates, theta, td, phi, pd = kat
+    out = _ocirc(n, gates).simulate().bloch(0)
+    assert abs(out[4] - theta) < tol(td)
+    if phi is not None:
+        assert abs(out[5] - phi) < tol(pd)
