@@ -249,6 +249,22 @@ KET_API int ket_circuit_matrix(ket_ctx* ctx, int nqubits, const ket_op* ops, siz
  * Im rho01, theta, phi} of qubit q's reduced density matrix, with
  * theta = acos(clamp(rho00 - rho11)) and phi = atan2(-2 Im rho01, 2 Re rho01). */
 KET_API int ket_bloch(const ket_state* st, int q, double* out);
+/* runDM (density.ts:475-588, Circuit.dm() circuit.ts:4562-4579): the exact
+ * density matrix of ops on n qubits from |0..0><0..0|, with per-gate
+ * depolarizing noise p1 (after single-qubit gates) and p2 (after cnot / swap /
+ * two / controlled); p <= 0 adds none.  rho is a state of 2n qubits holding
+ * rho[row][col] at index (row << n) | col; each op runs as U rho U^dagger with
+ * the reference's pruning of every output entry below |v|^2 = 1e-14.
+ * Unitary ops of more than 5 qubits: KET_ERR_UNSUPPORTED.  Read the result
+ * with ket_amplitudes / ket_state_get_amplitudes (entries), ket_norm2
+ * (purity, density.ts:314-318), ket_dm_probs and ket_dm_bloch. */
+KET_API int ket_dm_run(ket_state* rho, const ket_op* ops, size_t nops, const double* mats, size_t nmat, double p1,
+                       double p2);
+/* The diagonal of rho: out[r] = Re rho[r][r] (DensityMatrix.probabilities,
+ * density.ts:299-307, before its p > 1e-14 filter), 2^n values. */
+KET_API int ket_dm_probs(const ket_state* rho, double* out);
+/* DensityMatrix.blochAngles(q) (density.ts:356-372): out = {theta, phi}. */
+KET_API int ket_dm_bloch(const ket_state* rho, int q, double* out);
 /* run()'s per-shot path (circuit.ts:3455-3481 over applyOps, :169-207): one
  * trajectory per shot from |init>, using st as the device workspace (its
  * qubit count and precision; its contents are overwritten).  ops may hold

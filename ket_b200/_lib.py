@@ -111,6 +111,9 @@ def lib():
             "ket_debug_pershot_path": (i32, [i32]),
             "ket_circuit_matrix": (i32, [vp, i32, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts), P(dbl)]),
             "ket_bloch": (i32, [vp, i32, P(dbl)]),
+            "ket_dm_run": (i32, [vp, P(ket_op), sz, P(dbl), sz, dbl, dbl]),
+            "ket_dm_probs": (i32, [vp, P(dbl)]),
+            "ket_dm_bloch": (i32, [vp, i32, P(dbl)]),
             "ket_program_from_json": (i32, [C.c_char_p, sz, P(vp)]),
             "ket_program_free": (i32, [vp]),
             "ket_program_info": (i32, [vp, P(i32), P(sz), P(sz), P(i32), P(i32), P(i32)]),

@@ -46,6 +46,54 @@ DEVICES = {
 }
 
 
+# Density-matrix noise profiles (DM_DEVICE_NOISE, density.ts:453-457): p1, p2.
+DM_DEVICE_NOISE = {"aria-1": {"p1": 0.0003, "p2": 0.005}, "forte-1": {"p1": 0.0001, "p2": 0.002},
+                   "harmony": {"p1": 0.001, "p2": 0.015}}
+
+
+class DensityMatrix:
+    """DensityMatrix (density.ts:274-372) over a device state of 2n qubits
+    holding rho[row][col] at index (row << n) | col."""
+
+    def __init__(self, qubits: int, state: "DeviceState"):
+        self.qubits = qubits
+        self._st = state
+
+    def get(self, row: int, col: int) -> complex:
+        """rho[row][col] (density.ts:283-286)."""
+        return complex(self._st.amplitudes([(int(row) << self.qubits) | int(col)])[0])
+
+    def probabilities(self) -> Dict[str, float]:
+        """Diagonal probabilities, q0-leftmost keys, values > 1e-14 (density.ts:299-307)."""
+        d = np.empty(1 << self.qubits, dtype=np.float64)
+        check(lib().ket_dm_probs(self._st.h, d.ctypes.data_as(C.POINTER(C.c_double))))
+        return {index_to_bitstring(r, self.qubits): float(v) for r, v in enumerate(d) if v > 1e-14}
+
+    def purity(self) -> float:
+        """Tr(rho^2) = sum of |rho[r][c]|^2 (density.ts:314-318)."""
+        return self._st.norm2()
+
+    def entropy(self) -> float:
+        """Von Neumann entropy in bits (density.ts:328-346), from the eigenvalues of
+        the dense Hermitian rho (host LAPACK)."""
+        dim = 1 << self.qubits
+        if dim > 4096:
+            raise RangeError(f"entropy(): circuit too large (n={self.qubits}, dim={dim})")
+        rho = self._st.amplitudes_dense().reshape(dim, dim)
+        lam = np.linalg.eigvalsh(rho)
+        return float(-sum(x * math.log2(x) for x in lam if x > 1e-14))
+
+    def blochAngles(self, q: int) -> Dict[str, float]:
+        """Bloch angles of qubit q (density.ts:356-372)."""
+        out = np.empty(2, dtype=np.float64)
+        check(lib().ket_dm_bloch(self._st.h, q, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return {"theta": float(out[0]), "phi": float(out[1])}
+
+    def dense(self) -> np.ndarray:
+        dim = 1 << self.qubits
+        return self._st.amplitudes_dense().reshape(dim, dim)
+
+
 def resolve_noise(noise):
     """run()'s noise option (circuit.ts:3411-3418): None, a device name, or a
     NoiseParams mapping {p1, p2, pMeas} -> (p1, p2, pMeas), or None."""
@@ -530,6 +578,23 @@ class Circuit:
         """marginals() (circuit.ts:1508-1518): P(qubit q = 1) for each q."""
         self._require_pure("statevector()")
         return list(self._state(initialState).marginals())
+
+    def dm(self, noise=None) -> DensityMatrix:
+        """dm() (circuit.ts:4562-4579, runDM density.ts:475-588): the exact density
+        matrix from |0..0>, with depolarizing noise {p1, p2} or a DM_DEVICE_NOISE name."""
+        if any(op.kind in ("measure", "reset", "if") for op in self.ops):
+            raise TypeError("dm() requires a pure circuit — remove measure/reset/if ops")
+        if isinstance(noise, str):
+            if noise not in DM_DEVICE_NOISE:
+                raise TypeError(f"Unknown device profile '{noise}'. Known: {', '.join(DM_DEVICE_NOISE)}")
+            noise = DM_DEVICE_NOISE[noise]
+        p1 = float((noise or {}).get("p1") or 0)
+        p2 = float((noise or {}).get("p2") or 0)
+        arr, m, k = ops_to_abi(flatten_ops(self.ops))
+        st = DeviceState(2 * self.qubits)
+        mv = np.ascontiguousarray(m).view(np.float64)
+        check(lib().ket_dm_run(st.h, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, p1, p2))
+        return DensityMatrix(self.qubits, st)
 
     def blochAngles(self, q: int, initialState: Optional[str] = None) -> Dict[str, float]:
         """blochAngles(q) (circuit.ts:4102-4129): {theta, phi} of qubit q's

@@ -20,6 +20,9 @@
 //   src/circuit.ts:1491-1518      amplitude / probability / marginals
 //   src/circuit.ts:1462-1485      circuitMatrix
 //   src/circuit.ts:4102-4129      blochAngles
+//   src/density.ts:14-588         runDM: the density matrix with dmSet / dmAcc
+//                                 pruning, depolarizing channels, purity,
+//                                 entropy (Jacobi), blochAngles
 //   src/circuit.ts:3700-3753      exactProbs / expectation
 //   src/circuit.ts:1108-1146      #checkOp validation (RangeError / TypeError)
 //   src/algorithms.ts:16-38       qft / iqft
@@ -47,6 +50,7 @@
 #include <cstdlib>
 #include <string>
 #include <vector>
+#include <map>
 #include <unordered_map>
 #include <unordered_set>
 #include <algorithm>
@@ -818,6 +822,273 @@ static void bloch(const State* s, int q, double* out) {
   out[5] = std::atan2(ry, rx);
 }
 
+// ---------------------------------------------------------------- density.ts (runDM)
+// The reference keeps rho sparse, key = (row << n) | col (density.ts:14-35);
+// here an ordered map, so every iteration is in ascending key order (the
+// reference's Map iterates in insertion order, which changes only the order of
+// the sums in depolarize2 and so only their rounding).
+typedef std::map<uint64_t, C> DMap;
+static inline C conjc(C a) { return C{a.re, -a.im}; }
+static inline C dm_get(const DMap& m, uint64_t k) {
+  auto it = m.find(k);
+  return it == m.end() ? ZERO : it->second;
+}
+static inline void dm_set(DMap& m, uint64_t k, C v) {  // dmSet (:23-27)
+  if (!negligible(v)) m[k] = v;
+  else m.erase(k);
+}
+static inline void dm_acc(DMap& m, uint64_t k, C v) {  // dmAcc (:29-35)
+  auto it = m.find(k);
+  C nx = it != m.end() ? add(it->second, v) : v;
+  if (!negligible(nx)) m[k] = nx;
+  else if (it != m.end()) m.erase(it);
+}
+
+// applySingle (:46-79)
+static DMap dm_single(const DMap& dm, int n, int q, const Mat& g) {
+  DMap next;
+  const uint64_t dim_mask = (uint64_t(1) << n) - 1, qm = uint64_t(1) << q;
+  const uint64_t krm = qm << n, kcm = qm;
+  const C a = g[0], b = g[1], c = g[2], d = g[3];
+  const C ca = conjc(a), cb = conjc(b), cc = conjc(c), cd = conjc(d);
+  std::unordered_set<uint64_t> seen;
+  for (const auto& kv : dm) {
+    const uint64_t ctx = kv.first & ~krm & ~kcm;
+    if (!seen.insert(ctx).second) continue;
+    const uint64_t r0 = ctx >> n, c0 = ctx & dim_mask, r1 = r0 | qm, c1 = c0 | qm;
+    const C p00 = dm_get(dm, (r0 << n) | c0), p01 = dm_get(dm, (r0 << n) | c1);
+    const C p10 = dm_get(dm, (r1 << n) | c0), p11 = dm_get(dm, (r1 << n) | c1);
+    const C t00 = add(mul(a, p00), mul(b, p10)), t01 = add(mul(a, p01), mul(b, p11));
+    const C t10 = add(mul(c, p00), mul(d, p10)), t11 = add(mul(c, p01), mul(d, p11));
+    dm_set(next, (r0 << n) | c0, add(mul(ca, t00), mul(cb, t01)));
+    dm_set(next, (r0 << n) | c1, add(mul(cc, t00), mul(cd, t01)));
+    dm_set(next, (r1 << n) | c0, add(mul(ca, t10), mul(cb, t11)));
+    dm_set(next, (r1 << n) | c1, add(mul(cc, t10), mul(cd, t11)));
+  }
+  return next;
+}
+
+// applyUnitaryN (:133-180); applyTwo (:81-119) is its 2-qubit case with the
+// same sums
+static DMap dm_unitary(const DMap& dm, int n, const std::vector<int>& qs, const Mat& m) {
+  DMap next;
+  const uint64_t dim_mask = (uint64_t(1) << n) - 1;
+  const int k = (int)qs.size();
+  const size_t ld = size_t(1) << k;
+  uint64_t all = 0;
+  std::vector<uint64_t> masks(k);
+  for (int i = 0; i < k; i++) { masks[i] = uint64_t(1) << qs[i]; all |= masks[i]; }
+  auto bases = [&](uint64_t base) {
+    std::vector<uint64_t> b(ld);
+    for (size_t i = 0; i < ld; i++) {
+      uint64_t v = base;
+      for (int bit = 0; bit < k; bit++)
+        if ((i >> (k - 1 - bit)) & 1) v |= masks[bit];
+      b[i] = v;
+    }
+    return b;
+  };
+  std::unordered_set<uint64_t> seen;
+  for (const auto& kv : dm) {
+    const uint64_t ctx = kv.first & ~(all << n) & ~all;
+    if (!seen.insert(ctx).second) continue;
+    const std::vector<uint64_t> rb = bases(ctx >> n), cb = bases(ctx & dim_mask);
+    std::vector<C> p(ld * ld), t(ld * ld);
+    for (size_t ri = 0; ri < ld; ri++)
+      for (size_t ci = 0; ci < ld; ci++) p[ri * ld + ci] = dm_get(dm, (rb[ri] << n) | cb[ci]);
+    for (size_t ri = 0; ri < ld; ri++)
+      for (size_t ci = 0; ci < ld; ci++) {
+        C v = ZERO;
+        for (size_t j = 0; j < ld; j++) v = add(v, mul(m[ri * ld + j], p[j * ld + ci]));
+        t[ri * ld + ci] = v;
+      }
+    for (size_t ri = 0; ri < ld; ri++)
+      for (size_t ci = 0; ci < ld; ci++) {
+        C v = ZERO;
+        for (size_t j = 0; j < ld; j++) v = add(v, mul(t[ri * ld + j], conjc(m[ci * ld + j])));
+        dm_set(next, (rb[ri] << n) | cb[ci], v);
+      }
+  }
+  return next;
+}
+
+// applyPerm (:122-130)
+template <typename F>
+static DMap dm_perm(const DMap& dm, int n, F f) {
+  DMap next;
+  const uint64_t dim_mask = (uint64_t(1) << n) - 1;
+  for (const auto& kv : dm) next[(f(kv.first >> n) << n) | f(kv.first & dim_mask)] = kv.second;
+  return next;
+}
+
+// depolarize1 (:193-222)
+static DMap dm_dep1(const DMap& dm, int n, int q, double p) {
+  if (p <= 0) return dm;
+  DMap next;
+  const uint64_t dim_mask = (uint64_t(1) << n) - 1, qm = uint64_t(1) << q;
+  const double sa = 1 - 2 * p / 3, sb = 2 * p / 3, cf = 1 - 4 * p / 3;
+  std::unordered_set<uint64_t> seen;
+  for (const auto& kv : dm) {
+    const uint64_t ctx = kv.first & ~(qm << n) & ~qm;
+    if (!seen.insert(ctx).second) continue;
+    const uint64_t r0 = ctx >> n, c0 = ctx & dim_mask, r1 = r0 | qm, c1 = c0 | qm;
+    const C p00 = dm_get(dm, (r0 << n) | c0), p11 = dm_get(dm, (r1 << n) | c1);
+    dm_set(next, (r0 << n) | c0, C{sa * p00.re + sb * p11.re, sa * p00.im + sb * p11.im});
+    dm_set(next, (r1 << n) | c1, C{sa * p11.re + sb * p00.re, sa * p11.im + sb * p00.im});
+    const C p01 = dm_get(dm, (r0 << n) | c1), p10 = dm_get(dm, (r1 << n) | c0);
+    dm_set(next, (r0 << n) | c1, C{cf * p01.re, cf * p01.im});
+    dm_set(next, (r1 << n) | c0, C{cf * p10.re, cf * p10.im});
+  }
+  return next;
+}
+
+// PAULI15 (:226-231): {flip_a, flip_b, z_a, z_b} of the 15 non-identity 2-qubit Paulis
+static const int PAULI15[15][4] = {{0, 1, 0, 0}, {0, 1, 0, 1}, {0, 0, 0, 1}, {1, 0, 0, 0}, {1, 1, 0, 0},
+                                   {1, 1, 0, 1}, {1, 0, 0, 1}, {1, 0, 1, 0}, {1, 1, 1, 0}, {1, 1, 1, 1},
+                                   {1, 0, 1, 1}, {0, 0, 1, 0}, {0, 1, 1, 0}, {0, 1, 1, 1}, {0, 0, 1, 1}};
+
+// depolarize2 (:239-264)
+static DMap dm_dep2(const DMap& dm, int n, int a, int b, double p) {
+  if (p <= 0) return dm;
+  DMap next;
+  const uint64_t dim_mask = (uint64_t(1) << n) - 1, ma = uint64_t(1) << a, mb = uint64_t(1) << b;
+  const double w1 = 1 - p, w2 = p / 15;
+  for (const auto& kv : dm) {
+    const uint64_t r = kv.first >> n, c = kv.first & dim_mask;
+    const C v = kv.second;
+    dm_acc(next, (r << n) | c, C{w1 * v.re, w1 * v.im});
+    const int bar = (int)((r >> a) & 1), bbr = (int)((r >> b) & 1), bac = (int)((c >> a) & 1), bbc = (int)((c >> b) & 1);
+    for (const auto& P : PAULI15) {
+      const uint64_t perm = (P[0] ? ma : 0) | (P[1] ? mb : 0);
+      const int parity = (P[2] * (bar ^ bac)) ^ (P[3] * (bbr ^ bbc));
+      const double s = parity ? -w2 : w2;
+      dm_acc(next, ((r ^ perm) << n) | (c ^ perm), C{s * v.re, s * v.im});
+    }
+  }
+  return next;
+}
+
+// runDM's csrswap (:532-575): blocks by the control bit of row and column
+static DMap dm_csrswap(const DMap& dm, int n, int ctl, int a, int b) {
+  const uint64_t cm = uint64_t(1) << ctl, dim_mask = (uint64_t(1) << n) - 1;
+  const Mat S = {ONE, ZERO, ZERO, ZERO, ZERO, cx(sq2, 0), cx(0, sq2), ZERO,
+                 ZERO, cx(0, sq2), cx(sq2, 0), ZERO, ZERO, ZERO, ZERO, ONE};
+  DMap blk[4];
+  for (const auto& kv : dm) {
+    const uint64_t r = kv.first >> n, c = kv.first & dim_mask;
+    blk[((r & cm) ? 2 : 0) | ((c & cm) ? 1 : 0)][kv.first] = kv.second;
+  }
+  const std::vector<int> ab = {a, b};
+  DMap d11 = dm_unitary(blk[3], n, ab, S);
+  DMap t01;
+  for (const auto& kv : blk[1]) t01[((kv.first & dim_mask) << n) | (kv.first >> n)] = kv.second;
+  DMap t01a = dm_unitary(t01, n, ab, S), d01;
+  for (const auto& kv : t01a) d01[((kv.first & dim_mask) << n) | (kv.first >> n)] = kv.second;
+  DMap d10 = dm_unitary(blk[2], n, ab, S);
+  DMap out = blk[0];
+  for (const DMap* m : {&d01, &d10, &d11})
+    for (const auto& kv : *m) dm_acc(out, kv.first, kv.second);
+  return out;
+}
+
+// controlledGate (mps.ts:53-60): diag(I, G), control = first (most significant) qubit
+static Mat controlled_gate(const Mat& g) {
+  return {ONE, ZERO, ZERO, ZERO, ZERO, ONE, ZERO, ZERO, ZERO, ZERO, g[0], g[1], ZERO, ZERO, g[2], g[3]};
+}
+
+// runDM (:475-588)
+static DMap run_dm(const Circuit& c, double p1, double p2) {
+  const int n = c.n;
+  DMap dm;
+  dm[0] = ONE;
+  for (const Op& op : c.ops) {
+    const std::vector<int>& q = op.q;
+    switch (op.kind) {
+      case K_SINGLE:
+        dm = dm_single(dm, n, q[0], op.m);
+        if (p1) dm = dm_dep1(dm, n, q[0], p1);
+        break;
+      case K_CNOT: {
+        const uint64_t cm = uint64_t(1) << q[0], tm = uint64_t(1) << q[1];
+        dm = dm_perm(dm, n, [=](uint64_t i) { return (i & cm) ? i ^ tm : i; });
+        if (p2) dm = dm_dep2(dm, n, q[0], q[1], p2);
+        break;
+      }
+      case K_SWAP: {
+        const uint64_t am = uint64_t(1) << q[0], bm = uint64_t(1) << q[1];
+        dm = dm_perm(dm, n, [=](uint64_t i) { return (((i & am) != 0) == ((i & bm) != 0)) ? i : i ^ am ^ bm; });
+        if (p2) dm = dm_dep2(dm, n, q[0], q[1], p2);
+        break;
+      }
+      case K_TWO:
+        dm = dm_unitary(dm, n, {q[0], q[1]}, op.m);
+        if (p2) dm = dm_dep2(dm, n, q[0], q[1], p2);
+        break;
+      case K_CONTROLLED:
+        dm = dm_unitary(dm, n, {q[0], q[1]}, controlled_gate(op.m));
+        if (p2) dm = dm_dep2(dm, n, q[0], q[1], p2);
+        break;
+      case K_TOFFOLI: {
+        const uint64_t c1 = uint64_t(1) << q[0], c2 = uint64_t(1) << q[1], tm = uint64_t(1) << q[2];
+        dm = dm_perm(dm, n, [=](uint64_t i) { return ((i & c1) && (i & c2)) ? i ^ tm : i; });
+        break;
+      }
+      case K_CSWAP: {
+        const uint64_t cm = uint64_t(1) << q[0], am = uint64_t(1) << q[1], bm = uint64_t(1) << q[2];
+        dm = dm_perm(dm, n, [=](uint64_t i) {
+          if (!(i & cm)) return i;
+          return (((i & am) != 0) == ((i & bm) != 0)) ? i : i ^ am ^ bm;
+        });
+        break;
+      }
+      case K_CSRSWAP: dm = dm_csrswap(dm, n, q[0], q[1], q[2]); break;
+      case K_UNITARY: dm = dm_unitary(dm, n, q, op.m); break;
+      default: break;  // barrier (measure / reset / if are refused by the caller)
+    }
+  }
+  return dm;
+}
+
+// DensityMatrix.entropy's Jacobi eigenvalue solver (:382-440), restated
+static std::vector<double> jacobi_eigenvalues(std::vector<double> R, std::vector<double> I, int n) {
+  for (int sweep = 0; sweep < 30 * n; sweep++) {
+    double max_off = 0;
+    for (int p = 0; p < n - 1; p++)
+      for (int q = p + 1; q < n; q++) {
+        const double o = R[p * n + q] * R[p * n + q] + I[p * n + q] * I[p * n + q];
+        if (o > max_off) max_off = o;
+      }
+    if (max_off < 1e-28) break;
+    for (int p = 0; p < n - 1; p++)
+      for (int q = p + 1; q < n; q++) {
+        const double ore = R[p * n + q], oim = I[p * n + q], off2 = ore * ore + oim * oim;
+        if (off2 < 1e-28) continue;
+        const double phi = std::atan2(oim, ore), mag = std::sqrt(off2);
+        const double tau = (R[q * n + q] - R[p * n + p]) / 2;
+        const double t = mag / (std::fabs(tau) + std::sqrt(tau * tau + mag * mag)) * (tau < 0 ? -1 : 1);
+        const double cg = 1 / std::sqrt(1 + t * t), sg = t * cg;
+        const double sre = sg * std::cos(phi), sim = sg * std::sin(phi);
+        for (int k = 0; k < n; k++) {
+          const double xr = R[p * n + k], xi = I[p * n + k], yr = R[q * n + k], yi = I[q * n + k];
+          R[p * n + k] = cg * xr + sre * yr - sim * yi;
+          I[p * n + k] = cg * xi + sre * yi + sim * yr;
+          R[q * n + k] = -sre * xr + sim * xi + cg * yr;
+          I[q * n + k] = -sre * xi - sim * xr + cg * yi;
+        }
+        for (int k = 0; k < n; k++) {
+          const double xr = R[k * n + p], xi = I[k * n + p], yr = R[k * n + q], yi = I[k * n + q];
+          R[k * n + p] = cg * xr + sre * yr + sim * yi;
+          I[k * n + p] = cg * xi + sre * yi - sim * yr;
+          R[k * n + q] = -sre * xr + sim * xi + cg * yr;
+          I[k * n + q] = -sre * xi - sim * xr + cg * yi;
+        }
+      }
+  }
+  std::vector<double> ev(n);
+  for (int i = 0; i < n; i++) ev[i] = R[i * n + i];
+  return ev;
+}
+
 // ---------------------------------------------------------------- algorithms.ts
 static Circuit qft(int n) {                       // algorithms.ts:16-26
   Circuit c{n, {}};
@@ -1040,6 +1311,54 @@ int orc_add_if(void* cp, int reg0, int regn, int value, void* body) {
 uint32_t orc_run_pershot(void* cp, uint64_t init, int shots, uint32_t seed, double p1, double p2, double pm,
                          int ncbits, uint64_t* out_idx, uint8_t* out_bits) {
   return run_pershot(*(Circuit*)cp, init, shots, seed, Noise{p1, p2, pm}, ncbits, out_idx, out_bits);
+}
+
+// runDM and the DensityMatrix read-outs (density.ts:274-372, :475-588)
+void* orc_dm_run(void* cp, double p1, double p2) { return new DMap(run_dm(*(Circuit*)cp, p1, p2)); }
+void orc_dm_free(void* h) { delete (DMap*)h; }
+uint64_t orc_dm_nnz(void* h) { return ((DMap*)h)->size(); }
+// rho as a dense 2^n x 2^n row-major complex matrix
+void orc_dm_dense(void* h, int n, double* out) {
+  const uint64_t dim = uint64_t(1) << n;
+  std::memset(out, 0, sizeof(double) * 2 * dim * dim);
+  for (const auto& kv : *(DMap*)h) {
+    out[2 * kv.first] = kv.second.re;
+    out[2 * kv.first + 1] = kv.second.im;
+  }
+}
+double orc_dm_purity(void* h) {  // purity (:314-318)
+  double p = 0;
+  for (const auto& kv : *(DMap*)h) p += kv.second.re * kv.second.re + kv.second.im * kv.second.im;
+  return p;
+}
+double orc_dm_entropy(void* h, int n) {  // entropy (:328-346)
+  const int dim = 1 << n;
+  std::vector<double> re((size_t)dim * dim), im((size_t)dim * dim);
+  for (const auto& kv : *(DMap*)h) {
+    re[kv.first] = kv.second.re;
+    im[kv.first] = kv.second.im;
+  }
+  double s = 0;
+  for (double lam : jacobi_eigenvalues(re, im, dim))
+    if (lam > 1e-14) s -= lam * std::log2(lam);
+  return s;
+}
+void orc_dm_bloch(void* h, int n, int q, double* out) {  // blochAngles (:356-372)
+  const uint64_t qm = uint64_t(1) << q, dim_mask = (uint64_t(1) << n) - 1;
+  double r00 = 0, r11 = 0, re = 0, im = 0;
+  for (const auto& kv : *(DMap*)h) {
+    const uint64_t r = kv.first >> n, c = kv.first & dim_mask;
+    if (r == c) {
+      if (!(r & qm)) r00 += kv.second.re;
+      else r11 += kv.second.re;
+    } else if (!(r & qm) && c == (r | qm)) {
+      re += kv.second.re;
+      im += kv.second.im;
+    }
+  }
+  const double rz = r00 - r11, rx = 2 * re, ry = -2 * im;
+  out[0] = std::acos(std::max(-1.0, std::min(1.0, rz)));
+  out[1] = std::atan2(ry, rx);
 }
 
 void orc_circuit_matrix(void* cp, double* out) { circuit_matrix(*(Circuit*)cp, out); }

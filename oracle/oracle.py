@@ -82,6 +82,13 @@ def lib():
         "orc_prng_next": (u32, [P(u32)]),
         "orc_time_ops": (u64, [vp, u64, i32, i32, i32, P(dbl)]),
         "orc_circuit_matrix": (None, [vp, P(dbl)]),
+        "orc_dm_run": (vp, [vp, dbl, dbl]),
+        "orc_dm_free": (None, [vp]),
+        "orc_dm_nnz": (u64, [vp]),
+        "orc_dm_dense": (None, [vp, i32, P(dbl)]),
+        "orc_dm_purity": (dbl, [vp]),
+        "orc_dm_entropy": (dbl, [vp, i32]),
+        "orc_dm_bloch": (None, [vp, i32, i32, P(dbl)]),
         "orc_bloch": (None, [vp, i32, P(dbl)]),
         "orc_add_measure": (i32, [vp, i32, i32]),
         "orc_add_reset": (i32, [vp, i32]),
@@ -195,6 +202,10 @@ class OCircuit:
                                      bits.ctypes.data_as(C.POINTER(C.c_uint8)))
         return idx[:shots], bits[: shots * ncbits].reshape(shots, ncbits), int(st)
 
+    def dm(self, p1: float = 0.0, p2: float = 0.0) -> "ODM":
+        """runDM (density.ts:475-588) with depolarizing noise p1, p2."""
+        return ODM(self._L.orc_dm_run(self.h_, p1, p2), self.qubits)
+
     def circuit_matrix(self) -> np.ndarray:
         """circuitMatrix() (circuit.ts:1462-1485): one sparse simulation per column."""
         dim = 1 << self.qubits
@@ -227,6 +238,46 @@ def _terms(terms, n):
     ops = "".join(t[1] for t in terms)
     assert all(len(t[1]) == n for t in terms)
     return coeffs, ops.encode()
+
+
+class ODM:
+    """The oracle's density matrix (density.ts DensityMatrix)."""
+
+    def __init__(self, handle, n):
+        self._L = lib()
+        self.h_ = handle
+        self.n = n
+
+    def __del__(self):
+        try:
+            self._L.orc_dm_free(self.h_)
+        except Exception:
+            pass
+
+    def dense(self) -> np.ndarray:
+        dim = 1 << self.n
+        out = np.zeros((dim, dim), dtype=np.complex128)
+        self._L.orc_dm_dense(self.h_, self.n, out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+    def nnz(self) -> int:
+        return int(self._L.orc_dm_nnz(self.h_))
+
+    def purity(self) -> float:
+        return self._L.orc_dm_purity(self.h_)
+
+    def entropy(self) -> float:
+        return self._L.orc_dm_entropy(self.h_, self.n)
+
+    def bloch(self, q: int):
+        out = np.zeros(2)
+        self._L.orc_dm_bloch(self.h_, self.n, q, _dp(out))
+        return out
+
+    def probabilities(self) -> dict:
+        """probabilities() (density.ts:299-307): q0-leftmost key -> Re rho[r][r] > 1e-14."""
+        d = np.real(np.diag(self.dense()))
+        return {format(r, "b").zfill(self.n)[::-1]: float(v) for r, v in enumerate(d) if v > 1e-14}
 
 
 class OState:

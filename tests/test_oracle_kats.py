@@ -232,3 +232,79 @@ def test_bloch_kats_oracle(kat):
     assert abs(out[4] - theta) < tol(td)
     if phi is not None:
         assert abs(out[5] - phi) < tol(pd)
+
+
+# dm() (circuit.test.ts:5017-5245), restated: (id, n, gates, noise {p1, p2}, checks)
+#   ("purity", x, digits) ("purity_lt", x) ("prob", bits, x, digits) ("absent", bits)
+#   ("entropy", x, digits) ("entropy_in", lo, hi) ("theta", x, digits) ("phi", x, digits)
+#   ("get", row, col, re, digits) ("total", x, digits)
+H0 = ("h", [0], [])
+BELL = [H0, ("cnot", [0, 1], [])]
+DM_KATS = [
+    ("pure0", 1, [], None, [("purity", 1, 10), ("prob", "0", 1, 10), ("absent", "1"), ("entropy", 0, 10),
+                            ("theta", 0, 10), ("get", 0, 0, 1, 10), ("get", 1, 1, 0, 10), ("get", 0, 1, 0, 10)]),
+    ("pure1", 1, [("x", [0], [])], None, [("purity", 1, 10), ("absent", "0"), ("prob", "1", 1, 10),
+                                          ("theta", math.pi, 10)]),
+    ("plus", 1, [H0], None, [("purity", 1, 10), ("prob", "0", 0.5, 10), ("prob", "1", 0.5, 10), ("entropy", 0, 10),
+                             ("theta", math.pi / 2, 10), ("phi", 0, 10)]),
+    ("bell", 2, BELL, None, [("purity", 1, 10), ("prob", "00", 0.5, 10), ("prob", "11", 0.5, 10), ("absent", "01"),
+                             ("absent", "10"), ("entropy", 0, 10)]),
+    ("hhh", 3, [H0, ("h", [1], []), ("h", [2], [])], None, [("prob", "000", 0.125, 10), ("prob", "111", 0.125, 10)]),
+    ("noisy_h", 1, [H0], {"p1": 0.1}, [("purity_lt", 1), ("get", 0, 1, (1 - 4 * 0.1 / 3) * 0.5, 8)]),
+    ("p1_zero", 1, [H0], {"p1": 0}, [("purity", 1, 10)]),
+    ("noisy_bell", 2, BELL, {"p2": 0.05}, [("purity_lt", 1)]),
+    ("dep_02", 1, [H0], {"p1": 0.2}, [("entropy_in", 0, 1)]),
+    ("max_mixed", 1, [H0], {"p1": 0.75}, [("entropy", 1, 6)]),
+    ("noisy_total", 2, BELL, {"p1": 0.05, "p2": 0.05}, [("total", 1, 8)]),
+    ("ccx", 3, [("x", [0], []), ("x", [1], []), ("ccx", [0, 1, 2], [])], None, [("purity", 1, 10), ("prob", "111", 1, 10)]),
+    ("ccx_off", 3, [("x", [2], []), ("ccx", [0, 1, 2], [])], None, [("prob", "001", 1, 10)]),
+    ("cswap", 3, [("x", [0], []), ("x", [2], []), ("cswap", [0, 1, 2], [])], None, [("prob", "110", 1, 10)]),
+    ("cswap_off", 3, [("x", [2], []), ("cswap", [0, 1, 2], [])], None, [("prob", "001", 1, 10)]),
+]
+
+
+def check_dm(case, probs, purity, entropy, bloch, get):
+    for chk in case[4]:
+        k = chk[0]
+        if k == "purity":
+            assert abs(purity - chk[1]) < tol(chk[2]), (case[0], purity)
+        elif k == "purity_lt":
+            assert purity < chk[1], (case[0], purity)
+        elif k == "prob":
+            assert abs(probs.get(chk[1], 0.0) - chk[2]) < tol(chk[3]), (case[0], probs)
+        elif k == "absent":
+            assert chk[1] not in probs, (case[0], probs)
+        elif k == "entropy":
+            assert abs(entropy() - chk[1]) < tol(chk[2]), case[0]
+        elif k == "entropy_in":
+            assert chk[1] < entropy() < chk[2], case[0]
+        elif k == "theta":
+            assert abs(bloch(0)[0] - chk[1]) < tol(chk[2]), case[0]
+        elif k == "phi":
+            assert abs(bloch(0)[1] - chk[1]) < tol(chk[2]), case[0]
+        elif k == "get":
+            assert abs(get(chk[1], chk[2]).real - chk[3]) < tol(chk[4]), case[0]
+        elif k == "total":
+            assert abs(sum(probs.values()) - chk[1]) < tol(chk[2]), case[0]
+        else:
+            raise AssertionError(k)
+
+
+@pytest.mark.parametrize("case", DM_KATS, ids=[c[0] for c in DM_KATS])
+def test_dm_kats_oracle(case):
+    _, n, gates, noise, _ = case
+    nz = noise or {}
+    d = _ocirc(n, gates).dm(nz.get("p1", 0.0), nz.get("p2", 0.0))
+    dense = d.dense()
+    check_dm(case, d.probabilities(), d.purity(), d.entropy, d.bloch, lambda r, c: dense[r, c])
+
+
+def test_dm_noise_ordering_oracle():
+    """circuit.test.ts:5147-5153, :5175-5186: purity falls with noise; forte-1 is
+    cleaner than harmony; aria-1 is noisier than none."""
+    ps = [_ocirc(1, [H0]).dm(p, 0).purity() for p in (0.01, 0.1, 0.3)]
+    assert ps[0] > ps[1] > ps[2]
+    forte = _ocirc(2, BELL).dm(0.0001, 0.002).purity()
+    harmony = _ocirc(2, BELL).dm(0.001, 0.015).purity()
+    assert forte > harmony
+    assert _ocirc(2, BELL).dm(0.0003, 0.005).purity() < _ocirc(2, BELL).dm().purity()
