@@ -390,7 +390,8 @@ def extras():
                  of a 12-qubit brickwork with a mid-circuit measure and reset;
                  shot records checked against the oracle on a sample
       json       loading the 30-qubit workload's circuit JSON with the C ABI's
-                 loader and with the Python mirror's Circuit.fromJSON"""
+                 loader and with the Python mirror's Circuit.fromJSON
+      dm         density matrices with aria-1 noise (8 and 12 qubits)"""
     import numpy as np
 
     from ket_b200 import KET_C64, workloads as W
@@ -443,8 +444,39 @@ def extras():
                         "c64_33q_gates_per_s": k / t33, "c64_33q_norm": n33}
     out["pershot"] = pershot_measure()
     out["json"] = json_measure()
+    out["dm"] = dm_measure()
     return out
 
+
+def dm_measure():
+    """dm() with the aria-1 noise profile: brickwork(8, 10) on the engine and
+    on the oracle's restatement of runDM (the CPU checker), with the largest
+    entry difference, and brickwork(12, 10) on the engine alone."""
+    import numpy as np
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import flatten_ops
+    res = {"noise": "aria-1", "unit": "seconds per dm() (wall clock)"}
+    for n in (8, 12):
+        c, _ = W.brickwork_circuit(n, 10, 42)
+        c.dm(noise="aria-1")
+        t = time.perf_counter()
+        d = c.dm(noise="aria-1")
+        res[f"engine_{n}q_s"] = time.perf_counter() - t
+        res[f"purity_{n}q"] = d.purity()
+        if n == 8:
+            try:
+                from oracle import oracle as O
+            except Exception as e:
+                res["oracle"] = f"unavailable: {e}"
+                continue
+            oc = O.OCircuit(n)
+            for op in flatten_ops(c.ops):
+                oc.add(op.name, list(op.qubits), list(op.params))
+            t = time.perf_counter()
+            o = oc.dm(0.0003, 0.005)
+            res["oracle_8q_s"] = time.perf_counter() - t
+            res["max_entry_diff_8q"] = float(np.max(np.abs(d.dense() - o.dense())))
+    return res
 
 def json_measure(reps: int = 20):
     """Loading ket's circuit JSON for the 30-qubit workload (2260 gates):
