@@ -53,6 +53,9 @@ def parse_args():
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--layers", type=int, default=40)
     ap.add_argument("--prune", type=int, default=1, help="1: reference pruning semantics (default), 0: plain dense")
+    ap.add_argument("--specialize", type=int, default=1,
+                    help="register-tiled passes: 1 kernels compiled per pass program (compiled during warm-up), "
+                         "-1 the interpreter k_fused2, 0 automatic")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the VQE-gradient, QAOA-batch and complex64 measurements")
@@ -276,13 +279,18 @@ def run_ket(args):
 
     def step():
         st.set_basis(0)
-        st.apply_abi(arr, mats, k, prune=prune)
+        st.apply_abi(arr, mats, k, prune=prune, specialize=args.specialize)
         a = st.amplitudes(idx_arr)
         md = st.marginal_dist(marg_q)
         return a, md
 
+    tw = time.perf_counter()
     for _ in range(args.warmup):
         step()
+    warm_s = time.perf_counter() - tw
+    jst, jcs = (C.c_int64 * 4)(), C.c_double()
+    _lib.check(L.ket_jit_stats(jst, C.byref(jcs)))
+    jit0 = list(jst)
 
     def counters():
         lc = C.c_uint64()
@@ -321,6 +329,8 @@ def run_ket(args):
     kinds_all, ms_all = list(kinds[: cnt.value]), list(ms[: cnt.value])
     L.ket_ctx_profile(ctx, 0)
 
+    _lib.check(L.ket_jit_stats(jst, C.byref(jcs)))
+    jit_launches = jst[3] - jit0[3]
     dev_s = ev0.elapsed_time(ev1) / 1e3
     dev_max = dist.max(dev_s)
     wall_max = dist.max(wall)
@@ -352,13 +362,19 @@ def run_ket(args):
                    "pruning": "reference (|a|^2<1e-14 flushed per gate)" if prune else "off (plain dense)",
                    "l2_flush": "not needed: 16 GiB state > 126 MB L2",
                    "parallelism": f"replicas x{world}",
-                   "kernel_busy_ms_per_step": busy_s / args.steps * 1e3},
+                   "kernel_busy_ms_per_step": busy_s / args.steps * 1e3,
+                   "pass_kernels": (f"compiled per pass program at run time ({jit_launches} of {len(fused)} "
+                                    f"timed passes; {jst[1]} kernels compiled during warm-up in {warm_s:.1f} s "
+                                    f"wall, cached by program shape, matrices read at run time)")
+                   if jit_launches else "interpreter (k_fused2)"},
         "e2e": {"value": e2e, "unit": "gates/s", "h2d_bytes_per_step": (c1[1] - c0[1]) // args.steps,
                 "d2h_bytes_per_step": (c1[2] - c0[2]) // args.steps},
         "gpu_launches": c1[0] - c0[0],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                     "traffic": ncu_traffic(n), "kernel": "k_fused2 (register-tiled fused pass)",
+                     "traffic": ncu_traffic(n),
+                     "kernel": "ket_pass (register-tiled fused pass compiled per program)" if jit_launches
+                     else "k_fused2 (register-tiled fused pass)",
                      "bytes_per_launch": bytes_per_launch},
         "clocks": clk,
     }

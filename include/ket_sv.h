@@ -91,7 +91,12 @@ typedef struct ket_exec_opts {
   int32_t fusion;      /* -1 = automatic (default), 0 = one pass per gate, k > 0 = tile width cap (qubits) */
   int32_t prune;       /* 1 = reference accumulate() semantics: every computed amplitude with
                           |a|^2 < 1e-14 is flushed to zero (statevector.ts:19-27); 0 = plain dense */
-  int32_t reserved[6];
+  int32_t specialize;  /* register-tiled passes: 0 = automatic (default): kernels compiled for the
+                          pass's program where one is ready, the interpreter otherwise, compiling
+                          on background threads for states of 26+ qubits; 1 = compile what is
+                          missing first, then use compiled kernels only; -1 = interpreter only.
+                          Results are identical either way.  No counterpart in the reference. */
+  int32_t reserved[5];
 } ket_exec_opts;
 
 /* NoiseParams (circuit.ts:213-221): depolarizing probability per single-qubit
@@ -194,6 +199,19 @@ KET_API int ket_plan_stats(int nqubits, int precision, const ket_op* ops, size_t
  * counts[15] = other passes.  No counterpart in the reference. */
 KET_API int ket_plan_program_stats(int nqubits, int precision, const ket_op* ops, size_t nops, const double* mats,
                                    size_t nmat, const ket_exec_opts* opts, int64_t counts[16]);
+
+/* Run-time compiled pass kernels (ket_exec_opts.specialize).  ket_jit_wait
+ * blocks until no compile is queued or running (KET_ERR_CUDA if one failed);
+ * ket_jit_stats: out = {kernels known, compiled, failed, launches} and the
+ * compile seconds summed over threads.  ket_jit_compile plans an op list as
+ * ket_apply_ops would for an nqubits state and compiles, on all host cores,
+ * the kernel of every register-tiled pass that is not compiled yet (no GPU
+ * needed); *kernels = the number of distinct kernels the plan uses, log = a
+ * failed compile's log (logcap bytes).  No counterpart in the reference. */
+KET_API int ket_jit_wait(void);
+KET_API int ket_jit_stats(int64_t out[4], double* compile_seconds);
+KET_API int ket_jit_compile(int nqubits, int precision, const ket_op* ops, size_t nops, const double* mats,
+                            size_t nmat, const ket_exec_opts* opts, int64_t* kernels, char* log, size_t logcap);
 
 /* ---------------------------------------------------------------- read-outs */
 /* amplitude(): out[2i], out[2i+1] = re, im of amplitude idx[i] (circuit.ts:1491-1495). */

@@ -47,7 +47,7 @@ class ket_noise(C.Structure):
 
 
 class ket_exec_opts(C.Structure):
-    _fields_ = [("fusion", C.c_int32), ("prune", C.c_int32), ("reserved", C.c_int32 * 6)]
+    _fields_ = [("fusion", C.c_int32), ("prune", C.c_int32), ("specialize", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class ket_param_binding(C.Structure):
@@ -97,6 +97,10 @@ def lib():
             "ket_state_copy": (i32, [vp, vp]),
             "ket_apply_ops": (i32, [vp, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts)]),
             "ket_plan_stats": (i32, [i32, i32, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts), P(C.c_int64)]),
+            "ket_jit_wait": (i32, []),
+            "ket_jit_stats": (i32, [P(C.c_int64), P(dbl)]),
+            "ket_jit_compile": (i32, [i32, i32, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts), P(C.c_int64),
+                                    C.c_char_p, sz]),
             "ket_plan_program_stats": (i32, [i32, i32, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts),
                                              P(C.c_int64)]),
             "ket_amplitudes": (i32, [vp, P(u64), sz, P(dbl)]),
@@ -164,9 +168,10 @@ def default_ctx():
     return _ctx
 
 
-def exec_opts(fusion: int = -1, prune: bool = True) -> ket_exec_opts:
+def exec_opts(fusion: int = -1, prune: bool = True, specialize: int = 0) -> ket_exec_opts:
     o = ket_exec_opts()
     lib().ket_exec_opts_default(C.byref(o))
     o.fusion = fusion
     o.prune = 1 if prune else 0
+    o.specialize = specialize
     return o

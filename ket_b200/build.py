@@ -20,7 +20,29 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr",
-          "-I", os.path.join(HERE, "..", "include")]
+          "-I", os.path.join(HERE, "..", "include"), "-I", BUILD]
+
+
+# Device headers compiled into the run-time pass kernels (jit.cpp), embedded
+# in the library as strings.
+JIT_HEADERS = ["fused_abi.h", "common.cuh", "fused_ops.cuh", "jit_ops.cuh"]
+JIT_INC = os.path.join(BUILD, "jit_sources.inc")
+
+
+def write_jit_sources() -> None:
+    parts = ["// Written by ket_b200/build.py from the headers it names: do not edit.",
+             "struct JitHeader { const char* name; const char* text; };",
+             "static const JitHeader kJitHeaders[] = {"]
+    for h in JIT_HEADERS:
+        text = open(os.path.join(CSRC, h)).read()
+        if ")KETJIT\"" in text:
+            raise RuntimeError(f"{h} holds the raw-string delimiter")
+        parts.append(f'  {{"{h}", R"KETJIT({text})KETJIT"}},')
+    parts.append("};")
+    data = "\n".join(parts) + "\n"
+    if not os.path.exists(JIT_INC) or open(JIT_INC).read() != data:
+        with open(JIT_INC, "w") as f:
+            f.write(data)
 
 
 def sources():
@@ -56,12 +78,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force:
         for f in os.listdir(BUILD):
             os.remove(os.path.join(BUILD, f))
+    write_jit_sources()
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

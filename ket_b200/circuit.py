@@ -893,15 +893,17 @@ class DeviceState:
         check(lib().ket_state_set_amplitudes(self.h, offset, a.size, a.view(np.float64).ctypes.data_as(
             C.POINTER(C.c_double))))
 
-    def apply(self, ops, fusion: int = -1, prune: bool = True):
+    def apply(self, ops, fusion: int = -1, prune: bool = True, specialize: int = 0):
         arr, m, k = ops_to_abi(ops)
         mv = np.ascontiguousarray(m).view(np.float64)
-        o = exec_opts(fusion, prune)
+        o = exec_opts(fusion, prune, specialize)
         check(lib().ket_apply_ops(self.h, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, C.byref(o)))
 
-    def apply_abi(self, arr, m, k, fusion: int = -1, prune: bool = True):
+    def apply_abi(self, arr, m, k, fusion: int = -1, prune: bool = True, specialize: int = 0):
+        """specialize: 0 automatic, 1 run-time compiled pass kernels (compiled
+        first where missing), -1 the interpreter only."""
         mv = np.ascontiguousarray(m).view(np.float64)
-        o = exec_opts(fusion, prune)
+        o = exec_opts(fusion, prune, specialize)
         check(lib().ket_apply_ops(self.h, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, C.byref(o)))
 
     def amplitudes_dense(self) -> np.ndarray:

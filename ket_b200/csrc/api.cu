@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "ctx.h"
 #include "launch.h"
+#include "jit.h"
 #include "read.h"
 
 namespace ket {
@@ -380,6 +381,48 @@ int ket_plan_program_stats(int n, int precision, const ket_op* ops, size_t nops,
   return KET_OK;
 }
 
+int ket_jit_wait(void) {
+  const int rc = jit_wait_all();
+  return rc ? fail(rc, "a run-time compile of a pass kernel failed") : KET_OK;
+}
+
+int ket_jit_stats(int64_t out[4], double* compile_seconds) {
+  if (!out) return fail(KET_ERR_TYPE, "null argument");
+  jit_stats(out, compile_seconds);
+  return KET_OK;
+}
+
+int ket_jit_compile(int n, int precision, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
+                    const ket_exec_opts* opts, int64_t* kernels, char* log, size_t logcap) {
+  ket_exec_opts o;
+  if (opts) o = *opts; else ket_exec_opts_default(&o);
+  if (n < 1 || n > KET_MAX_QUBITS) return fail(KET_ERR_RANGE, "qubit count out of range");
+  if (kernels) *kernels = 0;
+  if (log && logcap) log[0] = 0;
+  Plan plan;
+  std::string err;
+  int rc = lower_ops(n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
+  if (rc) return fail(rc, err);
+  if (o.fusion != 0) fold_single_qubit(plan.gates, o.prune != 0);
+  plan_passes(n, precision, o.fusion, o.prune != 0, plan);
+  std::vector<std::vector<FOp>> progs;
+  for (auto& p : plan.passes) {
+    if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) continue;
+    progs.emplace_back();
+    uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
+    plan_program(plan, p, precision, o.prune != 0, KET_FUSED_NREG, progs.back(), lp, sp);
+  }
+  std::vector<JitPass> jp;
+  for (auto& pr : progs) jp.push_back(JitPass{pr.data(), (int)pr.size(), n});
+  std::string clog;
+  rc = jit_compile(jp, precision, kernels, clog);
+  if (log && logcap) {
+    strncpy(log, clog.c_str(), logcap - 1);
+    log[logcap - 1] = 0;
+  }
+  return rc ? fail(rc, "run-time compile of a pass kernel failed") : KET_OK;
+}
+
 int ket_apply_ops(ket_state* s, const ket_op* ops, size_t nops, const double* mats, size_t nmat,
                   const ket_exec_opts* opts) {
   if (!s) return fail(KET_ERR_TYPE, "null state");
@@ -474,6 +517,16 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
     cudaError_t e = cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(ops)");
   }
+  // run-time compiled kernels for the register-tiled passes (jit.cpp)
+  std::vector<JitFn> jf;
+  {
+    std::vector<JitPass> jp(np);
+    for (size_t i = 0; i < np; i++)
+      if (use2[i] && p2[i].nslots == 0) jp[i] = JitPass{fops.data() + off[i], p2[i].nops, s->n};
+    std::string err;
+    int rc = jit_prepare(jp, s->precision, o.specialize, c->device, jf, err);
+    if (rc) return fail(rc, err);
+  }
   const FOp* dfops = reinterpret_cast<const FOp*>(dev);
   const DevOp* dops = reinterpret_cast<const DevOp*>((const char*)dev + f_bytes);
   for (size_t i = 0; i < np; i++) {
@@ -483,7 +536,7 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
     prof_begin(c);
     if (use2[i]) {
       p2[i].ops = dfops + off[i];
-      e = launch_fused2(p2[i], s->precision, c->stream);
+      e = jf[i].fn ? jit_launch(jf[i], p2[i], s->precision, c->stream) : launch_fused2(p2[i], s->precision, c->stream);
     } else if (p.fused) {
       PassArgs a;
       memset(&a, 0, sizeof(a));

@@ -1,8 +1,10 @@
 // common.cuh -- device-side helpers shared by the engine's kernels.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 namespace ket {
 

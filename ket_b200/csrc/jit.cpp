@@ -1,0 +1,412 @@
+// jit.cpp -- register-tiled pass kernels compiled at run time, one per program shape.
+//
+// The interpreter k_fused2 pays, on every op of every tile, an op fetch, a
+// dispatch and, for X and CNOT on register bits, register moves.  This file
+// writes, for the program of one pass, a kernel with one compile-time step per
+// op (jit_ops.cuh) and compiles it with NVRTC for sm_100a.  A kernel depends
+// only on the program's shape -- each op's code, pruning flag and controls --
+// while the data (matrices, layouts, qubits, masks) stays in the op records
+// the interpreter reads, so the cache (keyed by shape) serves every circuit
+// and every parameter set with the same structure.
+//
+// Policy (ket_exec_opts.specialize):
+//  -1   interpreter only;
+//   1   compile what is missing, waiting for it, then run compiled kernels;
+//   0   (default) run compiled kernels that are ready; passes of states of 26
+//       qubits or more whose kernel is missing run on the interpreter and
+//       queue the compile on background threads, so a repeated circuit speeds
+//       up without a first call that waits for the compiler.
+//
+// NVRTC is loaded with dlopen on first use and the driver entry points come
+// from the runtime (cudaGetDriverEntryPoint): the library links neither.
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda.h>
+
+#include "launch.h"
+#include "jit.h"
+#include "jit_sources.inc"  // kJitHeaders: the device headers as strings (written by build.py)
+
+namespace ket {
+namespace {
+
+// ---------------------------------------------------------------- NVRTC
+typedef int nvrtcResult_t;
+typedef struct _nvrtcProgram* nvrtcProgram_t;
+struct Nvrtc {
+  bool ok = false;
+  std::string err;
+  nvrtcResult_t (*create)(nvrtcProgram_t*, const char*, const char*, int, const char* const*, const char* const*);
+  nvrtcResult_t (*compile)(nvrtcProgram_t, int, const char* const*);
+  nvrtcResult_t (*cubin_size)(nvrtcProgram_t, size_t*);
+  nvrtcResult_t (*cubin)(nvrtcProgram_t, char*);
+  nvrtcResult_t (*log_size)(nvrtcProgram_t, size_t*);
+  nvrtcResult_t (*log)(nvrtcProgram_t, char*);
+  nvrtcResult_t (*destroy)(nvrtcProgram_t*);
+};
+
+Nvrtc load_nvrtc() {
+  Nvrtc n;
+  const char* names[] = {"libnvrtc.so.12", "/usr/local/cuda/lib64/libnvrtc.so.12", "libnvrtc.so"};
+  void* h = nullptr;
+  for (const char* nm : names)
+    if ((h = dlopen(nm, RTLD_NOW | RTLD_LOCAL))) break;
+  if (!h) {
+    n.err = "NVRTC (libnvrtc.so.12) not found";
+    return n;
+  }
+  auto sym = [&](const char* s) { return dlsym(h, s); };
+  n.create = (decltype(n.create))sym("nvrtcCreateProgram");
+  n.compile = (decltype(n.compile))sym("nvrtcCompileProgram");
+  n.cubin_size = (decltype(n.cubin_size))sym("nvrtcGetCUBINSize");
+  n.cubin = (decltype(n.cubin))sym("nvrtcGetCUBIN");
+  n.log_size = (decltype(n.log_size))sym("nvrtcGetProgramLogSize");
+  n.log = (decltype(n.log))sym("nvrtcGetProgramLog");
+  n.destroy = (decltype(n.destroy))sym("nvrtcDestroyProgram");
+  n.ok = n.create && n.compile && n.cubin_size && n.cubin && n.log_size && n.log && n.destroy;
+  if (!n.ok) n.err = "NVRTC is missing an entry point";
+  return n;
+}
+
+Nvrtc& nvrtc() {
+  static Nvrtc n = load_nvrtc();
+  return n;
+}
+
+// Compile one kernel source to an sm_100a cubin; false and a log on failure.
+bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string& log) {
+  Nvrtc& N = nvrtc();
+  if (!N.ok) {
+    log = N.err;
+    return false;
+  }
+  std::vector<const char*> hs, hn;
+  for (const JitHeader& h : kJitHeaders) {
+    hn.push_back(h.name);
+    hs.push_back(h.text);
+  }
+  nvrtcProgram_t prog = nullptr;
+  if (N.create(&prog, src.c_str(), "ket_pass.cu", (int)hs.size(), hs.data(), hn.data()) != 0) {
+    log = "nvrtcCreateProgram failed";
+    return false;
+  }
+  std::vector<const char*> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DNDEBUG"};
+  if (getenv("KET_JIT_VERBOSE")) opts.push_back("-Xptxas=-v");  // register and spill report in the log
+  const int rc = N.compile(prog, (int)opts.size(), opts.data());
+  size_t ls = 0;
+  N.log_size(prog, &ls);
+  if (ls > 1) {
+    log.resize(ls);
+    N.log(prog, &log[0]);
+  }
+  bool ok = rc == 0;
+  if (ok) {
+    size_t cs = 0;
+    ok = N.cubin_size(prog, &cs) == 0 && cs > 0;
+    if (ok) {
+      cubin.resize(cs);
+      ok = N.cubin(prog, cubin.data()) == 0;
+    }
+  }
+  N.destroy(&prog);
+  return ok;
+}
+
+// ---------------------------------------------------------------- driver entry points
+struct Driver {
+  bool ok = false;
+  CUresult (*load)(CUmodule*, const void*);
+  CUresult (*get)(CUfunction*, CUmodule, const char*);
+  CUresult (*attr)(CUfunction, CUfunction_attribute, int);
+  CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
+                     void**, void**);
+};
+
+Driver& driver() {
+  static Driver d = [] {
+    Driver r;
+    void* p[4] = {nullptr, nullptr, nullptr, nullptr};
+    const char* names[4] = {"cuModuleLoadData", "cuModuleGetFunction", "cuFuncSetAttribute", "cuLaunchKernel"};
+    bool ok = true;
+    for (int i = 0; i < 4; i++) {
+      cudaDriverEntryPointQueryResult q;
+      if (cudaGetDriverEntryPoint(names[i], &p[i], cudaEnableDefault, &q) != cudaSuccess ||
+          q != cudaDriverEntryPointSuccess || !p[i])
+        ok = false;
+    }
+    r.load = (decltype(r.load))p[0];
+    r.get = (decltype(r.get))p[1];
+    r.attr = (decltype(r.attr))p[2];
+    r.launch = (decltype(r.launch))p[3];
+    r.ok = ok;
+    return r;
+  }();
+  return d;
+}
+
+// ---------------------------------------------------------------- source
+const char* real_name(int precision) { return precision == KET_C64 ? "float" : "double"; }
+
+std::string make_source(const FOp* prog, int nops, int precision) {
+  const char* R = real_name(precision);
+  const int NR = KET_FUSED_NREG, NT = 32 << (7 - NR);
+  std::string s;
+  s.reserve(200 + 96 * (size_t)nops);
+  s += "#include \"jit_ops.cuh\"\n";
+  s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(NT) + ", 2) ket_pass(const ket::Pass2Args a) {\n";
+  s += "  using namespace ket;\n";
+  s += "  const FOp* o = a.ops;\n";
+  s += std::string("  jit::run_tiles<") + R + ", " + std::to_string(NR) + ">(a, [&](cpx<" + R + "> (&x)[" +
+       std::to_string(1 << NR) + "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
+  for (int k = 0; k < nops; k++) {
+    const FOp& f = prog[k];
+    if (f.type == FO_CONT || f.opc == OC_NOP) continue;
+    const unsigned fl = f.flags & (FOF_PRUNE | FOF_D0ONE);
+    s += std::string("    jit::step<") + R + ", " + std::to_string(NR) + ", " + std::to_string((int)f.opc) + ", " +
+         std::to_string(fl) + ", " + std::to_string((int)f.creg) + ", " + std::to_string((unsigned)f.cthr) + "u, " +
+         (f.cctx ? "true" : "false") + ">(x, sl, o + " + std::to_string(k) + ", t);\n";
+  }
+  s += "  });\n}\n";
+  return s;
+}
+
+// The shape of a program: what selects code in make_source.
+std::string shape_key(const FOp* prog, int nops, int precision) {
+  std::string k = precision == KET_C64 ? "f" : "d";
+  k.reserve(8 * (size_t)nops + 1);
+  for (int i = 0; i < nops; i++) {
+    const FOp& f = prog[i];
+    if (f.type == FO_CONT || f.opc == OC_NOP) {
+      k += '.';
+      continue;
+    }
+    const unsigned fl = f.flags & (FOF_PRUNE | FOF_D0ONE);
+    char buf[32];
+    snprintf(buf, sizeof buf, "%x,%x,%x,%x,%d;", (unsigned)f.opc, fl, (unsigned)f.creg, (unsigned)f.cthr,
+             f.cctx ? 1 : 0);
+    k += buf;
+  }
+  return k;
+}
+
+// A kernel's state: queued / compiling / compiled (cubin) / failed; modules per device.
+struct Entry {
+  enum { QUEUED, BUSY, READY, FAILED } st = QUEUED;
+  std::string src, log;
+  std::vector<char> cubin;
+  std::map<int, CUfunction> fn;  // device -> loaded kernel
+};
+
+struct Cache {
+  std::mutex mu;
+  std::condition_variable cv;       // a compile finished
+  std::condition_variable work;     // a job was queued
+  std::unordered_map<std::string, Entry> map;
+  std::deque<std::string> queue;
+  std::vector<std::thread> pool;
+  bool stop = false;
+  int busy = 0;
+  int64_t compiled = 0, failed = 0, launches = 0;
+  double compile_s = 0;
+
+  ~Cache() {
+    {
+      std::lock_guard<std::mutex> g(mu);
+      stop = true;
+      queue.clear();
+    }
+    work.notify_all();
+    for (auto& t : pool) t.join();
+  }
+
+  void start_pool() {  // under mu
+    if (!pool.empty()) return;
+    unsigned n = std::thread::hardware_concurrency();
+    n = n < 2 ? 2 : (n > 32 ? 32 : n);
+    for (unsigned i = 0; i < n; i++) pool.emplace_back([this] { worker(); });
+  }
+
+  void worker() {
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+      work.wait(lk, [this] { return stop || !queue.empty(); });
+      if (stop) return;
+      const std::string key = queue.front();
+      queue.pop_front();
+      Entry& e = map[key];
+      if (e.st != Entry::QUEUED) continue;
+      e.st = Entry::BUSY;
+      busy++;
+      const std::string src = e.src;
+      lk.unlock();
+      std::vector<char> cubin;
+      std::string log;
+      const auto t0 = std::chrono::steady_clock::now();
+      const bool ok = compile_cubin(src, cubin, log);
+      const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      lk.lock();
+      Entry& e2 = map[key];
+      e2.st = ok ? Entry::READY : Entry::FAILED;
+      e2.cubin.swap(cubin);
+      e2.log.swap(log);
+      busy--;
+      compile_s += dt;
+      (ok ? compiled : failed)++;
+      cv.notify_all();
+    }
+  }
+};
+
+Cache& cache() {
+  static Cache c;
+  return c;
+}
+
+}  // namespace
+
+namespace {
+
+// Queue the kernels of passes that are not known yet (under C.mu); keys[i] is
+// the shape of pass i, empty for a pass without a kernel or below min_qubits.
+std::vector<std::string> enqueue(Cache& C, const std::vector<JitPass>& passes, int precision, int min_qubits) {
+  std::vector<std::string> keys(passes.size());
+  bool queued = false;
+  for (size_t i = 0; i < passes.size(); i++) {
+    const JitPass& p = passes[i];
+    if (!p.prog || p.nqubits < min_qubits) continue;
+    keys[i] = shape_key(p.prog, p.nops, precision);
+    if (C.map.find(keys[i]) == C.map.end()) {
+      Entry& e = C.map[keys[i]];
+      e.src = make_source(p.prog, p.nops, precision);
+      C.queue.push_back(keys[i]);
+      queued = true;
+    }
+  }
+  if (queued) {
+    C.start_pool();
+    C.work.notify_all();
+  }
+  return keys;
+}
+
+// Wait until every listed kernel is compiled; false and its log if one failed.
+bool wait_keys(Cache& C, std::unique_lock<std::mutex>& lk, const std::vector<std::string>& keys, std::string& log) {
+  for (const std::string& k : keys) {
+    if (k.empty()) continue;
+    C.cv.wait(lk, [&] {
+      const Entry& e = C.map[k];
+      return e.st == Entry::READY || e.st == Entry::FAILED;
+    });
+    const Entry& e = C.map[k];
+    if (e.st == Entry::FAILED) {
+      log = e.log;
+      return false;
+    }
+  }
+  return true;
+}
+
+}  // namespace
+
+int jit_compile(const std::vector<JitPass>& passes, int precision, int64_t* distinct, std::string& log) {
+  Cache& C = cache();
+  std::unique_lock<std::mutex> lk(C.mu);
+  const std::vector<std::string> keys = enqueue(C, passes, precision, 0);
+  if (distinct) {
+    std::vector<std::string> u;
+    for (const std::string& k : keys)
+      if (!k.empty()) u.push_back(k);
+    std::sort(u.begin(), u.end());
+    *distinct = (int64_t)(std::unique(u.begin(), u.end()) - u.begin());
+  }
+  return wait_keys(C, lk, keys, log) ? KET_OK : KET_ERR_CUDA;
+}
+
+int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, int device, std::vector<JitFn>& out,
+                std::string& err) {
+  out.assign(passes.size(), JitFn{});
+  if (mode < 0) return KET_OK;
+  if (!driver().ok) {
+    if (mode == 1) return err = "driver entry points for run-time kernels are unavailable", KET_ERR_UNSUPPORTED;
+    return KET_OK;
+  }
+  Cache& C = cache();
+  std::unique_lock<std::mutex> lk(C.mu);
+  const std::vector<std::string> keys = enqueue(C, passes, precision, mode == 1 ? 0 : KET_JIT_AUTO_QUBITS);
+  if (mode == 1) {  // wait for every kernel this plan needs
+    std::string log;
+    if (!wait_keys(C, lk, keys, log)) return err = "run-time compile of a pass kernel failed: " + log, KET_ERR_CUDA;
+  }
+  Driver& D = driver();
+  for (size_t i = 0; i < passes.size(); i++) {
+    if (keys[i].empty()) continue;
+    Entry& e = C.map[keys[i]];
+    if (e.st != Entry::READY) continue;
+    auto f = e.fn.find(device);
+    if (f == e.fn.end()) {
+      CUmodule mod;
+      CUfunction fn;
+      if (D.load(&mod, e.cubin.data()) != CUDA_SUCCESS || D.get(&fn, mod, "ket_pass") != CUDA_SUCCESS) {
+        if (mode == 1) return err = "loading a run-time compiled pass kernel failed", KET_ERR_CUDA;
+        continue;
+      }
+      const int smem = (precision == KET_C64 ? 8 : 16) << KET_T2_BITS;
+      if (D.attr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem) != CUDA_SUCCESS) {
+        if (mode == 1) return err = "setting the shared memory of a pass kernel failed", KET_ERR_CUDA;
+        continue;
+      }
+      f = e.fn.emplace(device, fn).first;
+    }
+    out[i].fn = (void*)f->second;
+  }
+  return KET_OK;
+}
+
+cudaError_t jit_launch(const JitFn& f, const Pass2Args& in, int precision, cudaStream_t s) {
+  Pass2Args a = in;
+  fill_pass2_offsets(a, precision);
+  const int smem = (precision == KET_C64 ? 8 : 16) << KET_T2_BITS;
+  const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
+  const unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)fused2_grid(KET_FUSED_NREG));
+  void* params[1] = {&a};
+  const CUresult r = driver().launch((CUfunction)f.fn, blocks, 1, 1, 32 << (7 - KET_FUSED_NREG), 1, 1, smem,
+                                     (CUstream)s, params, nullptr);
+  {
+    std::lock_guard<std::mutex> g(cache().mu);
+    cache().launches++;
+  }
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;
+}
+
+int jit_wait_all() {
+  Cache& C = cache();
+  std::unique_lock<std::mutex> lk(C.mu);
+  C.cv.wait(lk, [&] { return C.queue.empty() && C.busy == 0; });
+  return C.failed ? KET_ERR_CUDA : KET_OK;
+}
+
+void jit_stats(int64_t out[4], double* compile_s) {
+  Cache& C = cache();
+  std::lock_guard<std::mutex> g(C.mu);
+  out[0] = (int64_t)C.map.size();
+  out[1] = C.compiled;
+  out[2] = C.failed;
+  out[3] = C.launches;
+  if (compile_s) *compile_s = C.compile_s;
+}
+
+}  // namespace ket

@@ -1,0 +1,291 @@
+// jit_ops.cuh -- the body of a register-tiled pass compiled for one program.
+//
+// k_fused2 interprets a program: every thread fetches each op's header,
+// dispatches on its op code and runs the matching code for the op's target
+// register bit, register controls and matrix form.  A pass kernel compiled
+// for one program (jit.cpp writes one `step<...>` call per op and compiles the
+// source at run time) has all of that as template arguments instead:
+//   * no op fetch or dispatch, and the code of consecutive ops can overlap;
+//   * register controls are compile-time slot masks;
+//   * X and CNOT on register bits are renamings of the tile's registers, so
+//     they cost no instruction.
+// Everything else -- matrices, exchange layouts, shuffle member masks,
+// out-of-tile controls and phase-fan terms -- is still read from the op
+// records at run time, so one compiled kernel serves every program of the
+// same shape (a parameterised circuit at any angles, the same circuit on any
+// state).  The arithmetic of every op is the interpreter's (fused_ops.cuh),
+// so results equal k_fused2's bit for bit.
+#pragma once
+
+#include "fused_ops.cuh"
+
+namespace ket {
+namespace jit {
+
+template <int NS>
+__host__ __device__ constexpr uint32_t slotmask(int creg) {
+  uint32_t v = 0;
+  for (int j = 0; j < NS; j++)
+    if ((j & creg) == creg) v |= 1u << j;
+  return v;
+}
+
+// A swap the compiler resolves by renaming: the tile lives in registers
+// indexed only by constants, so straight-line code needs no moves.
+template <typename R>
+__device__ __forceinline__ void swp(cpx<R>& a, cpx<R>& b) {
+  const cpx<R> t = a;
+  a = b;
+  b = t;
+}
+
+// Per-tile context of the ops.
+struct Tile {
+  uint32_t smb;   // exchange buffer (shared-memory address)
+  int tid, lane, warp;
+  uint64_t ctx0;  // global index bits of the tile outside its 12 bits
+};
+
+// Rare ops on the shared-memory copy of the tile, as in k_fused2.
+template <typename R, int NR, int OPC, int FL>
+__device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl, const FOp* op, const Tile& t) {
+  constexpr int NT = 32 << (7 - NR);
+  constexpr double thr = 1e-14, qthr = 1e-7;
+  const uint4 h = __ldg(reinterpret_cast<const uint4*>(op));
+  const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);
+  const uint32_t ct = h2.y;
+  const int oa = (h.x >> 8) & 0xff, ob = (int)(h2.w & 0xffu);
+  const double* M = op->m;
+  const uint32_t smb = t.smb;
+  __syncthreads();
+  write_tile<R, NR>(smb, sl, x);
+  __syncthreads();
+  if constexpr (OPC == OC_X1S) {
+    for (uint32_t g = t.tid; g < (1u << (KET_T2_BITS - 1)); g += NT) {
+      const uint32_t i0 = insert0_32(g, ob);
+      if ((i0 & ct) != ct) continue;
+      cpx<R> t0, t1;
+      lds(smb + swz<R>(i0), t0);
+      lds(smb + swz<R>(i0 | (1u << ob)), t1);
+      sts(smb + swz<R>(i0), t1);
+      sts(smb + swz<R>(i0 | (1u << ob)), t0);
+    }
+  } else if constexpr (OPC == OC_DIAG) {
+    const int b0t = (int8_t)(h.y >> 8), b1t = (int8_t)(h.y >> 16);
+    const uint64_t dg0 = __ldg(reinterpret_cast<const unsigned long long*>(op) + 4);
+    const uint64_t dg1 = __ldg(reinterpret_cast<const unsigned long long*>(op) + 5);
+    const int u0 = (int)((t.ctx0 & dg0) != 0), u1 = (int)((t.ctx0 & dg1) != 0);
+    for (uint32_t i = t.tid; i < (1u << KET_T2_BITS); i += NT) {
+      if ((i & ct) != ct) continue;
+      const int k0 = b0t >= 0 ? (int)((i >> b0t) & 1) : u0;
+      const int k1 = b1t >= 0 ? (int)((i >> b1t) & 1) : u1;
+      const int kk = 2 * k0 + k1;
+      cpx<R> v;
+      lds(smb + swz<R>(i), v);
+      v = cmul<R>((R)__ldg(M + 2 * kk), (R)__ldg(M + 2 * kk + 1), v);
+      sts(smb + swz<R>(i), v);
+    }
+  } else {
+    const int ta = oa, tb = ob;
+    const int lo = ta < tb ? ta : tb, hi = ta < tb ? tb : ta;
+    for (uint32_t g = t.tid; g < (1u << (KET_T2_BITS - 2)); g += NT) {
+      const uint32_t b0 = insert0_32(insert0_32(g, lo), hi);
+      if ((b0 & ct) != ct) continue;
+      const uint32_t i1 = b0 | (1u << tb), i2 = b0 | (1u << ta), i3 = b0 | (1u << ta) | (1u << tb);
+      if constexpr (OPC == OC_SWAPS) {
+        cpx<R> t1, t2;
+        lds(smb + swz<R>(i1), t1);
+        lds(smb + swz<R>(i2), t2);
+        sts(smb + swz<R>(i1), t2);
+        sts(smb + swz<R>(i2), t1);
+      } else {
+        const uint32_t idx[4] = {b0, i1, i2, i3};
+        cpx<R> v[4];
+        for (int c = 0; c < 4; c++) lds(smb + swz<R>(idx[c]), v[c]);
+        for (int r = 0; r < 4; r++) {
+          cpx<R> s0 = mac2<R>((R)__ldg(M + 8 * r), (R)__ldg(M + 8 * r + 1), v[0], (R)__ldg(M + 8 * r + 2),
+                              (R)__ldg(M + 8 * r + 3), v[1]);
+          cpx<R> s1 = mac2<R>((R)__ldg(M + 8 * r + 4), (R)__ldg(M + 8 * r + 5), v[2], (R)__ldg(M + 8 * r + 6),
+                              (R)__ldg(M + 8 * r + 7), v[3]);
+          cpx<R> y;
+          y.re = s0.re + s1.re;
+          y.im = s0.im + s1.im;
+          if (FL & FOF_PRUNE) prune_amp(y, thr, qthr);
+          sts(smb + swz<R>(idx[r]), y);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  read_tile<R, NR>(smb, sl, x);
+}
+
+// One op of the program.  OPC: op code; FL: flags; CREG: register controls;
+// CTHR: thread-id controls; CCTX: whether the op has controls outside the tile.
+template <typename R, int NR, int OPC, int FL, int CREG, uint32_t CTHR, bool CCTX>
+__device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const FOp* op, const Tile& t) {
+  constexpr int NS = 1 << NR;
+  constexpr double thr = 1e-14, qthr = 1e-7;
+  if constexpr (OPC == OC_EXCH) {
+    __syncthreads();
+    write_tile<R, NR>(t.smb, sl, x);
+    __syncthreads();
+    sl = exch_slay<NR>(op, t.lane, t.warp);
+    read_tile<R, NR>(t.smb, sl, x);
+    return;
+  }
+  if constexpr (CCTX) {
+    const uint64_t cctx = __ldg(reinterpret_cast<const unsigned long long*>(op) + 1);
+    if ((t.ctx0 & cctx) != cctx) return;  // uniform over the CTA
+  }
+  if constexpr (OPC == OC_SWAPS || OPC == OC_MAT2S || OPC == OC_DIAG || OPC == OC_X1S) {
+    smem_op<R, NR, OPC, FL>(x, sl, op, t);
+    return;
+  }
+  if constexpr (CTHR != 0) {
+    if (((uint32_t)t.tid & CTHR) != CTHR) return;
+  }
+  constexpr uint32_t SM = slotmask<NS>(CREG);
+  if constexpr (OPC >= OC_MAT1R && OPC < OC_MAT1R + 15) {
+    constexpr int A = (OPC - OC_MAT1R) / 3, F = (OPC - OC_MAT1R) % 3;
+    const double2* mp = reinterpret_cast<const double2*>(op->m);
+    const double2 q0 = __ldg(mp), q1 = __ldg(mp + 1), q2 = __ldg(mp + 2), q3 = __ldg(mp + 3);
+    const R m[8] = {(R)q0.x, (R)q0.y, (R)q1.x, (R)q1.y, (R)q2.x, (R)q2.y, (R)q3.x, (R)q3.y};
+    mat1_reg<R, A, F, NS>(x, m, SM);
+  } else if constexpr (OPC >= OC_MAT1L && OPC < OC_MAT1L + 3) {
+    const double2* mp = reinterpret_cast<const double2*>(op->m);
+    const double2 q0 = __ldg(mp), q1 = __ldg(mp + 1), q2 = __ldg(mp + 2), q3 = __ldg(mp + 3);
+    const uint32_t members = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
+    const int oa = (__ldg(reinterpret_cast<const uint32_t*>(op)) >> 8) & 0xff;
+    const int bitv = (t.lane >> oa) & 1;
+    const double2 e0 = bitv ? q3 : q0;
+    const double2 e1 = bitv ? q2 : q1;
+    const R c0r = (R)e0.x, c0i = (R)e0.y, c1r = (R)e1.x, c1i = (R)e1.y;
+    const int msk = 1 << oa;
+#pragma unroll
+    for (int j = 0; j < NS; j++) {
+      if (!((SM >> j) & 1)) continue;
+      const cpx<R> p = shfl_xor_c<R>(x[j], msk, members);
+      cpx<R> y;
+      if constexpr (OPC == OC_MAT1L + 1) {
+        y.re = fma(c0r, x[j].re, c1r * p.re);
+        y.im = fma(c0r, x[j].im, c1r * p.im);
+      } else if constexpr (OPC == OC_MAT1L + 2) {
+        y.re = fma(c0r, x[j].re, -c1i * p.im);
+        y.im = fma(c0r, x[j].im, c1i * p.re);
+      } else {
+        y = mac2<R>(c0r, c0i, x[j], c1r, c1i, p);
+      }
+      x[j] = y;
+    }
+  } else if constexpr (OPC >= OC_X1R && OPC < OC_X1R + 5) {
+    constexpr int A = OPC - OC_X1R;
+#pragma unroll
+    for (int j = 0; j < NS; j++)
+      if (!(j & (1 << A)) && ((SM >> j) & 1)) swp<R>(x[j], x[j | (1 << A)]);
+  } else if constexpr (OPC >= OC_X1RC && OPC < OC_X1RC + 25) {
+    constexpr int A = (OPC - OC_X1RC) / 5, C = (OPC - OC_X1RC) % 5;
+#pragma unroll
+    for (int j = 0; j < NS; j++)
+      if (!(j & (1 << A)) && (j & (1 << C))) swp<R>(x[j], x[j | (1 << A)]);
+  } else if constexpr (OPC == OC_X1L) {
+    const uint32_t members = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
+    const int oa = (__ldg(reinterpret_cast<const uint32_t*>(op)) >> 8) & 0xff;
+#pragma unroll
+    for (int j = 0; j < NS; j++)
+      if ((SM >> j) & 1) x[j] = shfl_xor_c<R>(x[j], 1 << oa, members);
+  } else if constexpr ((OPC >= OC_DIAGR && OPC < OC_DIAGR + 5) || (OPC >= OC_DIAGR1 && OPC < OC_DIAGR1 + 5)) {
+    constexpr bool ONE = OPC >= OC_DIAGR1;
+    constexpr int A = OPC - (ONE ? OC_DIAGR1 : OC_DIAGR);
+    const double2* mp = reinterpret_cast<const double2*>(op->m);
+    const double2 q0 = __ldg(mp), q1 = __ldg(mp + 1);
+    diag_reg<R, A, ONE, NS>(x, (R)q0.x, (R)q0.y, (R)q1.x, (R)q1.y, SM);
+  } else if constexpr (OPC >= OC_DIAGR1C && OPC < OC_DIAGR1C + 25) {
+    constexpr int A = (OPC - OC_DIAGR1C) / 5, C = (OPC - OC_DIAGR1C) % 5;
+    const double2 q1 = __ldg(reinterpret_cast<const double2*>(op->m) + 1);
+    diag1c_reg<R, A, C, NS>(x, (R)q1.x, (R)q1.y);
+  } else if constexpr (OPC >= OC_CPHASE && OPC < OC_CPHASE + 5) {
+    constexpr int A = OPC - OC_CPHASE;
+    const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);
+    phase_fan<R, A, 1, NS>(reinterpret_cast<cpx<R>(&)[1][NS]>(x), op, h2.x, t.ctx0, 0, t.tid);
+  } else if constexpr (OPC == OC_DIAGT || OPC == OC_DIAGX) {
+    const double2* mp = reinterpret_cast<const double2*>(op->m);
+    bool one;
+    if constexpr (OPC == OC_DIAGT) {
+      const int oa = (__ldg(reinterpret_cast<const uint32_t*>(op)) >> 8) & 0xff;
+      one = (t.tid >> oa) & 1;
+    } else {
+      one = (t.ctx0 & __ldg(reinterpret_cast<const unsigned long long*>(op) + 4)) != 0;
+    }
+    if ((FL & FOF_D0ONE) && !one) return;
+    const double2 e = __ldg(mp + (one ? 1 : 0));
+    phase_all<R, NS>(x, (R)e.x, (R)e.y, SM);
+  } else {
+    // handled above (the exchange and the shared-memory ops return early)
+    static_assert(OPC == OC_NOP || OPC == OC_EXCH || OPC == OC_SWAPS || OPC == OC_MAT2S || OPC == OC_DIAG ||
+                      OPC == OC_X1S,
+                  "op code without a compiled form");
+    return;
+  }
+  if constexpr ((FL & FOF_PRUNE) != 0) prune_slots<R, NS>(x, thr, qthr);
+}
+
+// The tile loop around a program: load each tile in the load layout, run the
+// ops, store it in the store layout -- the same addressing as k_fused2.
+template <typename R, int NR, typename Body>
+__device__ __forceinline__ void run_tiles(const Pass2Args& a, Body body) {
+  constexpr int NW = 7 - NR, NS = 1 << NR;
+  typedef typename Vec2<R>::T V;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  Tile t;
+  t.smb = (uint32_t)__cvta_generic_to_shared(smraw);
+  t.tid = threadIdx.x;
+  t.lane = t.tid & 31;
+  t.warp = t.tid >> 5;
+  char* const amp = reinterpret_cast<char*>(a.amp);
+  const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
+  uint64_t gl = 0, gs = 0;
+#pragma unroll
+  for (int r = 0; r < 5; r++)
+    if ((t.lane >> r) & 1) {
+      gl += a.lgb[r];
+      gs += a.sgb[r];
+    }
+#pragma unroll
+  for (int r = 0; r < NW; r++)
+    if ((t.warp >> r) & 1) {
+      gl += a.lgb[5 + r];
+      gs += a.sgb[5 + r];
+    }
+  cpx<R> x[NS];
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    t.ctx0 = ctx_of(a, tile);
+    {
+      const char* p = amp + t.ctx0 * sizeof(V) + gl;
+#pragma unroll
+      for (int j = 0; j < NS; j++) {
+        uint64_t o = 0;
+#pragma unroll
+        for (int k = 0; k < NR; k++)
+          if (j & (1 << k)) o += a.lgb[5 + NW + k];
+        x[j] = ld_amp<R>(reinterpret_cast<const V*>(p + o));
+      }
+    }
+    SLay<NR> sl = make_slay<NR>(a.lbx, t.lane, t.warp);
+    body(x, sl, t);
+    {
+      char* p = amp + t.ctx0 * sizeof(V) + gs;
+#pragma unroll
+      for (int j = 0; j < NS; j++) {
+        uint64_t o = 0;
+#pragma unroll
+        for (int k = 0; k < NR; k++)
+          if (j & (1 << k)) o += a.sgb[5 + NW + k];
+        st_amp<R>(reinterpret_cast<V*>(p + o), x[j]);
+      }
+    }
+  }
+}
+
+}  // namespace jit
+}  // namespace ket

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "fused_abi.h"
 
 namespace ket {
 
@@ -21,9 +22,6 @@ struct DevOp {
   double m[32];    // interleaved complex matrix (MAT1: 4, DIAG1: 2, DIAG2: 4, MAT2: 16 entries)
 };
 
-#define KET_MAX_TILE_HBITS 16
-#define KET_MAX_CTX_BITS 48
-
 struct PassArgs {
   void* amp;
   const DevOp* ops;
@@ -35,145 +33,18 @@ struct PassArgs {
 };
 
 // ---------------------------------------------------------------- register-tiled pass
-// The tile's 12 bits are split into roles: 5 lane bits, NW warp bits and NR
-// register bits (NW + NR = 7; each thread holds 2^NR amplitudes).  Role r < 5
-// is lane bit r, 5 <= r < 5 + NW is warp bit r - 5 (thread-id bit r), and r >=
-// 5 + NW is register bit r - 5 - NW.  A layout lists which tile bit plays
-// each role.  Ordinary passes use NR = 5 (128 threads per CTA, two CTAs per
-// SM); adjoint passes use NR = 4 (256 threads).
-#define KET_T2_BITS 12
-#define KET_NR_MAX 5
-// Register bits of ordinary (non-adjoint) passes.
-#define KET_FUSED_NREG 5
-enum FOpType : uint8_t {
-  FO_EXCH = 0,    // re-layout the tile through shared memory
-  FO_MAT1R = 1,   // 2x2 on register bit a
-  FO_MAT1L = 2,   // 2x2 on lane bit a (warp shuffles)
-  FO_X1R = 3,     // X on register bit a
-  FO_X1L = 4,     // X on lane bit a
-  FO_SWAPS = 5,   // swap tile bits a, b (controls on tile bits: ctile) through shared memory
-  FO_MAT2S = 6,   // 4x4 on tile bits a (MSB), b through shared memory
-  FO_DIAG = 7,    // 4-entry diagonal on tile bits d0 (MSB), d1 (-1 = outside the tile), through shared memory
-  FO_DIAGR = 8,   // diag(m0, m1) on register bit a
-  FO_DIAGT = 9,   // diag(m0, m1) on thread-id bit a (lane 0-4 / warp 5-7): one phase per thread
-  FO_DIAGX = 10,  // diag(m0, m1) on a qubit outside the tile (mask dg0): one phase per tile
-  FO_CPHASE = 11, // fan of phases on register bit a (see below), followed by continuation records
-  FO_GRADM = 12,  // adjoint probe, D 2x2 on register bit a (ancilla on register bit 3)
-  FO_GRADD = 13,  // adjoint probe, D = diag(m0, m1) on target a (register / thread / outside, see flags)
-  FO_GRADM2 = 14, // adjoint probe, D 4x4 on tile bits a (MSB), b through shared memory; ancilla tile bit anc
-  FO_CONT = 15    // continuation record of the op before it (data only, never dispatched)
-};
-
-// flags
-#define FOF_PRUNE 1u    // flush computed amplitudes with |a|^2 < 1e-14
-#define FOF_REAL 2u     // MAT1: every matrix entry is real
-#define FOF_D0ONE 4u    // DIAG*: m0 == 1 exactly (only bit-1 amplitudes change)
-#define FOF_RXFORM 8u   // MAT1: m00, m11 real and m01, m10 imaginary (Rx-like)
-#define FOF_TGT_THR 32u // FO_GRADD: target is a thread-id bit (a)
-#define FOF_TGT_CTX 64u // FO_GRADD: target is outside the tile (mask dg0)
-
-// Kernel op codes: one flat dispatch per op (the type, the target's register
-// bit, the matrix form and a register control are folded in by the host).
-enum FOpCode : uint8_t {
-  OC_EXCH = 0,
-  OC_MAT1R = 1,       // + 3 * A + form (form 0 general, 1 real, 2 Rx-like): 1..15
-  OC_MAT1L = 16,      // + form: 16..18
-  OC_X1R = 19,        // + A: 19..23 (no register control)
-  OC_X1RC = 24,       // + 5 * A + C: 24..48, X on register bit A controlled by register bit C only
-  OC_X1L = 49,
-  OC_DIAGR = 50,      // + A: 50..54 (general diag)
-  OC_DIAGR1 = 55,     // + A: 55..59 (m0 == 1)
-  OC_DIAGR1C = 60,    // + 5 * A + C: 60..84 (m0 == 1, controlled by register bit C only)
-  OC_DIAGT = 85,
-  OC_DIAGX = 86,
-  OC_DIAG = 87,
-  OC_SWAPS = 88,
-  OC_MAT2S = 89,
-  OC_GRADM = 90,      // + A: 90..93
-  OC_GRADD = 94,
-  OC_GRADM2 = 95,
-  OC_X1S = 96,        // X on tile bit b with controls ctile, through shared memory (multi-controlled X)
-  OC_CPHASE = 97,     // + A: 97..101, phase fan on register bit A
-  OC_NOP = 0xFF       // continuation record: dispatched as an op that does nothing
-};
-
-// FO_CPHASE: a run of phase gates diag(1, e^{i phi}) on one target (register
-// bit A), each with at most one control, merged into one op.  Every amplitude
-// whose bit A is 1 is multiplied by
-//   T[k] * prod_{thread-id bits s set} H[s] * exp(i * sum_{terms: ctx & mask} angle)
-// where k is the slot index with bit A removed.  m holds T[0 .. 2^(NR-1)-1]
-// (constant and register-bit controls).  Continuation records (FO_CONT) follow
-// the op; each has a 16-byte header that makes it a no-op (OC_NOP, no
-// controls).  Record 0 holds H[0..7] (lanes, then warps) after its header;
-// records 1.. hold the out-of-tile controls as (angle, global qubit mask)
-// double2 pairs, 19 per record.  The op's `lmask` field holds the number of
-// pairs and `ctile` the number of records.
-enum : int {
-  KET_CPHASE_TERMS_PER_RECORD = 19
-};
-
-struct FOp {
-  // bytes 0..15: everything the kernel needs to decide whether and how an op runs
-  uint8_t opc;                // FOpCode
-  uint8_t a;                  // target: register bit / lane bit / thread-id bit / tile bit (by type)
-  uint8_t flags;
-  uint8_t creg;               // controls on register bits (bit k = register bit k)
-  uint8_t cthr;               // controls on thread-id bits (lane bits 0-4, then the warp bits)
-  int8_t d0, d1;              // FO_DIAG: tile bits of t0 (MSB) and t1, -1 = outside the tile
-  uint8_t type;               // FOpType (host-side classification, used by the planner's tests)
-  uint64_t cctx;              // controls on global bits outside the tile
-  // bytes 16..31
-  uint32_t lmask;             // lanes whose lane-bit controls hold (shuffle member mask)
-  uint32_t ctile;             // shared-memory ops: controls as a tile-bit mask
-  int16_t slot, anc;          // adjoint probes: gradient slot; FO_GRADM2: ancilla tile bit
-  uint8_t b;                  // shared-memory ops: second tile bit
-  uint8_t pad0[3];
-  // bytes 32..63
-  uint64_t dg0, dg1;          // DIAGX / DIAG / GRADD: global mask of the target(s) outside the tile
-  uint8_t pos[KET_T2_BITS];   // FO_EXCH: new layout (role -> tile bit)
-  uint32_t pad1;
-  // FO_EXCH: m holds, as 12 uint16, the swizzled byte offset of each role's tile
-  // bit in the exchange buffer (see exch_offset); other ops: the matrix
-  double m[32];
-};
-static_assert(sizeof(FOp) == 64 + 256, "FOp layout");
+// The op records (FOp) and arguments (Pass2Args) are in fused_abi.h.
 
 // Fill in op.opc from op.type, op.a, op.flags and op.creg.
 void assign_opcode(FOp& op);
-
-// Byte offset of tile index i in the XOR-swizzled exchange buffer.  The map is
-// linear over GF(2), so the offset of a sum of disjoint bits is the XOR of
-// their offsets.
-__host__ __device__ inline uint32_t exch_offset(uint32_t i, bool c64) {
-  return c64 ? ((i ^ (((i >> 4) ^ (i >> 8)) & 15u)) << 3) : ((i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7u)) << 4);
-}
-
-struct Pass2Args {
-  void* amp;
-  const FOp* ops;
-  int nops;
-  int n, L, nh, nctx;
-  uint8_t load_pos[KET_T2_BITS];   // layout used for the global load
-  uint8_t store_pos[KET_T2_BITS];  // layout in force at the global store
-  int hbits[KET_MAX_TILE_HBITS];   // global qubit of tile bits L..11
-  int ctxbits[KET_MAX_CTX_BITS];
-  double thr, qthr;
-  int* status;                     // device status word: set to KET_ERR_TIMEOUT if a bounded wait ran out
-  double* gpart;                   // adjoint: per-CTA gradient partials [cta][slot][warp]
-  int nslots;                      // adjoint: gradient probes in this pass
-  int nreg;                        // register bits of the layouts (4 or 5)
-  int pairbit;                     // index into ctxbits of the qubit that tells apart the two tiles a
-                                   // thread holds, -1 = one tile per thread (see choose_pairbit)
-  // filled by launch_fused2 from the fields above:
-  uint64_t lgb[KET_T2_BITS];       // byte offset in the state of each role's tile bit, load layout
-  uint64_t sgb[KET_T2_BITS];       // same, store layout
-  uint32_t lbx[KET_T2_BITS];       // exchange-buffer offset of each role's tile bit, load layout
-};
 
 // Sum the adjoint partials of one pass: out[s] = sum over CTAs and warps (fixed order).
 cudaError_t launch_grad_reduce(const double* gpart, int nctas, int nslots, double* out, cudaStream_t s);
 // Persistent grid of the register-tiled pass for a register-bit count.
 int fused2_grid(int nreg);
+// Fill a.lgb, a.sgb and a.lbx (per-role byte offsets in the state and in the
+// exchange buffer) from the layouts and tile bits.
+void fill_pass2_offsets(Pass2Args& a, int precision);
 // A qubit outside the tile (index into a.ctxbits) that no op of the program
 // reads as a control or a diagonal target, or -1.
 int choose_pairbit(const std::vector<FOp>& prog, const Pass2Args& a);

@@ -1,0 +1,39 @@
+"""The pass kernels compiled per program (jit.cpp) build for sm_100a without a
+GPU: the program generator's output for circuits that use every op kind is
+turned into kernel source and compiled with NVRTC, in both precisions, with
+and without the reference's pruning."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from test_gpu_parity import random_gates
+
+
+def _compile(n, gates, precision, prune):
+    import ket_b200 as K
+    from ket_b200 import _lib
+    from ket_b200.circuit import flatten_ops, ops_to_abi
+    c = K.Circuit(n)
+    for name, qs, ps in gates:
+        c = c.unitary(ps, *qs) if name == "unitary" else getattr(c, name)(*ps, *qs)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    mv = np.ascontiguousarray(m).view(np.float64)
+    o = _lib.exec_opts(prune=prune)
+    kernels = C.c_int64()
+    log = C.create_string_buffer(1 << 14)
+    rc = _lib.lib().ket_jit_compile(n, precision, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size,
+                                    C.byref(o), C.byref(kernels), log, len(log))
+    return rc, kernels.value, log.value.decode(errors="replace")
+
+
+@pytest.mark.parametrize("precision,prune", [(0, True), (1, False)])
+def test_generated_kernels_compile(precision, prune):
+    rc, kernels, log = _compile(13, random_gates(13, 70, 5), precision, prune)
+    assert rc == 0, log
+    assert kernels >= 1
+
+
+def test_plan_without_tiled_passes_compiles_nothing():
+    rc, kernels, _ = _compile(8, random_gates(8, 20, 1), 0, True)
+    assert rc == 0 and kernels == 0
