@@ -374,8 +374,10 @@ int ket_plan_program_stats(int n, int precision, const ket_op* ops, size_t nops,
     std::vector<FOp> prog;
     uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
     plan_program(plan, p, precision, o.prune != 0, KET_FUSED_NREG, prog, lp, sp);
-    for (const FOp& f : prog)
+    for (const FOp& f : prog) {
       if (f.type != FO_CONT) counts[f.type]++;
+      if (f.type == FO_MAT1R || f.type == FO_MAT1L) counts[(f.flags & (FOF_REAL | FOF_RXFORM)) ? 13 : 12]++;
+    }
     counts[14]++;
   }
   return KET_OK;
@@ -410,10 +412,10 @@ int ket_jit_compile(int n, int precision, const ket_op* ops, size_t nops, const 
     if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) continue;
     progs.emplace_back();
     uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
-    plan_program(plan, p, precision, o.prune != 0, KET_FUSED_NREG, progs.back(), lp, sp);
+    plan_program(plan, p, precision, o.prune != 0, tiled_nreg(n), progs.back(), lp, sp);
   }
   std::vector<JitPass> jp;
-  for (auto& pr : progs) jp.push_back(JitPass{pr.data(), (int)pr.size(), n});
+  for (auto& pr : progs) jp.push_back(JitPass{pr.data(), (int)pr.size(), n, tiled_nreg(n)});
   std::string clog;
   rc = jit_compile(jp, precision, kernels, clog);
   if (log && logcap) {
@@ -462,8 +464,8 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
       std::vector<FOp> prog;
       Pass2Args& a = p2[i];
       memset(&a, 0, sizeof(a));
-      plan_program(plan, p, s->precision, prune, KET_FUSED_NREG, prog, a.load_pos, a.store_pos);
-      a.nreg = KET_FUSED_NREG;
+      a.nreg = tiled_nreg(s->n);
+      plan_program(plan, p, s->precision, prune, a.nreg, prog, a.load_pos, a.store_pos);
       off[i] = fops.size();
       fops.insert(fops.end(), prog.begin(), prog.end());
       a.amp = s->amp;
@@ -522,9 +524,9 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
   {
     std::vector<JitPass> jp(np);
     for (size_t i = 0; i < np; i++)
-      if (use2[i] && p2[i].nslots == 0) jp[i] = JitPass{fops.data() + off[i], p2[i].nops, s->n};
+      if (use2[i] && p2[i].nslots == 0) jp[i] = JitPass{fops.data() + off[i], p2[i].nops, s->n, p2[i].nreg};
     std::string err;
-    int rc = jit_prepare(jp, s->precision, o.specialize, c->device, jf, err);
+    int rc = jit_prepare(jp, s->precision, o.specialize, c->stream, jf, err);
     if (rc) return fail(rc, err);
   }
   const FOp* dfops = reinterpret_cast<const FOp*>(dev);

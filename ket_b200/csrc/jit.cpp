@@ -40,6 +40,7 @@
 #include "launch.h"
 #include "jit.h"
 #include "jit_sources.inc"  // kJitHeaders: the device headers as strings (written by build.py)
+#include "jit_ops.cuh"
 
 namespace ket {
 namespace {
@@ -134,15 +135,18 @@ struct Driver {
   CUresult (*attr)(CUfunction, CUfunction_attribute, int);
   CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
                      void**, void**);
+  CUresult (*global)(CUdeviceptr*, size_t*, CUmodule, const char*);
+  CUresult (*copy2d)(const CUDA_MEMCPY2D*, CUstream);
 };
 
 Driver& driver() {
   static Driver d = [] {
     Driver r;
-    void* p[4] = {nullptr, nullptr, nullptr, nullptr};
-    const char* names[4] = {"cuModuleLoadData", "cuModuleGetFunction", "cuFuncSetAttribute", "cuLaunchKernel"};
+    void* p[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    const char* names[6] = {"cuModuleLoadData", "cuModuleGetFunction", "cuFuncSetAttribute", "cuLaunchKernel",
+                            "cuModuleGetGlobal", "cuMemcpy2DAsync"};
     bool ok = true;
-    for (int i = 0; i < 4; i++) {
+    for (int i = 0; i < 6; i++) {
       cudaDriverEntryPointQueryResult q;
       if (cudaGetDriverEntryPoint(names[i], &p[i], cudaEnableDefault, &q) != cudaSuccess ||
           q != cudaDriverEntryPointSuccess || !p[i])
@@ -152,6 +156,8 @@ Driver& driver() {
     r.get = (decltype(r.get))p[1];
     r.attr = (decltype(r.attr))p[2];
     r.launch = (decltype(r.launch))p[3];
+    r.global = (decltype(r.global))p[4];
+    r.copy2d = (decltype(r.copy2d))p[5];
     r.ok = ok;
     return r;
   }();
@@ -161,15 +167,22 @@ Driver& driver() {
 // ---------------------------------------------------------------- source
 const char* real_name(int precision) { return precision == KET_C64 ? "float" : "double"; }
 
-std::string make_source(const FOp* prog, int nops, int precision) {
+// The lane or thread-id bit that lane ops and thread diagonals take as a
+// template argument (0 for other ops).
+int static_lane(const FOp& f) {
+  return (f.opc >= OC_MAT1L && f.opc < OC_MAT1L + 3) || f.opc == OC_X1L || f.opc == OC_DIAGT ? f.a : 0;
+}
+
+std::string make_source(const FOp* prog, int nops, int precision, int NR) {
   const char* R = real_name(precision);
-  const int NR = KET_FUSED_NREG, NT = 32 << (7 - NR);
+  const int NT = 32 << (7 - NR);
   std::string s;
   s.reserve(200 + 96 * (size_t)nops);
   s += "#include \"jit_ops.cuh\"\n";
+  s += "__constant__ ket::jit::COp c_ops[" + std::to_string(nops > 0 ? nops : 1) + "];\n";
   s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(NT) + ", 2) ket_pass(const ket::Pass2Args a) {\n";
   s += "  using namespace ket;\n";
-  s += "  const FOp* o = a.ops;\n";
+  s += "  const FOp* g = a.ops;\n";
   s += std::string("  jit::run_tiles<") + R + ", " + std::to_string(NR) + ">(a, [&](cpx<" + R + "> (&x)[" +
        std::to_string(1 << NR) + "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
   for (int k = 0; k < nops; k++) {
@@ -178,15 +191,16 @@ std::string make_source(const FOp* prog, int nops, int precision) {
     const unsigned fl = f.flags & (FOF_PRUNE | FOF_D0ONE);
     s += std::string("    jit::step<") + R + ", " + std::to_string(NR) + ", " + std::to_string((int)f.opc) + ", " +
          std::to_string(fl) + ", " + std::to_string((int)f.creg) + ", " + std::to_string((unsigned)f.cthr) + "u, " +
-         (f.cctx ? "true" : "false") + ">(x, sl, o + " + std::to_string(k) + ", t);\n";
+         (f.cctx ? "true" : "false") + ", " + std::to_string(static_lane(f)) + ">(x, sl, c_ops[" + std::to_string(k) +
+         "], g + " + std::to_string(k) + ", t);\n";
   }
   s += "  });\n}\n";
   return s;
 }
 
 // The shape of a program: what selects code in make_source.
-std::string shape_key(const FOp* prog, int nops, int precision) {
-  std::string k = precision == KET_C64 ? "f" : "d";
+std::string shape_key(const FOp* prog, int nops, int precision, int nreg) {
+  std::string k = std::string(precision == KET_C64 ? "f" : "d") + std::to_string(nreg);
   k.reserve(8 * (size_t)nops + 1);
   for (int i = 0; i < nops; i++) {
     const FOp& f = prog[i];
@@ -196,8 +210,8 @@ std::string shape_key(const FOp* prog, int nops, int precision) {
     }
     const unsigned fl = f.flags & (FOF_PRUNE | FOF_D0ONE);
     char buf[32];
-    snprintf(buf, sizeof buf, "%x,%x,%x,%x,%d;", (unsigned)f.opc, fl, (unsigned)f.creg, (unsigned)f.cthr,
-             f.cctx ? 1 : 0);
+    snprintf(buf, sizeof buf, "%x,%x,%x,%x,%d,%d;", (unsigned)f.opc, fl, (unsigned)f.creg, (unsigned)f.cthr,
+             f.cctx ? 1 : 0, static_lane(f));
     k += buf;
   }
   return k;
@@ -208,7 +222,7 @@ struct Entry {
   enum { QUEUED, BUSY, READY, FAILED } st = QUEUED;
   std::string src, log;
   std::vector<char> cubin;
-  std::map<int, CUfunction> fn;  // device -> loaded kernel
+  std::map<void*, JitFn> fn;  // stream -> kernel loaded for it (each stream owns its constant array)
 };
 
 struct Cache {
@@ -287,11 +301,19 @@ std::vector<std::string> enqueue(Cache& C, const std::vector<JitPass>& passes, i
   bool queued = false;
   for (size_t i = 0; i < passes.size(); i++) {
     const JitPass& p = passes[i];
-    if (!p.prog || p.nqubits < min_qubits) continue;
-    keys[i] = shape_key(p.prog, p.nops, precision);
+    // the constant op array holds at most 64 KB (512 records)
+    if (!p.prog || p.nqubits < min_qubits || (size_t)p.nops * sizeof(jit::COp) > 60000) continue;
+    keys[i] = shape_key(p.prog, p.nops, precision, p.nreg);
     if (C.map.find(keys[i]) == C.map.end()) {
       Entry& e = C.map[keys[i]];
-      e.src = make_source(p.prog, p.nops, precision);
+      e.src = make_source(p.prog, p.nops, precision, p.nreg);
+      if (const char* dir = getenv("KET_JIT_DUMP")) {  // kernel sources, for inspection
+        const std::string path = std::string(dir) + "/ket_pass_" + std::to_string(C.map.size()) + ".cu";
+        if (FILE* fp = fopen(path.c_str(), "w")) {
+          fputs(e.src.c_str(), fp);
+          fclose(fp);
+        }
+      }
       C.queue.push_back(keys[i]);
       queued = true;
     }
@@ -336,8 +358,8 @@ int jit_compile(const std::vector<JitPass>& passes, int precision, int64_t* dist
   return wait_keys(C, lk, keys, log) ? KET_OK : KET_ERR_CUDA;
 }
 
-int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, int device, std::vector<JitFn>& out,
-                std::string& err) {
+int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cudaStream_t stream,
+                std::vector<JitFn>& out, std::string& err) {
   out.assign(passes.size(), JitFn{});
   if (mode < 0) return KET_OK;
   if (!driver().ok) {
@@ -356,11 +378,14 @@ int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, int
     if (keys[i].empty()) continue;
     Entry& e = C.map[keys[i]];
     if (e.st != Entry::READY) continue;
-    auto f = e.fn.find(device);
+    auto f = e.fn.find((void*)stream);
     if (f == e.fn.end()) {
       CUmodule mod;
       CUfunction fn;
-      if (D.load(&mod, e.cubin.data()) != CUDA_SUCCESS || D.get(&fn, mod, "ket_pass") != CUDA_SUCCESS) {
+      CUdeviceptr cops = 0;
+      size_t cbytes = 0;
+      if (D.load(&mod, e.cubin.data()) != CUDA_SUCCESS || D.get(&fn, mod, "ket_pass") != CUDA_SUCCESS ||
+          D.global(&cops, &cbytes, mod, "c_ops") != CUDA_SUCCESS) {
         if (mode == 1) return err = "loading a run-time compiled pass kernel failed", KET_ERR_CUDA;
         continue;
       }
@@ -369,21 +394,48 @@ int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, int
         if (mode == 1) return err = "setting the shared memory of a pass kernel failed", KET_ERR_CUDA;
         continue;
       }
-      f = e.fn.emplace(device, fn).first;
+      JitFn j;
+      j.fn = (void*)fn;
+      j.cops = (unsigned long long)cops;
+      j.cops_bytes = cbytes;
+      f = e.fn.emplace((void*)stream, j).first;
     }
-    out[i].fn = (void*)f->second;
+    out[i] = f->second;
   }
   return KET_OK;
+}
+
+int tiled_nreg(int nqubits) {
+  static const int large = [] {
+    const char* e = getenv("KET_JIT_NREG");
+    return e && atoi(e) == 5 ? 5 : 4;
+  }();
+  return nqubits >= KET_JIT_AUTO_QUBITS ? large : KET_FUSED_NREG;
 }
 
 cudaError_t jit_launch(const JitFn& f, const Pass2Args& in, int precision, cudaStream_t s) {
   Pass2Args a = in;
   fill_pass2_offsets(a, precision);
+  // the ops' first 128 bytes into the kernel's constant array (stream-ordered
+  // after the program's upload and the previous pass's kernel)
+  if ((size_t)a.nops * sizeof(jit::COp) > f.cops_bytes) return cudaErrorInvalidValue;
+  CUDA_MEMCPY2D cp;
+  memset(&cp, 0, sizeof(cp));
+  cp.srcMemoryType = CU_MEMORYTYPE_DEVICE;
+  cp.srcDevice = (CUdeviceptr)a.ops;
+  cp.srcPitch = sizeof(FOp);
+  cp.dstMemoryType = CU_MEMORYTYPE_DEVICE;
+  cp.dstDevice = (CUdeviceptr)f.cops;
+  cp.dstPitch = sizeof(jit::COp);
+  cp.WidthInBytes = sizeof(jit::COp);
+  cp.Height = (size_t)a.nops;
+  if (a.nops > 0 && driver().copy2d(&cp, (CUstream)s) != CUDA_SUCCESS) return cudaErrorLaunchFailure;
   const int smem = (precision == KET_C64 ? 8 : 16) << KET_T2_BITS;
   const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
-  const unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)fused2_grid(KET_FUSED_NREG));
+  // two CTAs per SM at either register-bit count (__launch_bounds__(NT, 2))
+  const unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)2 * num_sms());
   void* params[1] = {&a};
-  const CUresult r = driver().launch((CUfunction)f.fn, blocks, 1, 1, 32 << (7 - KET_FUSED_NREG), 1, 1, smem,
+  const CUresult r = driver().launch((CUfunction)f.fn, blocks, 1, 1, 32 << (7 - a.nreg), 1, 1, smem,
                                      (CUstream)s, params, nullptr);
   {
     std::lock_guard<std::mutex> g(cache().mu);

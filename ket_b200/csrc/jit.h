@@ -19,15 +19,29 @@ struct JitPass {
   const FOp* prog = nullptr;  // host copy of the pass's program; null = not a register-tiled pass
   int nops = 0;
   int nqubits = 0;
-};
-struct JitFn {
-  void* fn = nullptr;  // CUfunction, null = run the interpreter
+  int nreg = KET_FUSED_NREG;  // register bits of the program's layouts (4 or 5)
 };
 
-// For each pass, the compiled kernel to launch (null where none is ready).
+// Register bits of the register-tiled programs of an n-qubit state.  Below
+// KET_JIT_AUTO_QUBITS: 5 (128 threads of 32 amplitudes; the interpreter runs
+// two CTAs per SM).  From there on: 4 (256 threads of 16 amplitudes), the
+// faster shape for compiled kernels, which run two such CTAs per SM (16 warps);
+// KET_JIT_NREG=5 in the environment keeps 5.  The choice depends on the state
+// size only, never on whether a pass runs compiled or interpreted, so the two
+// give bit-identical results.
+int tiled_nreg(int nqubits);
+struct JitFn {
+  void* fn = nullptr;               // CUfunction, null = run the interpreter
+  unsigned long long cops = 0;      // device address of the kernel's constant op array
+  size_t cops_bytes = 0;
+};
+
+// For each pass, the compiled kernel to launch on this stream (null where none
+// is ready).  Each stream gets its own instance of a kernel's module, since a
+// launch first fills the module's constant op array.
 // mode: ket_exec_opts.specialize (0 automatic, 1 always, -1 never).
-int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, int device, std::vector<JitFn>& out,
-                std::string& err);
+int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cudaStream_t stream,
+                std::vector<JitFn>& out, std::string& err);
 cudaError_t jit_launch(const JitFn& f, const Pass2Args& a, int precision, cudaStream_t s);
 // Wait until no compile is queued or running.
 int jit_wait_all();

@@ -6,6 +6,7 @@
 // for one program (jit.cpp writes one `step<...>` call per op and compiles the
 // source at run time) has all of that as template arguments instead:
 //   * no op fetch or dispatch, and the code of consecutive ops can overlap;
+//   * the ops' matrices and masks are constant-bank operands (COp);
 //   * register controls are compile-time slot masks;
 //   * X and CNOT on register bits are renamings of the tile's registers, so
 //     they cost no instruction.
@@ -37,6 +38,40 @@ __device__ __forceinline__ void swp(cpx<R>& a, cpx<R>& b) {
   const cpx<R> t = a;
   a = b;
   b = t;
+}
+
+// The part of an op record a compiled kernel reads on every tile: the FOp's
+// 64-byte header and its first 8 matrix entries.  The host copies it for each
+// launch into the module's constant array, so these reads are constant-bank
+// operands rather than loads; the rest (phase-fan tables, 4x4 matrices) is read
+// from the global copy of the program.
+struct COp {
+  uint8_t opc, a, flags, creg, cthr;
+  int8_t d0, d1;
+  uint8_t type;
+  uint64_t cctx;
+  uint32_t lmask, ctile;
+  int16_t slot, anc;
+  uint8_t b, pad0[3];
+  uint64_t dg0, dg1;
+  uint8_t pos[KET_T2_BITS];
+  uint32_t pad1;
+  double m[8];
+};
+static_assert(sizeof(COp) == 128, "COp layout");
+#ifndef __CUDACC_RTC__  // checked where the host side includes this header
+static_assert(__builtin_offsetof(COp, m) == __builtin_offsetof(FOp, m), "COp mirrors FOp");
+static_assert(__builtin_offsetof(COp, dg0) == __builtin_offsetof(FOp, dg0), "COp mirrors FOp");
+#endif
+
+// FO_EXCH's new layout: its 12 uint16 exchange-buffer offsets are in m[0..2].
+template <int NR>
+__device__ __forceinline__ SLay<NR> exch_slay_c(const COp& c, int lane, int warp) {
+  uint32_t bx[12];
+#pragma unroll
+  for (int r = 0; r < 12; r++)
+    bx[r] = (uint32_t)((unsigned long long)__double_as_longlong(c.m[r >> 2]) >> (16 * (r & 3))) & 0xffffu;
+  return make_slay<NR>(bx, lane, warp);
 }
 
 // Per-tile context of the ops.
@@ -121,25 +156,27 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
 }
 
 // One op of the program.  OPC: op code; FL: flags; CREG: register controls;
-// CTHR: thread-id controls; CCTX: whether the op has controls outside the tile.
-template <typename R, int NR, int OPC, int FL, int CREG, uint32_t CTHR, bool CCTX>
-__device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const FOp* op, const Tile& t) {
+// CTHR: thread-id controls; CCTX: whether the op has controls outside the
+// tile; LA: the lane or thread-id bit of lane ops and thread diagonals.
+// c: the op's constant copy; g: the op in the global copy of the program.
+template <typename R, int NR, int OPC, int FL, int CREG, uint32_t CTHR, bool CCTX, int LA>
+__device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const COp& c, const FOp* g,
+                                     const Tile& t) {
   constexpr int NS = 1 << NR;
   constexpr double thr = 1e-14, qthr = 1e-7;
   if constexpr (OPC == OC_EXCH) {
     __syncthreads();
     write_tile<R, NR>(t.smb, sl, x);
     __syncthreads();
-    sl = exch_slay<NR>(op, t.lane, t.warp);
+    sl = exch_slay_c<NR>(c, t.lane, t.warp);
     read_tile<R, NR>(t.smb, sl, x);
     return;
   }
   if constexpr (CCTX) {
-    const uint64_t cctx = __ldg(reinterpret_cast<const unsigned long long*>(op) + 1);
-    if ((t.ctx0 & cctx) != cctx) return;  // uniform over the CTA
+    if ((t.ctx0 & c.cctx) != c.cctx) return;  // uniform over the CTA
   }
   if constexpr (OPC == OC_SWAPS || OPC == OC_MAT2S || OPC == OC_DIAG || OPC == OC_X1S) {
-    smem_op<R, NR, OPC, FL>(x, sl, op, t);
+    smem_op<R, NR, OPC, FL>(x, sl, g, t);
     return;
   }
   if constexpr (CTHR != 0) {
@@ -148,24 +185,18 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const F
   constexpr uint32_t SM = slotmask<NS>(CREG);
   if constexpr (OPC >= OC_MAT1R && OPC < OC_MAT1R + 15) {
     constexpr int A = (OPC - OC_MAT1R) / 3, F = (OPC - OC_MAT1R) % 3;
-    const double2* mp = reinterpret_cast<const double2*>(op->m);
-    const double2 q0 = __ldg(mp), q1 = __ldg(mp + 1), q2 = __ldg(mp + 2), q3 = __ldg(mp + 3);
-    const R m[8] = {(R)q0.x, (R)q0.y, (R)q1.x, (R)q1.y, (R)q2.x, (R)q2.y, (R)q3.x, (R)q3.y};
+    const R m[8] = {(R)c.m[0], (R)c.m[1], (R)c.m[2], (R)c.m[3], (R)c.m[4], (R)c.m[5], (R)c.m[6], (R)c.m[7]};
     mat1_reg<R, A, F, NS>(x, m, SM);
   } else if constexpr (OPC >= OC_MAT1L && OPC < OC_MAT1L + 3) {
-    const double2* mp = reinterpret_cast<const double2*>(op->m);
-    const double2 q0 = __ldg(mp), q1 = __ldg(mp + 1), q2 = __ldg(mp + 2), q3 = __ldg(mp + 3);
-    const uint32_t members = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
-    const int oa = (__ldg(reinterpret_cast<const uint32_t*>(op)) >> 8) & 0xff;
-    const int bitv = (t.lane >> oa) & 1;
-    const double2 e0 = bitv ? q3 : q0;
-    const double2 e1 = bitv ? q2 : q1;
-    const R c0r = (R)e0.x, c0i = (R)e0.y, c1r = (R)e1.x, c1i = (R)e1.y;
-    const int msk = 1 << oa;
+    const uint32_t members = c.lmask;
+    const bool bitv = (t.lane >> LA) & 1;
+    // own output = c0 * own + c1 * partner
+    const R c0r = (R)(bitv ? c.m[6] : c.m[0]), c0i = (R)(bitv ? c.m[7] : c.m[1]);
+    const R c1r = (R)(bitv ? c.m[4] : c.m[2]), c1i = (R)(bitv ? c.m[5] : c.m[3]);
 #pragma unroll
     for (int j = 0; j < NS; j++) {
       if (!((SM >> j) & 1)) continue;
-      const cpx<R> p = shfl_xor_c<R>(x[j], msk, members);
+      const cpx<R> p = shfl_xor_c<R>(x[j], 1 << LA, members);
       cpx<R> y;
       if constexpr (OPC == OC_MAT1L + 1) {
         y.re = fma(c0r, x[j].re, c1r * p.re);
@@ -189,37 +220,27 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const F
     for (int j = 0; j < NS; j++)
       if (!(j & (1 << A)) && (j & (1 << C))) swp<R>(x[j], x[j | (1 << A)]);
   } else if constexpr (OPC == OC_X1L) {
-    const uint32_t members = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);
-    const int oa = (__ldg(reinterpret_cast<const uint32_t*>(op)) >> 8) & 0xff;
+    const uint32_t members = c.lmask;
 #pragma unroll
     for (int j = 0; j < NS; j++)
-      if ((SM >> j) & 1) x[j] = shfl_xor_c<R>(x[j], 1 << oa, members);
+      if ((SM >> j) & 1) x[j] = shfl_xor_c<R>(x[j], 1 << LA, members);
   } else if constexpr ((OPC >= OC_DIAGR && OPC < OC_DIAGR + 5) || (OPC >= OC_DIAGR1 && OPC < OC_DIAGR1 + 5)) {
     constexpr bool ONE = OPC >= OC_DIAGR1;
     constexpr int A = OPC - (ONE ? OC_DIAGR1 : OC_DIAGR);
-    const double2* mp = reinterpret_cast<const double2*>(op->m);
-    const double2 q0 = __ldg(mp), q1 = __ldg(mp + 1);
-    diag_reg<R, A, ONE, NS>(x, (R)q0.x, (R)q0.y, (R)q1.x, (R)q1.y, SM);
+    diag_reg<R, A, ONE, NS>(x, (R)c.m[0], (R)c.m[1], (R)c.m[2], (R)c.m[3], SM);
   } else if constexpr (OPC >= OC_DIAGR1C && OPC < OC_DIAGR1C + 25) {
     constexpr int A = (OPC - OC_DIAGR1C) / 5, C = (OPC - OC_DIAGR1C) % 5;
-    const double2 q1 = __ldg(reinterpret_cast<const double2*>(op->m) + 1);
-    diag1c_reg<R, A, C, NS>(x, (R)q1.x, (R)q1.y);
+    diag1c_reg<R, A, C, NS>(x, (R)c.m[2], (R)c.m[3]);
   } else if constexpr (OPC >= OC_CPHASE && OPC < OC_CPHASE + 5) {
     constexpr int A = OPC - OC_CPHASE;
-    const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);
-    phase_fan<R, A, 1, NS>(reinterpret_cast<cpx<R>(&)[1][NS]>(x), op, h2.x, t.ctx0, 0, t.tid);
+    const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(g) + 1);
+    phase_fan<R, A, 1, NS>(reinterpret_cast<cpx<R>(&)[1][NS]>(x), g, h2.x, t.ctx0, 0, t.tid);
   } else if constexpr (OPC == OC_DIAGT || OPC == OC_DIAGX) {
-    const double2* mp = reinterpret_cast<const double2*>(op->m);
     bool one;
-    if constexpr (OPC == OC_DIAGT) {
-      const int oa = (__ldg(reinterpret_cast<const uint32_t*>(op)) >> 8) & 0xff;
-      one = (t.tid >> oa) & 1;
-    } else {
-      one = (t.ctx0 & __ldg(reinterpret_cast<const unsigned long long*>(op) + 4)) != 0;
-    }
+    if constexpr (OPC == OC_DIAGT) one = (t.tid >> LA) & 1;
+    else one = (t.ctx0 & c.dg0) != 0;
     if ((FL & FOF_D0ONE) && !one) return;
-    const double2 e = __ldg(mp + (one ? 1 : 0));
-    phase_all<R, NS>(x, (R)e.x, (R)e.y, SM);
+    phase_all<R, NS>(x, (R)(one ? c.m[2] : c.m[0]), (R)(one ? c.m[3] : c.m[1]), SM);
   } else {
     // handled above (the exchange and the shared-memory ops return early)
     static_assert(OPC == OC_NOP || OPC == OC_EXCH || OPC == OC_SWAPS || OPC == OC_MAT2S || OPC == OC_DIAG ||

@@ -58,6 +58,19 @@ def test_compiled_equals_interpreter_brickwork_qft(n):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("n,prune", [(26, True), (27, False)])
+def test_compiled_equals_interpreter_large_states(n, prune):
+    """From 26 qubits on the programs use 4 register bits (256 threads of 16
+    amplitudes) whichever way a pass runs."""
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import flatten_ops, ops_to_abi
+    c, _ = W.brickwork_qft(n, 3, 11)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    got = _run(n, arr, m, k, 1, prune)
+    want = _run(n, arr, m, k, -1, prune)
+    assert np.array_equal(got, want)
+
+
 def test_compiled_equals_interpreter_c64():
     from ket_b200 import workloads as W
     from ket_b200.circuit import flatten_ops, ops_to_abi

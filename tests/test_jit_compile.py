@@ -34,6 +34,13 @@ def test_generated_kernels_compile(precision, prune):
     assert kernels >= 1
 
 
+def test_generated_kernels_compile_four_register_bits():
+    """States of 26 qubits and more use programs with 4 register bits."""
+    rc, kernels, log = _compile(26, random_gates(26, 60, 9), 0, True)
+    assert rc == 0, log
+    assert kernels >= 1
+
+
 def test_plan_without_tiled_passes_compiles_nothing():
     rc, kernels, _ = _compile(8, random_gates(8, 20, 1), 0, True)
     assert rc == 0 and kernels == 0
