@@ -457,15 +457,40 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
   std::vector<Pass2Args> p2(np);
   std::vector<bool> use2(np, false);
   size_t matk_bytes = 0;
+  // Register-tiled passes: compiled kernels (jit.cpp) use programs with
+  // tiled_nreg(n) register bits; a pass whose kernel is not ready runs on the
+  // interpreter with KET_FUSED_NREG.
+  const int jit_nr = tiled_nreg(s->n);
+  std::vector<std::vector<FOp>> progs(np);
+  std::vector<JitFn> jf(np);
+  auto lower_pass = [&](size_t i, int nreg) {
+    Pass2Args& a = p2[i];
+    memset(&a, 0, sizeof(a));
+    a.nreg = nreg;
+    plan_program(plan, plan.passes[i], s->precision, prune, nreg, progs[i], a.load_pos, a.store_pos);
+  };
   for (size_t i = 0; i < np; i++) {
     const Pass& p = plan.passes[i];
     if (p.fused && p.m == KET_T2_BITS && s->n >= KET_T2_BITS) {
       use2[i] = true;
-      std::vector<FOp> prog;
+      lower_pass(i, o.specialize < 0 ? KET_FUSED_NREG : jit_nr);
+    }
+  }
+  if (o.specialize >= 0) {
+    std::vector<JitPass> jp(np);
+    for (size_t i = 0; i < np; i++)
+      if (use2[i]) jp[i] = JitPass{progs[i].data(), (int)progs[i].size(), s->n, jit_nr};
+    std::string err;
+    int rc = jit_prepare(jp, s->precision, o.specialize, c->stream, jf, err);
+    if (rc) return fail(rc, err);
+    for (size_t i = 0; i < np; i++)
+      if (use2[i] && !jf[i].fn && jit_nr != KET_FUSED_NREG) lower_pass(i, KET_FUSED_NREG);
+  }
+  for (size_t i = 0; i < np; i++) {
+    const Pass& p = plan.passes[i];
+    if (use2[i]) {
+      const std::vector<FOp>& prog = progs[i];
       Pass2Args& a = p2[i];
-      memset(&a, 0, sizeof(a));
-      a.nreg = tiled_nreg(s->n);
-      plan_program(plan, p, s->precision, prune, a.nreg, prog, a.load_pos, a.store_pos);
       off[i] = fops.size();
       fops.insert(fops.end(), prog.begin(), prog.end());
       a.amp = s->amp;
@@ -518,16 +543,6 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
     c->h2d_bytes += total;
     cudaError_t e = cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(ops)");
-  }
-  // run-time compiled kernels for the register-tiled passes (jit.cpp)
-  std::vector<JitFn> jf;
-  {
-    std::vector<JitPass> jp(np);
-    for (size_t i = 0; i < np; i++)
-      if (use2[i] && p2[i].nslots == 0) jp[i] = JitPass{fops.data() + off[i], p2[i].nops, s->n, p2[i].nreg};
-    std::string err;
-    int rc = jit_prepare(jp, s->precision, o.specialize, c->stream, jf, err);
-    if (rc) return fail(rc, err);
   }
   const FOp* dfops = reinterpret_cast<const FOp*>(dev);
   const DevOp* dops = reinterpret_cast<const DevOp*>((const char*)dev + f_bytes);

@@ -22,13 +22,15 @@ struct JitPass {
   int nreg = KET_FUSED_NREG;  // register bits of the program's layouts (4 or 5)
 };
 
-// Register bits of the register-tiled programs of an n-qubit state.  Below
-// KET_JIT_AUTO_QUBITS: 5 (128 threads of 32 amplitudes; the interpreter runs
-// two CTAs per SM).  From there on: 4 (256 threads of 16 amplitudes), the
-// faster shape for compiled kernels, which run two such CTAs per SM (16 warps);
-// KET_JIT_NREG=5 in the environment keeps 5.  The choice depends on the state
-// size only, never on whether a pass runs compiled or interpreted, so the two
-// give bit-identical results.
+// Register bits of the programs of compiled pass kernels for an n-qubit
+// state.  Below KET_JIT_AUTO_QUBITS: 5, the interpreter's (128 threads of 32
+// amplitudes), so a compiled kernel gives the interpreter's result bit for
+// bit.  From there on: 4 (256 threads of 16 amplitudes, two CTAs and 16 warps
+// per SM), the faster shape for compiled kernels and much the slower one for
+// the interpreter, which keeps 5; KET_JIT_NREG=5 in the environment keeps 5
+// throughout.  Register and lane forms of a gate round alike, but merged
+// phase fans group their factors by role, so there the two paths agree to
+// rounding rather than bit for bit.
 int tiled_nreg(int nqubits);
 struct JitFn {
   void* fn = nullptr;               // CUfunction, null = run the interpreter

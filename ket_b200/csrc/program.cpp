@@ -402,7 +402,12 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
   for (size_t i = 0; i < p.gates.size(); i++) {
     const Gate& g = plan.gates[p.gates[i]];
     if (!fits(g, p, cur)) {
-      cur = choose(plan, p, i, false, precision);
+      // A layout with the store's lanes that holds every remaining gate saves
+      // the exchange back to it at the end of the pass.
+      Lay a0 = choose(plan, p, i, true, precision);
+      bool all = true;
+      for (size_t j = i; j < p.gates.size() && all; j++) all = fits(plan.gates[p.gates[j]], p, a0);
+      cur = all ? a0 : choose(plan, p, i, false, precision);
       prog.push_back(make_exch(cur, precision));
     }
     prog.push_back(make_op(g, p, cur, prune));
