@@ -210,6 +210,12 @@ KET_API int ket_plan_program_stats(int nqubits, int precision, const ket_op* ops
  * needed); *kernels = the number of distinct kernels the plan uses, log = a
  * failed compile's log (logcap bytes).  No counterpart in the reference. */
 KET_API int ket_jit_wait(void);
+/* Drop queued background compiles and wait for the running ones (each takes
+ * about a second).  A host calls it before exiting: a compile still running
+ * while the process tears down NVRTC would crash the exit.  The Python
+ * binding registers it with atexit; the N-API addon with
+ * napi_add_env_cleanup_hook. */
+KET_API int ket_jit_shutdown(void);
 KET_API int ket_jit_stats(int64_t out[4], double* compile_seconds);
 KET_API int ket_jit_compile(int nqubits, int precision, const ket_op* ops, size_t nops, const double* mats,
                             size_t nmat, const ket_exec_opts* opts, int64_t* kernels, char* log, size_t logcap);

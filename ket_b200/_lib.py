@@ -7,6 +7,7 @@ CUDA library is missing or no GPU is present, the calls raise.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
 import threading
@@ -98,6 +99,7 @@ def lib():
             "ket_apply_ops": (i32, [vp, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts)]),
             "ket_plan_stats": (i32, [i32, i32, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts), P(C.c_int64)]),
             "ket_jit_wait": (i32, []),
+            "ket_jit_shutdown": (i32, []),
             "ket_jit_stats": (i32, [P(C.c_int64), P(dbl)]),
             "ket_jit_compile": (i32, [i32, i32, P(ket_op), sz, P(dbl), sz, P(ket_exec_opts), P(C.c_int64),
                                     C.c_char_p, sz]),
@@ -136,6 +138,8 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+        # no pass-kernel compile may still run when the process tears down NVRTC
+        atexit.register(L.ket_jit_shutdown)
         _lib = L
         return L
 

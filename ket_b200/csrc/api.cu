@@ -388,6 +388,11 @@ int ket_jit_wait(void) {
   return rc ? fail(rc, "a run-time compile of a pass kernel failed") : KET_OK;
 }
 
+int ket_jit_shutdown(void) {
+  jit_shutdown();
+  return KET_OK;
+}
+
 int ket_jit_stats(int64_t out[4], double* compile_seconds) {
   if (!out) return fail(KET_ERR_TYPE, "null argument");
   jit_stats(out, compile_seconds);

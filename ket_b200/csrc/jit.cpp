@@ -286,6 +286,9 @@ struct Cache {
 };
 
 Cache& cache() {
+  // NVRTC is opened before the cache exists, so the cache (and its threads) is
+  // torn down before NVRTC's own statics at exit
+  nvrtc();
   static Cache c;
   return c;
 }
@@ -442,6 +445,21 @@ cudaError_t jit_launch(const JitFn& f, const Pass2Args& in, int precision, cudaS
     cache().launches++;
   }
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;
+}
+
+void jit_shutdown() {
+  Cache& C = cache();
+  std::unique_lock<std::mutex> lk(C.mu);
+  for (const std::string& k : C.queue) {
+    Entry& e = C.map[k];
+    if (e.st == Entry::QUEUED) {
+      e.st = Entry::FAILED;
+      e.log = "compile cancelled at shutdown";
+    }
+  }
+  C.queue.clear();
+  C.cv.notify_all();
+  C.cv.wait(lk, [&] { return C.busy == 0; });
 }
 
 int jit_wait_all() {

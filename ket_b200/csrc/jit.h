@@ -47,6 +47,10 @@ int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cud
 cudaError_t jit_launch(const JitFn& f, const Pass2Args& a, int precision, cudaStream_t s);
 // Wait until no compile is queued or running.
 int jit_wait_all();
+// Drop queued compiles and wait for running ones.  A host calls this before it
+// exits: a compile still running when the process tears down NVRTC's statics
+// would crash the exit.
+void jit_shutdown();
 // out: kernels known, compiled, failed, launches; *compile_s: compile seconds summed over threads.
 void jit_stats(int64_t out[4], double* compile_s);
 // Compile (on the pool, waiting) the kernels of all listed passes that are not

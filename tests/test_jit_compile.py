@@ -44,3 +44,36 @@ def test_generated_kernels_compile_four_register_bits():
 def test_plan_without_tiled_passes_compiles_nothing():
     rc, kernels, _ = _compile(8, random_gates(8, 20, 1), 0, True)
     assert rc == 0 and kernels == 0
+
+
+EXIT_SCRIPT = r"""
+import sys, threading, time, ctypes as C
+sys.path.insert(0, sys.argv[1])
+import numpy as np
+from ket_b200 import _lib
+from ket_b200.workloads import brickwork_qft
+from ket_b200.circuit import ops_to_abi, flatten_ops
+L = _lib.lib()
+c, _ = brickwork_qft(22, 30, 5)
+arr, m, k = ops_to_abi(flatten_ops(c.ops))
+mv = np.ascontiguousarray(m).view(np.float64)
+o = _lib.exec_opts()
+def run():
+    kern, log = C.c_int64(), C.create_string_buffer(256)
+    L.ket_jit_compile(22, 0, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, C.byref(o),
+                      C.byref(kern), log, 256)
+threading.Thread(target=run, daemon=True).start()
+time.sleep(2.0)
+"""
+
+
+def test_exit_while_compiling_is_clean():
+    """A process that exits while kernels are still compiling exits cleanly:
+    the binding's exit hook (ket_jit_shutdown) drops the queued compiles and
+    waits for the running ones before the process tears NVRTC down."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", EXIT_SCRIPT, root], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
