@@ -454,10 +454,18 @@ def extras():
     s33.apply_abi(arr, m, k)
     t33 = time.perf_counter() - t
     n33 = s33.norm2()
+    # the same with the pass kernels compiled for its programs (compiled first, untimed)
+    s33.set_basis(0)
+    s33.apply_abi(arr, m, k, specialize=1)
+    s33.set_basis(0)
+    t = time.perf_counter()
+    s33.apply_abi(arr, m, k, specialize=1)
+    t33c = time.perf_counter() - t
     del s33
     out["precision"] = {"fidelity_31q": abs(ov) ** 2 / (na * nb), "max_abs_amp_err_31q": mx,
                         "norm_c128_31q": na, "norm_c64_31q": nb, "c64_33q_seconds": t33,
-                        "c64_33q_gates_per_s": k / t33, "c64_33q_norm": n33}
+                        "c64_33q_gates_per_s": k / t33, "c64_33q_norm": n33,
+                        "c64_33q_seconds_compiled": t33c, "c64_33q_gates_per_s_compiled": k / t33c}
     out["pershot"] = pershot_measure()
     out["json"] = json_measure()
     out["dm"] = dm_measure()

@@ -308,6 +308,12 @@ std::vector<std::string> enqueue(Cache& C, const std::vector<JitPass>& passes, i
     if (!p.prog || p.nqubits < min_qubits || (size_t)p.nops * sizeof(jit::COp) > 60000) continue;
     keys[i] = shape_key(p.prog, p.nops, precision, p.nreg);
     if (C.map.find(keys[i]) == C.map.end()) {
+      // a process compiles at most KET_JIT_MAX_KERNELS shapes (modules stay
+      // loaded); beyond that new shapes run on the interpreter
+      if (C.map.size() >= KET_JIT_MAX_KERNELS) {
+        keys[i].clear();
+        continue;
+      }
       Entry& e = C.map[keys[i]];
       e.src = make_source(p.prog, p.nops, precision, p.nreg);
       if (const char* dir = getenv("KET_JIT_DUMP")) {  // kernel sources, for inspection

@@ -14,6 +14,9 @@ namespace ket {
 // interpreter (a pass takes under a millisecond there, so compiling pays off
 // only after thousands of runs).
 #define KET_JIT_AUTO_QUBITS 26
+// Distinct program shapes a process compiles at most (their modules stay
+// loaded for the life of the process).
+#define KET_JIT_MAX_KERNELS 4096
 
 struct JitPass {
   const FOp* prog = nullptr;  // host copy of the pass's program; null = not a register-tiled pass
