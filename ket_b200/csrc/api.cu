@@ -413,14 +413,17 @@ int ket_jit_compile(int n, int precision, const ket_op* ops, size_t nops, const 
   if (o.fusion != 0) fold_single_qubit(plan.gates, o.prune != 0);
   plan_passes(n, precision, o.fusion, o.prune != 0, plan);
   std::vector<std::vector<FOp>> progs;
+  std::vector<std::vector<uint8_t>> lps;
   for (auto& p : plan.passes) {
     if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) continue;
     progs.emplace_back();
-    uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
-    plan_program(plan, p, precision, o.prune != 0, tiled_nreg(n), progs.back(), lp, sp);
+    lps.emplace_back(KET_T2_BITS);
+    uint8_t sp[KET_T2_BITS];
+    plan_program(plan, p, precision, o.prune != 0, tiled_nreg(n), progs.back(), lps.back().data(), sp);
   }
   std::vector<JitPass> jp;
-  for (auto& pr : progs) jp.push_back(JitPass{pr.data(), (int)pr.size(), n, tiled_nreg(n)});
+  for (size_t i = 0; i < progs.size(); i++)
+    jp.push_back(JitPass{progs[i].data(), (int)progs[i].size(), n, tiled_nreg(n), lps[i].data()});
   std::string clog;
   rc = jit_compile(jp, precision, kernels, clog);
   if (log && logcap) {
@@ -484,7 +487,7 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
   if (o.specialize >= 0) {
     std::vector<JitPass> jp(np);
     for (size_t i = 0; i < np; i++)
-      if (use2[i]) jp[i] = JitPass{progs[i].data(), (int)progs[i].size(), s->n, jit_nr};
+      if (use2[i]) jp[i] = JitPass{progs[i].data(), (int)progs[i].size(), s->n, jit_nr, p2[i].load_pos};
     std::string err;
     int rc = jit_prepare(jp, s->precision, o.specialize, c->stream, jf, err);
     if (rc) return fail(rc, err);

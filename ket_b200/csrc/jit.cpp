@@ -320,6 +320,15 @@ std::vector<std::string> enqueue(Cache& C, const std::vector<JitPass>& passes, i
         const std::string path = std::string(dir) + "/ket_pass_" + std::to_string(C.map.size()) + ".cu";
         if (FILE* fp = fopen(path.c_str(), "w")) {
           fputs(e.src.c_str(), fp);
+          // the layouts (role -> tile bit): the load layout, then each exchange's
+          auto lay = [&](const char* what, int k, const uint8_t* pos) {
+            fprintf(fp, "// %s %d:", what, k);
+            for (int r = 0; r < KET_T2_BITS; r++) fprintf(fp, " %d", pos[r]);
+            fputc('\n', fp);
+          };
+          if (p.load_pos) lay("load", -1, p.load_pos);
+          for (int k = 0; k < p.nops; k++)
+            if (p.prog[k].type == FO_EXCH) lay("exch", k, p.prog[k].pos);
           fclose(fp);
         }
       }

@@ -23,6 +23,7 @@ struct JitPass {
   int nops = 0;
   int nqubits = 0;
   int nreg = KET_FUSED_NREG;  // register bits of the program's layouts (4 or 5)
+  const uint8_t* load_pos = nullptr;  // the program's load layout (role -> tile bit)
 };
 
 // Register bits of the programs of compiled pass kernels for an n-qubit

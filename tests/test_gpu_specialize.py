@@ -73,6 +73,17 @@ def test_compiled_large_state_brickwork_bitwise():
     assert np.array_equal(got, want)
 
 
+def test_compiled_large_state_brickwork_c64_bitwise():
+    """The same at complex64 (FP32 gate arithmetic)."""
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import flatten_ops, ops_to_abi
+    c, _ = W.brickwork_circuit(26, 5, 13)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    got = _run(26, arr, m, k, 1, True, precision=1)
+    want = _run(26, arr, m, k, -1, True, precision=1)
+    assert np.array_equal(got, want)
+
+
 def test_compiled_large_state_qft_to_rounding():
     """Merged phase fans group their factors by role, so with the QFT's fans
     the two register-bit counts agree to rounding."""
