@@ -96,6 +96,20 @@ def test_compiled_large_state_qft_to_rounding():
     assert np.max(np.abs(got - want)) < 1e-13
 
 
+def test_compiled_large_state_random_gates_to_rounding():
+    """Every op kind at 4 register bits (shared-memory ops, controlled gates,
+    multi-qubit unitaries) against the interpreter's 5-bit programs."""
+    import ket_b200 as K
+    from ket_b200.circuit import flatten_ops, ops_to_abi
+    c = K.Circuit(26)
+    for name, qs, ps in random_gates(26, 90, 26):
+        c = c.unitary(ps, *qs) if name == "unitary" else getattr(c, name)(*ps, *qs)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    got = _run(26, arr, m, k, 1, True, init=12345)
+    want = _run(26, arr, m, k, -1, True, init=12345)
+    assert np.max(np.abs(got - want)) < 1e-13
+
+
 def test_compiled_equals_interpreter_c64():
     from ket_b200 import workloads as W
     from ket_b200.circuit import flatten_ops, ops_to_abi
