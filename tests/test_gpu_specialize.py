@@ -105,8 +105,10 @@ def test_compiled_large_state_random_gates_to_rounding():
     for name, qs, ps in random_gates(26, 90, 26):
         c = c.unitary(ps, *qs) if name == "unitary" else getattr(c, name)(*ps, *qs)
     arr, m, k = ops_to_abi(flatten_ops(c.ops))
-    got = _run(26, arr, m, k, 1, True, init=12345)
-    want = _run(26, arr, m, k, -1, True, init=12345)
+    # without pruning: a last-bit difference from a phase fan next to the
+    # 1e-7 threshold could flip a prune decision
+    got = _run(26, arr, m, k, 1, False, init=12345)
+    want = _run(26, arr, m, k, -1, False, init=12345)
     assert np.max(np.abs(got - want)) < 1e-13
 
 
