@@ -217,12 +217,15 @@ std::string shape_key(const FOp* prog, int nops, int precision, int nreg) {
   return k;
 }
 
-// A kernel's state: queued / compiling / compiled (cubin) / failed; modules per device.
+// A kernel's state: queued / compiling / compiled (cubin) / failed, and its
+// module instances.
 struct Entry {
   enum { QUEUED, BUSY, READY, FAILED } st = QUEUED;
   std::string src, log;
   std::vector<char> cubin;
-  std::map<void*, JitFn> fn;  // stream -> kernel loaded for it (each stream owns its constant array)
+  // (device, stream) -> the kernel loaded for it: each stream owns a module
+  // instance, because a launch fills the module's constant array
+  std::map<std::pair<int, void*>, JitFn> fn;
 };
 
 struct Cache {
@@ -392,11 +395,14 @@ int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cud
     if (!wait_keys(C, lk, keys, log)) return err = "run-time compile of a pass kernel failed: " + log, KET_ERR_CUDA;
   }
   Driver& D = driver();
+  int device = 0;
+  cudaGetDevice(&device);
   for (size_t i = 0; i < passes.size(); i++) {
     if (keys[i].empty()) continue;
     Entry& e = C.map[keys[i]];
     if (e.st != Entry::READY) continue;
-    auto f = e.fn.find((void*)stream);
+    const std::pair<int, void*> where(device, (void*)stream);
+    auto f = e.fn.find(where);
     if (f == e.fn.end()) {
       CUmodule mod;
       CUfunction fn;
@@ -416,7 +422,7 @@ int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cud
       j.fn = (void*)fn;
       j.cops = (unsigned long long)cops;
       j.cops_bytes = cbytes;
-      f = e.fn.emplace((void*)stream, j).first;
+      f = e.fn.emplace(where, j).first;
     }
     out[i] = f->second;
   }
