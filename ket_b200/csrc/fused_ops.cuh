@@ -99,16 +99,35 @@ __device__ __forceinline__ float hiabs(float v) { return fabsf(v); }
 __device__ __forceinline__ float tiny_screen(double) { return __int_as_float(0x3E7AD7F3); }
 __device__ __forceinline__ float tiny_screen(float) { return __int_as_float(0x33D6BF96); }  // just above 1e-7f
 
+// Three-input minimum (sm_100): min over N values in about N/2 instructions.
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+// t[0] = min(t[0..N)), one tree level of three-input minima at a time.
+template <int N>
+__device__ __forceinline__ void min_tree(float* t) {
+  if constexpr (N > 1) {
+    constexpr int M = (N + 2) / 3;
+#pragma unroll
+    for (int i = 0; i < M; i++) {
+      const int a = 3 * i;  // a >= i: t[i] is written after its inputs are read
+      if (a + 2 < N) t[i] = fmin3(t[a], t[a + 1], t[a + 2]);
+      else if (a + 1 < N) t[i] = fminf(t[a], t[a + 1]);
+      else t[i] = t[a];
+    }
+    min_tree<M>(t);
+  }
+}
+
 template <typename R, int NS>
 __device__ __forceinline__ void prune_slots(cpx<R>* x, double thr, double qthr) {
   // an amplitude can be pruned only if both components are below 1e-7
   float t[NS];
 #pragma unroll
   for (int j = 0; j < NS; j++) t[j] = fmaxf(hiabs(x[j].re), hiabs(x[j].im));
-#pragma unroll
-  for (int w = NS / 2; w > 0; w >>= 1)
-#pragma unroll
-    for (int j = 0; j < w; j++) t[j] = fminf(t[j], t[j + w]);
+  min_tree<NS>(t);
   if (t[0] < tiny_screen(R(0))) {
 #pragma unroll
     for (int j = 0; j < NS; j++) prune_amp(x[j], thr, qthr);
