@@ -99,11 +99,16 @@ __device__ __forceinline__ float hiabs(float v) { return fabsf(v); }
 __device__ __forceinline__ float tiny_screen(double) { return __int_as_float(0x3E7AD7F3); }
 __device__ __forceinline__ float tiny_screen(float) { return __int_as_float(0x33D6BF96); }  // just above 1e-7f
 
-// Three-input minimum (sm_100): min over N values in about N/2 instructions.
+// Three-input minimum (sm_100, PTX of CUDA 12.9 on): min over N values in
+// about N/2 instructions.  KET_NO_MIN3: an older runtime compiler.
 __device__ __forceinline__ float fmin3(float a, float b, float c) {
+#ifdef KET_NO_MIN3
+  return fminf(fminf(a, b), c);
+#else
   float r;
   asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
   return r;
+#endif
 }
 // t[0] = min(t[0..N)), one tree level of three-input minima at a time.
 template <int N>

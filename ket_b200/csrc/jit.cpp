@@ -51,6 +51,7 @@ typedef struct _nvrtcProgram* nvrtcProgram_t;
 struct Nvrtc {
   bool ok = false;
   std::string err;
+  int major = 0, minor = 0;
   nvrtcResult_t (*create)(nvrtcProgram_t*, const char*, const char*, int, const char* const*, const char* const*);
   nvrtcResult_t (*compile)(nvrtcProgram_t, int, const char* const*);
   nvrtcResult_t (*cubin_size)(nvrtcProgram_t, size_t*);
@@ -62,7 +63,9 @@ struct Nvrtc {
 
 Nvrtc load_nvrtc() {
   Nvrtc n;
-  const char* names[] = {"libnvrtc.so.12", "/usr/local/cuda/lib64/libnvrtc.so.12", "libnvrtc.so"};
+  // The toolkit's NVRTC first, by path: after `import torch` the soname
+  // resolves to torch's bundled (possibly older) copy already in the process.
+  const char* names[] = {"/usr/local/cuda/lib64/libnvrtc.so.12", "libnvrtc.so.12", "libnvrtc.so"};
   void* h = nullptr;
   for (const char* nm : names)
     if ((h = dlopen(nm, RTLD_NOW | RTLD_LOCAL))) break;
@@ -80,6 +83,7 @@ Nvrtc load_nvrtc() {
   n.destroy = (decltype(n.destroy))sym("nvrtcDestroyProgram");
   n.ok = n.create && n.compile && n.cubin_size && n.cubin && n.log_size && n.log && n.destroy;
   if (!n.ok) n.err = "NVRTC is missing an entry point";
+  if (auto ver = (nvrtcResult_t(*)(int*, int*))sym("nvrtcVersion")) ver(&n.major, &n.minor);
   return n;
 }
 
@@ -106,6 +110,8 @@ bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string
     return false;
   }
   std::vector<const char*> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-DNDEBUG"};
+  // three-input min.f32 needs the PTX of CUDA 12.9 or later
+  if (N.major < 12 || (N.major == 12 && N.minor < 9)) opts.push_back("-DKET_NO_MIN3");
   if (getenv("KET_JIT_VERBOSE")) opts.push_back("-Xptxas=-v");  // register and spill report in the log
   const int rc = N.compile(prog, (int)opts.size(), opts.data());
   size_t ls = 0;

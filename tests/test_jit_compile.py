@@ -77,3 +77,34 @@ def test_exit_while_compiling_is_clean():
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     r = subprocess.run([sys.executable, "-c", EXIT_SCRIPT, root], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+TORCH_FIRST_SCRIPT = r"""
+import sys, ctypes as C
+sys.path.insert(0, sys.argv[1])
+import torch  # noqa: F401  (brings its own libnvrtc.so.12 into the process)
+import numpy as np
+from ket_b200 import _lib
+from ket_b200.workloads import brickwork_qft
+from ket_b200.circuit import ops_to_abi, flatten_ops
+c, _ = brickwork_qft(14, 2, 3)
+arr, m, k = ops_to_abi(flatten_ops(c.ops))
+mv = np.ascontiguousarray(m).view(np.float64)
+o = _lib.exec_opts()
+kern, log = C.c_int64(), C.create_string_buffer(1 << 14)
+rc = _lib.lib().ket_jit_compile(14, 0, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, C.byref(o),
+                                C.byref(kern), log, len(log))
+assert rc == 0 and kern.value >= 1, log.value.decode(errors="replace")[:2000]
+"""
+
+
+def test_compiles_after_torch_is_imported():
+    """torch links its own, older NVRTC under the same soname; the kernels
+    still compile when torch was imported first."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", TORCH_FIRST_SCRIPT, root], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
