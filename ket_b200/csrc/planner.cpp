@@ -356,11 +356,14 @@ void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& pl
     return;
   }
 
-  // Gates a pass over tile set S would absorb (the sweep below, counted).
+  // Score of a pass over tile set S: the gates it would absorb (the sweep
+  // below, counted).  With the reference's pruning, mixing gates must keep
+  // their order, so how far a pass gets along them decides how many passes
+  // follow: mixing gates absorbed count first, then all gates.
   auto absorbed = [&](uint64_t S, std::vector<uint64_t>* cand) -> int {
     uint64_t B = 0;
     bool mixblocked = false;
-    int taken = 0;
+    int taken = 0, tmix = 0;
     for (int gi : pending) {
       const Gate& g = G[gi];
       uint64_t qs = gate_qubits(g);
@@ -378,8 +381,9 @@ void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& pl
         continue;
       }
       taken++;
+      if (mixing) tmix++;
     }
-    return taken;
+    return tmix * 65536 + taken;
   };
 
   while (!pending.empty()) {
