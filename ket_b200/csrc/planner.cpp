@@ -360,11 +360,15 @@ void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& pl
   // below, counted).  With the reference's pruning, mixing gates must keep
   // their order, so how far a pass gets along them decides how many passes
   // follow: mixing gates absorbed count first, then all gates.
+  // Every gate touches a qubit, so once the skipped gates block all of them
+  // (B == everything) no later gate can join.
+  const uint64_t allq = n >= 64 ? ~uint64_t(0) : bit(n) - 1;
   auto absorbed = [&](uint64_t S, std::vector<uint64_t>* cand) -> int {
     uint64_t B = 0;
     bool mixblocked = false;
     int taken = 0, tmix = 0;
     for (int gi : pending) {
+      if ((B & allq) == allq) break;
       const Gate& g = G[gi];
       uint64_t qs = gate_qubits(g);
       bool mixing = keep_mix_order && is_mixing(g);
