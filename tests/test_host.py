@@ -181,6 +181,23 @@ def plan(c, fusion=-1, prec=0):
     return list(out)
 
 
+def test_planner_pass_counts_on_the_bench_workload():
+    """The tile planner on the 30-qubit bench circuit (no GPU needed): with
+    the reference's pruning, mixing gates keep their order and a candidate
+    tile scores first by the mixing gates it takes (106 passes; 90 is a lower
+    bound for the mixing gates alone); without pruning, 42 passes."""
+    c, _ = W.brickwork_qft(30, 40, 42)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    mv = np.ascontiguousarray(m).view(np.float64)
+    for prune, most in ((True, 106), (False, 42)):
+        o = _lib.exec_opts(-1, prune)
+        out = (C.c_int64 * 3)()
+        _lib.check(_lib.lib().ket_plan_stats(30, 0, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size,
+                                             C.byref(o), out))
+        assert 90 <= out[0] <= most if prune else out[0] <= most, (prune, list(out))
+        assert out[1] == 0 and out[2] <= k
+
+
 def test_planner_statistics():
     c, _ = W.brickwork_circuit(16, 20, 42)
     fused = plan(c)
