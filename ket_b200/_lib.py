@@ -172,6 +172,14 @@ def default_ctx():
     return _ctx
 
 
+def jit_stats() -> dict:
+    """Compiled pass kernels in this process: shapes known, compiled, failed,
+    launches, and the compile seconds summed over threads."""
+    out, cs = (C.c_int64 * 4)(), C.c_double()
+    check(lib().ket_jit_stats(out, C.byref(cs)))
+    return {"kernels": out[0], "compiled": out[1], "failed": out[2], "launches": out[3], "compile_s": cs.value}
+
+
 def exec_opts(fusion: int = -1, prune: bool = True, specialize: int = 0) -> ket_exec_opts:
     o = ket_exec_opts()
     lib().ket_exec_opts_default(C.byref(o))

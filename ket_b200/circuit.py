@@ -23,7 +23,7 @@ from typing import Callable, Dict, Iterable, List, NamedTuple, Optional, Sequenc
 import numpy as np
 
 from . import gates as G
-from ._lib import (KET_C128, KET_C64, OP_BARRIER, OP_CNOT, OP_CONTROLLED, OP_CSRSWAP, OP_CSWAP, OP_IF, OP_MEASURE,
+from ._lib import (KET_C128, KET_C64, KetError, OP_BARRIER, OP_CNOT, OP_CONTROLLED, OP_CSRSWAP, OP_CSWAP, OP_IF, OP_MEASURE,
                    OP_RESET, OP_SINGLE, OP_SWAP, OP_TOFFOLI, OP_TWO, OP_UNITARY, RangeError, check, default_ctx,
                    exec_opts, ket_noise, ket_op, lib)
 
@@ -553,6 +553,23 @@ class Circuit:
         a = self._state(initialState).amplitudes_dense()
         nz = np.nonzero(a)[0]
         return {int(i): complex(a[i]) for i in nz}
+
+    def compile_kernels(self, precision: int = KET_C128, prune: bool = True) -> int:
+        """Compile, on all host cores and ahead of the first run, the pass
+        kernels this circuit's plan uses (ket_jit_compile; no GPU needed).
+        Returns the number of distinct kernels.  No counterpart in the
+        reference."""
+        self._require_pure("compile_kernels()")
+        arr, m, k = ops_to_abi(flatten_ops(self.ops))
+        mv = np.ascontiguousarray(m).view(np.float64)
+        o = exec_opts(-1, prune)
+        kernels = C.c_int64()
+        log = C.create_string_buffer(1 << 14)
+        rc = lib().ket_jit_compile(self.qubits, precision, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size,
+                                   C.byref(o), C.byref(kernels), log, len(log))
+        if rc:
+            raise KetError(log.value.decode(errors="replace") or lib().ket_last_error().decode(), rc)
+        return int(kernels.value)
 
     def statevector_array(self, initialState: Optional[str] = None, precision: int = KET_C128) -> np.ndarray:
         """Dense complex128 array of all 2^n amplitudes (index bit q = qubit q)."""

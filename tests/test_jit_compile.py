@@ -108,3 +108,19 @@ def test_compiles_after_torch_is_imported():
     r = subprocess.run([sys.executable, "-c", TORCH_FIRST_SCRIPT, root], capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+def test_circuit_compile_kernels_ahead_of_a_run():
+    """Circuit.compile_kernels fills the process's kernel cache (no GPU)."""
+    import ket_b200 as K
+    from ket_b200 import _lib
+    from ket_b200.workloads import brickwork_qft
+    c, _ = brickwork_qft(13, 3, 8)
+    before = _lib.jit_stats()
+    n = c.compile_kernels()
+    after = _lib.jit_stats()
+    assert n >= 1 and after["kernels"] >= before["kernels"] and after["failed"] == before["failed"]
+    assert c.compile_kernels() == n  # cached: nothing new to compile
+    assert _lib.jit_stats()["compiled"] == after["compiled"]
+    with pytest.raises(TypeError):
+        K.Circuit(1).creg("c", 1).measure(0, "c", 0).compile_kernels()
