@@ -92,8 +92,9 @@ typedef struct ket_exec_opts {
   int32_t prune;       /* 1 = reference accumulate() semantics: every computed amplitude with
                           |a|^2 < 1e-14 is flushed to zero (statevector.ts:19-27); 0 = plain dense */
   int32_t specialize;  /* register-tiled passes: 0 = automatic (default): kernels compiled for the
-                          pass's program where one is ready, the interpreter otherwise, compiling
-                          on background threads for states of 26+ qubits; 1 = compile what is
+                          pass's program where one is ready (from earlier runs or ket_jit_compile),
+                          the interpreter otherwise, compiling on background threads for states of
+                          26+ qubits; 1 = compile what is
                           missing first, then use compiled kernels only; -1 = interpreter only.
                           Results are identical either way.  No counterpart in the reference. */
   int32_t reserved[5];

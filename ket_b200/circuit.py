@@ -556,7 +556,8 @@ class Circuit:
 
     def compile_kernels(self, precision: int = KET_C128, prune: bool = True) -> int:
         """Compile, on all host cores and ahead of the first run, the pass
-        kernels this circuit's plan uses (ket_jit_compile; no GPU needed).
+        kernels this circuit's plan uses (ket_jit_compile; no GPU needed), so
+        that runs under the default policy use them at any qubit count.
         Returns the number of distinct kernels.  No counterpart in the
         reference."""
         self._require_pure("compile_kernels()")

@@ -12,10 +12,11 @@
 // Policy (ket_exec_opts.specialize):
 //  -1   interpreter only;
 //   1   compile what is missing, waiting for it, then run compiled kernels;
-//   0   (default) run compiled kernels that are ready; passes of states of 26
-//       qubits or more whose kernel is missing run on the interpreter and
-//       queue the compile on background threads, so a repeated circuit speeds
-//       up without a first call that waits for the compiler.
+//   0   (default) run compiled kernels that are ready (from earlier runs or
+//       ket_jit_compile); passes of states of 26 qubits or more whose kernel
+//       is missing run on the interpreter and queue the compile on background
+//       threads, so a repeated circuit speeds up without a first call that
+//       waits for the compiler.
 //
 // NVRTC is loaded with dlopen on first use and the driver entry points come
 // from the runtime (cudaGetDriverEntryPoint): the library links neither.
@@ -307,16 +308,22 @@ Cache& cache() {
 namespace {
 
 // Queue the kernels of passes that are not known yet (under C.mu); keys[i] is
-// the shape of pass i, empty for a pass without a kernel or below min_qubits.
+// the shape of pass i, empty for a pass without a kernel, or without a known
+// one on a state below min_qubits.
 std::vector<std::string> enqueue(Cache& C, const std::vector<JitPass>& passes, int precision, int min_qubits) {
   std::vector<std::string> keys(passes.size());
   bool queued = false;
   for (size_t i = 0; i < passes.size(); i++) {
     const JitPass& p = passes[i];
     // the constant op array holds at most 64 KB (512 records)
-    if (!p.prog || p.nqubits < min_qubits || (size_t)p.nops * sizeof(jit::COp) > 60000) continue;
+    if (!p.prog || (size_t)p.nops * sizeof(jit::COp) > 60000) continue;
     keys[i] = shape_key(p.prog, p.nops, precision, p.nreg);
     if (C.map.find(keys[i]) == C.map.end()) {
+      // below min_qubits a ready kernel is used but none is compiled
+      if (p.nqubits < min_qubits) {
+        keys[i].clear();
+        continue;
+      }
       // a process compiles at most KET_JIT_MAX_KERNELS shapes (modules stay
       // loaded); beyond that new shapes run on the interpreter
       if (C.map.size() >= KET_JIT_MAX_KERNELS) {

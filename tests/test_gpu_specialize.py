@@ -136,3 +136,18 @@ def test_automatic_policy_uses_ready_kernels():
     got = _run(26, arr, m, k, 0, True)
     assert _jit_stats()[3] > before
     assert np.array_equal(got, want)
+
+
+def test_kernels_compiled_ahead_serve_the_default_policy():
+    """Below 26 qubits the default policy compiles nothing itself, but uses
+    kernels compiled ahead of time (Circuit.compile_kernels)."""
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import flatten_ops, ops_to_abi
+    c, _ = W.brickwork_qft(15, 6, 77)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    want = _run(15, arr, m, k, -1, True)
+    assert c.compile_kernels() >= 1
+    before = _jit_stats()[3]
+    got = _run(15, arr, m, k, 0, True)
+    assert _jit_stats()[3] > before
+    assert np.array_equal(got, want)
