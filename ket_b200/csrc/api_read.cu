@@ -35,6 +35,9 @@ int launched(cudaError_t e) { return e == cudaSuccess ? KET_OK : cuda_fail(e, "k
 
 // Launch a read-out kernel bracketed for accounting/profiling.
 #define LAUNCH_READ(c, expr) (prof_begin(c), prof_end_ret((c), (expr)))
+// The same for a launcher that issues two kernels (block partials, then their
+// fixed-order sum): the launch counter counts both.
+#define LAUNCH_READ2(c, expr) ((c)->launches++, LAUNCH_READ(c, expr))
 int prof_end_ret(ket_ctx* c, cudaError_t e) {
   prof_end(c, PK_READ);
   return launched(e);
@@ -71,7 +74,7 @@ int ket_norm2(const ket_state* s, double* out) {
   void* scr;
   TRY(ctx_scratch(s->ctx, norm2_scratch(s->n) + 64, &scr));
   double* res = (double*)scr;
-  TRY(LAUNCH_READ(s->ctx, launch_norm2(s->amp, s->n, s->precision, res + 8, res, s->ctx->stream)));
+  TRY(LAUNCH_READ2(s->ctx, launch_norm2(s->amp, s->n, s->precision, res + 8, res, s->ctx->stream)));
   TRY(d2h(s->ctx, out, res, 8));
   return ctx_wait(s->ctx);
 }
@@ -85,7 +88,7 @@ int ket_state_compare(const ket_state* a, const ket_state* b, double* overlap_re
   void* scr;
   TRY(ctx_scratch(a->ctx, compare_scratch(a->n) + 64, &scr));
   double* res = (double*)scr;
-  TRY(LAUNCH_READ(a->ctx, launch_compare(a->amp, a->precision, b->amp, b->precision, a->n, res + 8, res,
+  TRY(LAUNCH_READ2(a->ctx, launch_compare(a->amp, a->precision, b->amp, b->precision, a->n, res + 8, res,
                                          a->ctx->stream)));
   double h[3];
   TRY(d2h(a->ctx, h, res, 24));
@@ -147,7 +150,7 @@ int ket_marginals(const ket_state* s, double* out) {
   TRY(ctx_scratch(s->ctx, 8 * (nb * s->n + s->n) + 512, &scr));
   double* res = (double*)scr;
   double* partial = (double*)align_up((char*)(res + s->n), 256);
-  TRY(LAUNCH_READ(s->ctx, launch_marginals(s->amp, s->n, s->precision, partial, res, s->ctx->stream)));
+  TRY(LAUNCH_READ2(s->ctx, launch_marginals(s->amp, s->n, s->precision, partial, res, s->ctx->stream)));
   TRY(d2h(s->ctx, out, res, 8 * s->n));
   return ctx_wait(s->ctx);
 }
@@ -172,7 +175,7 @@ int ket_marginal_dist(const ket_state* s, const int* qubits, int m, double* out)
   TRY(ctx_scratch(s->ctx, 8 * (nb * width + width) + 512, &scr));
   double* res = (double*)scr;
   double* partial = (double*)align_up((char*)(res + width), 256);
-  TRY(LAUNCH_READ(s->ctx, launch_marginal_dist(s->amp, s->n, s->precision, spec, partial, res, s->ctx->stream)));
+  TRY(LAUNCH_READ2(s->ctx, launch_marginal_dist(s->amp, s->n, s->precision, spec, partial, res, s->ctx->stream)));
   TRY(d2h(s->ctx, out, res, 8 * width));
   return ctx_wait(s->ctx);
 }
@@ -235,7 +238,7 @@ int pauli_terms_expect(const ket_state* s, const std::vector<Term>& terms, doubl
   double* res = (double*)scr;
   double* partial = (double*)align_up((char*)(res + gl.size()), 256);
   for (size_t i = 0; i < gl.size(); i++)
-    TRY(LAUNCH_READ(s->ctx, launch_pauli_group(s->amp, s->n, s->precision, gl[i], partial, res + i, s->ctx->stream)));
+    TRY(LAUNCH_READ2(s->ctx, launch_pauli_group(s->amp, s->n, s->precision, gl[i], partial, res + i, s->ctx->stream)));
   std::vector<double> h(gl.size());
   TRY(d2h(s->ctx, h.data(), res, 8 * gl.size()));
   TRY(ctx_wait(s->ctx));
