@@ -199,6 +199,8 @@ int sample_indices(const ket_state* s, const double* r, size_t shots, double thr
   uint64_t* dout = (uint64_t*)align_up((char*)(dr + shots), 256);
   void* work = align_up((char*)(dout + shots), 256);
   TRY(h2d(s->ctx, dr, r, 8 * shots));
+  // the sequential CDF path runs two kernels, the chunked one three
+  s->ctx->launches += (s->n <= seq_qubits || s->n < 10) ? 1 : 2;
   TRY(LAUNCH_READ(s->ctx, launch_sample(s->amp, s->n, s->precision, thr, seq_qubits, dr, shots, work, dout,
                                          s->ctx->stream)));
   TRY(d2h(s->ctx, out, dout, 8 * shots));
