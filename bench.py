@@ -186,8 +186,9 @@ SAMPLE_N, SAMPLE_FIRST, SAMPLE_OPS = 20, 70, 12
 
 def cpu_sample(_=None):
     """Time the reference algorithm (sparse map with pruning, 1 thread) on
-    ops [100, 112) of the 20-qubit brickwork(40)+qft(20) circuit (seed 42),
-    after simulating ops [0, 100) untimed.  Returns (seconds, amplitude updates)."""
+    ops [SAMPLE_FIRST, SAMPLE_FIRST + SAMPLE_OPS) = [70, 82) of the 20-qubit
+    brickwork(40)+qft(20) circuit (seed 42), after simulating ops [0, 70)
+    untimed.  Returns (seconds, amplitude updates)."""
     from oracle import oracle as O
     c, _ = O.brickwork(SAMPLE_N, 40, 42, with_qft=True)
     return c.time_ops(SAMPLE_FIRST, SAMPLE_OPS, mode=O.SPARSE)

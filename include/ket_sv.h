@@ -97,7 +97,11 @@ typedef struct ket_exec_opts {
                           26+ qubits; 1 = compile what is
                           missing first, then use compiled kernels only; -1 = interpreter only.
                           Results are identical either way.  No counterpart in the reference. */
-  int32_t reserved[5];
+  int32_t reg_bits;    /* register bits of the compiled kernels' programs: 0 = automatic (default:
+                          5 below 26 qubits, 4 from there on), 4 or 5 = that count at any size, so
+                          that the programs large states run can be checked on small ones.  The
+                          interpreter always uses 5.  No counterpart in the reference. */
+  int32_t reserved[4];
 } ket_exec_opts;
 
 /* NoiseParams (circuit.ts:213-221): depolarizing probability per single-qubit
@@ -245,6 +249,9 @@ KET_API int ket_marginals(const ket_state* st, double* out);
  * would exceed it.  The first call on a device looks the array up
  * (cudaGetSymbolAddress) and should come before any stream capture.  All calls
  * share the array: calls that overlap on the GPU race and give wrong results.
+ * amp and out must be device (or managed) memory of the current device, else
+ * KET_ERR_TYPE.  The array's address is kept per device for the life of the
+ * process, so the call must not be used on a device after cudaDeviceReset.
  * No counterpart in the reference. */
 #define KET_NOALLOC_SCRATCH_BYTES (2048u * 40u * 8u)
 KET_API int ket_marginals_noalloc(const void* amp, int nqubits, int precision, double* out, void* stream);

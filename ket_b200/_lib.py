@@ -48,7 +48,8 @@ class ket_noise(C.Structure):
 
 
 class ket_exec_opts(C.Structure):
-    _fields_ = [("fusion", C.c_int32), ("prune", C.c_int32), ("specialize", C.c_int32), ("reserved", C.c_int32 * 5)]
+    _fields_ = [("fusion", C.c_int32), ("prune", C.c_int32), ("specialize", C.c_int32), ("reg_bits", C.c_int32),
+                ("reserved", C.c_int32 * 4)]
 
 
 class ket_param_binding(C.Structure):
@@ -180,10 +181,11 @@ def jit_stats() -> dict:
     return {"kernels": out[0], "compiled": out[1], "failed": out[2], "launches": out[3], "compile_s": cs.value}
 
 
-def exec_opts(fusion: int = -1, prune: bool = True, specialize: int = 0) -> ket_exec_opts:
+def exec_opts(fusion: int = -1, prune: bool = True, specialize: int = 0, reg_bits: int = 0) -> ket_exec_opts:
     o = ket_exec_opts()
     lib().ket_exec_opts_default(C.byref(o))
     o.fusion = fusion
     o.prune = 1 if prune else 0
     o.specialize = specialize
+    o.reg_bits = reg_bits
     return o

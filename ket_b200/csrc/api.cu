@@ -404,6 +404,7 @@ int ket_jit_compile(int n, int precision, const ket_op* ops, size_t nops, const 
   ket_exec_opts o;
   if (opts) o = *opts; else ket_exec_opts_default(&o);
   if (n < 1 || n > KET_MAX_QUBITS) return fail(KET_ERR_RANGE, "qubit count out of range");
+  if (o.reg_bits != 0 && o.reg_bits != 4 && o.reg_bits != 5) return fail(KET_ERR_RANGE, "reg_bits must be 0, 4 or 5");
   if (kernels) *kernels = 0;
   if (log && logcap) log[0] = 0;
   Plan plan;
@@ -419,11 +420,11 @@ int ket_jit_compile(int n, int precision, const ket_op* ops, size_t nops, const 
     progs.emplace_back();
     lps.emplace_back(KET_T2_BITS);
     uint8_t sp[KET_T2_BITS];
-    plan_program(plan, p, precision, o.prune != 0, tiled_nreg(n), progs.back(), lps.back().data(), sp);
+    plan_program(plan, p, precision, o.prune != 0, tiled_nreg(n, o.reg_bits), progs.back(), lps.back().data(), sp);
   }
   std::vector<JitPass> jp;
   for (size_t i = 0; i < progs.size(); i++)
-    jp.push_back(JitPass{progs[i].data(), (int)progs[i].size(), n, tiled_nreg(n), lps[i].data()});
+    jp.push_back(JitPass{progs[i].data(), (int)progs[i].size(), n, tiled_nreg(n, o.reg_bits), lps[i].data()});
   std::string clog;
   rc = jit_compile(jp, precision, kernels, clog);
   if (log && logcap) {
@@ -439,6 +440,7 @@ int ket_apply_ops(ket_state* s, const ket_op* ops, size_t nops, const double* ma
   if (nops && !ops) return fail(KET_ERR_TYPE, "null op list");
   ket_exec_opts o;
   if (opts) o = *opts; else ket_exec_opts_default(&o);
+  if (o.reg_bits != 0 && o.reg_bits != 4 && o.reg_bits != 5) return fail(KET_ERR_RANGE, "reg_bits must be 0, 4 or 5");
   Plan plan;
   std::string err;
   int rc = lower_ops(s->n, ops, nops, mats, nmat, o.prune != 0, plan.gates, err);
@@ -468,7 +470,7 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
   // Register-tiled passes: compiled kernels (jit.cpp) use programs with
   // tiled_nreg(n) register bits; a pass whose kernel is not ready runs on the
   // interpreter with KET_FUSED_NREG.
-  const int jit_nr = tiled_nreg(s->n);
+  const int jit_nr = tiled_nreg(s->n, o.reg_bits);
   std::vector<std::vector<FOp>> progs(np);
   std::vector<JitFn> jf(np);
   auto lower_pass = [&](size_t i, int nreg) {

@@ -21,6 +21,7 @@
 // masks and a per-layer table of |E|+1 phases.  <C> partials are written per
 // (instance, tile) and reduced in a fixed order.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -152,18 +153,29 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
     const int nhigh = n - T;               // qubits >= T
     const int lowB = T - nhigh;            // low qubits kept in pass-B tiles
     if (w.pass > 0) {
-      // wait until every tile of the previous pass has been written back
+      // wait until every tile of the previous pass has been written back; a
+      // wait that ran out anywhere (status set) ends every later wait at once
       const unsigned int need = (unsigned int)w.pass * (unsigned int)I.ntiles;
       if (threadIdx.x == 0) {
         volatile unsigned int* d = a.done + w.inst;
+        volatile int* st = a.status;
         uint32_t spins = 0;
         while (*d < need) {
+          if (*st != 0) break;
           if (++spins > a.spin_limit) { atomicExch(a.status, (int)KET_ERR_TIMEOUT); break; }
           __nanosleep(200);
         }
         __threadfence();
+        item_sh = *st;
       }
       __syncthreads();
+      const bool failed = item_sh != 0;
+      __syncthreads();
+      if (failed) {
+        // the call reports the timeout; drain the queue without the tile's work
+        if (threadIdx.x == 0) atomicAdd(a.done + w.inst, 1u);
+        continue;
+      }
     }
     double2* g = a.work + I.state;
     // global index of tile element i
@@ -248,11 +260,14 @@ using namespace ket;
 // when use_graph is set.
 template <int NT>
 static cudaError_t run_batch(ket_ctx* c, const QArgs& a, size_t smem, int ninst, double* dout, int use_graph) {
-  static bool attr = false;
-  if (!attr) {
+  // the shared-memory limit is a per-device attribute of the kernel
+  static std::atomic<uint64_t> attr_set{0};
+  const uint64_t bit = uint64_t(1) << (c->device & 63);
+  if (!(attr_set.load() & bit)) {
     const size_t smax = (16u << 12) + 16 * (KQ_MAX_EDGES + 1) + 8 * KQ_MAX_EDGES + 8 * 32;
-    cudaFuncSetAttribute(k_batch_qaoa<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
-    attr = true;
+    cudaError_t e = cudaFuncSetAttribute(k_batch_qaoa<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+    if (e != cudaSuccess) return e;
+    attr_set.fetch_or(bit);
   }
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_qaoa<NT>, NT, smem);
@@ -265,6 +280,21 @@ static cudaError_t run_batch(ket_ctx* c, const QArgs& a, size_t smem, int ninst,
     return cudaGetLastError();
   };
   if (!use_graph) return record();
+  // A batch of the same shape reuses the executable graph: its inputs were
+  // re-uploaded to the same addresses, so only a changed launch (sizes,
+  // buffers, shape) is captured and instantiated again.
+  uint64_t key = 1469598103934665603ull;
+  auto mix = [&](const void* p, size_t nb) {
+    for (size_t i = 0; i < nb; i++) key = (key ^ ((const unsigned char*)p)[i]) * 1099511628211ull;
+  };
+  const int nt = NT;
+  mix(&a, sizeof(a));
+  mix(&smem, sizeof(smem));
+  mix(&ninst, sizeof(ninst));
+  mix(&dout, sizeof(dout));
+  mix(&nt, sizeof(nt));
+  mix(&grid, sizeof(grid));
+  if (c->graph_exec && c->graph_key == key) return cudaGraphLaunch(c->graph_exec, c->stream);
   cudaGraph_t graph;
   cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return e;
@@ -273,9 +303,11 @@ static cudaError_t run_batch(ket_ctx* c, const QArgs& a, size_t smem, int ninst,
   if (e != cudaSuccess) return e;
   if (e2 != cudaSuccess) return e2;
   if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+  c->graph_key = 0;
   e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return e;
+  c->graph_key = key;
   return cudaGraphLaunch(c->graph_exec, c->stream);
 }
 
@@ -362,6 +394,7 @@ extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne
     int rc = ctx_wait(c);
     if (rc) return rc;
     if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+    c->graph_key = 0;
     if (c->scratch2) cudaFree(c->scratch2);
     c->scratch2 = nullptr;
     c->scratch2_bytes = 0;

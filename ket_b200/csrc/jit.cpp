@@ -442,7 +442,8 @@ int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cud
   return KET_OK;
 }
 
-int tiled_nreg(int nqubits) {
+int tiled_nreg(int nqubits, int reg_bits) {
+  if (reg_bits == 4 || reg_bits == 5) return reg_bits;
   static const int large = [] {
     const char* e = getenv("KET_JIT_NREG");
     return e && atoi(e) == 5 ? 5 : 4;

@@ -34,8 +34,9 @@ struct JitPass {
 // the interpreter, which keeps 5; KET_JIT_NREG=5 in the environment keeps 5
 // throughout.  Register and lane forms of a gate round alike, but merged
 // phase fans group their factors by role, so there the two paths agree to
-// rounding rather than bit for bit.
-int tiled_nreg(int nqubits);
+// rounding rather than bit for bit.  reg_bits (ket_exec_opts.reg_bits) 4 or 5
+// forces that count at any size; 0 leaves the choice above.
+int tiled_nreg(int nqubits, int reg_bits = 0);
 struct JitFn {
   void* fn = nullptr;               // CUfunction, null = run the interpreter
   unsigned long long cops = 0;      // device address of the kernel's constant op array

@@ -220,25 +220,88 @@ __global__ void k_marginal_dist(const typename Vec2<R>::T* a, int c, MarginalSpe
 }
 
 // ------------------------------------------------------------------ sampling
-// Exact reference order (small states): one thread accumulates the running
-// FP64 sum over kept entries in ascending index order (circuit.ts:3429-3436).
+// Exact reference order (small states): the running FP64 sum over kept
+// entries in ascending index order (circuit.ts:3429-3436).  The sum itself is
+// one dependent chain of additions and stays on one thread; what surrounds it
+// is spread over the block.  The state streams through three shared-memory
+// chunks: while thread 0 sums chunk c, warps 1.. load chunk c+1 as kept
+// probabilities and write chunk c-1's running sums to cum, all coalesced.  An
+// entry that is not kept is stored as -0.0: adding it leaves a non-negative
+// sum unchanged, so the chain equals the reference's conditional sum bit for
+// bit, and its sign bit tells it apart from a kept p = +0.0 (a threshold
+// below zero keeps those).  The last kept index stays on the device for the
+// sampler.
+constexpr int kCdfChunk = 2048;
+constexpr int kCdfThreads = 1024;
+
 template <typename R>
-__global__ void k_cdf_sequential(const typename Vec2<R>::T* a, uint64_t N, double thr, double* cum, uint64_t* last) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  double acc = 0.0;
-  uint64_t lk = ~uint64_t(0);
-  for (uint64_t i = 0; i < N; i++) {
-    double p = pref<R>(a, i);
-    if (p > thr) { acc += p; lk = i; }
-    cum[i] = acc;
+__global__ void __launch_bounds__(kCdfThreads) k_cdf_sequential(const typename Vec2<R>::T* a, uint64_t N, double thr,
+                                                                double* cum, uint64_t* last) {
+  __shared__ __align__(16) double buf[3][kCdfChunk];  // 48 KB, the static limit
+  const uint64_t CH = N < (uint64_t)kCdfChunk ? N : (uint64_t)kCdfChunk;
+  const uint64_t nch = N / CH;
+  const int tid = threadIdx.x;
+  const int wtid = tid - 32;  // worker index (warps 1..)
+  const int nwork = kCdfThreads - 32;
+  // chunk 0 by every thread
+  for (uint64_t i = tid; i < CH; i += kCdfThreads) {
+    const double p = pref<R>(a, i);
+    buf[0][i] = p > thr ? p : -0.0;
   }
-  *last = lk;
-  if (lk != ~uint64_t(0))
-    for (uint64_t i = lk; i < N; i++) cum[i] = 1.0;
+  double acc = 0.0;
+  long long lk = -1;
+  __syncthreads();
+  for (uint64_t c = 0; c <= nch; c++) {
+    if (tid == 0 && c < nch) {
+      double* b = buf[c % 3];
+      const long long base = (long long)(c * CH);
+      int i = 0;
+      for (; i + 8 <= (int)CH; i += 8) {
+        double v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) v[j] = b[i + j];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          acc += v[j];
+          if (__double_as_longlong(v[j]) >= 0) lk = base + i + j;
+          b[i + j] = acc;
+        }
+      }
+      for (; i < (int)CH; i++) {  // states of fewer than 8 amplitudes
+        const double v = b[i];
+        acc += v;
+        if (__double_as_longlong(v) >= 0) lk = base + i;
+        b[i] = acc;
+      }
+    } else if (tid >= 32) {
+      if (c >= 1) {  // running sums of chunk c-1 out
+        const double* b = buf[(c - 1) % 3];
+        for (int i = wtid; i < (int)CH; i += nwork) cum[(c - 1) * CH + i] = b[i];
+      }
+      if (c + 1 < nch) {  // kept probabilities of chunk c+1 in
+        double* b = buf[(c + 1) % 3];
+        const uint64_t base = (c + 1) * CH;
+        for (int i = wtid; i < (int)CH; i += nwork) {
+          const double p = pref<R>(a, base + i);
+          b[i] = p > thr ? p : -0.0;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) buf[0][0] = __longlong_as_double(lk);  // the chunks are spent: broadcast through them
+  __syncthreads();
+  const uint64_t l = (uint64_t)__double_as_longlong(buf[0][0]);
+  if (tid == 0) *last = l;
+  // the reference sets the last kept entry's cumP to 1.0; entries after it
+  // are never kept, so the search treats them alike
+  if (l != ~uint64_t(0))
+    for (uint64_t i = l + tid; i < N; i += kCdfThreads) cum[i] = 1.0;
 }
 
-__global__ void k_sample_dense(const double* cum, uint64_t N, const double* r, uint64_t shots, uint64_t last,
+__global__ void k_sample_dense(const double* cum, uint64_t N, const double* r, uint64_t shots, const uint64_t* lastp,
                                uint64_t* out) {
+  const uint64_t last = *lastp;
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < shots; s += (uint64_t)gridDim.x * blockDim.x) {
     if (last == ~uint64_t(0)) { out[s] = 0; continue; }
     double rv = r[s];
@@ -473,12 +536,8 @@ static cudaError_t sample_t(const void* amp, int n, double thr, int seq_qubits, 
   if (n <= seq_qubits || n < 10) {
     double* cum = (double*)scratch;
     uint64_t* last = (uint64_t*)(cum + N);
-    k_cdf_sequential<R><<<1, 32, 0, s>>>(a, N, thr, cum, last);
-    uint64_t lasth = 0;
-    cudaMemcpyAsync(&lasth, last, 8, cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return e;
-    k_sample_dense<<<gridn(shots, 256), 256, 0, s>>>(cum, N, r, shots, lasth, out);
+    k_cdf_sequential<R><<<1, kCdfThreads, 0, s>>>(a, N, thr, cum, last);
+    k_sample_dense<<<gridn(shots, 256), 256, 0, s>>>(cum, N, r, shots, last, out);
   } else {
     const uint64_t nchunks = N / 1024;
     double* cs = (double*)scratch;

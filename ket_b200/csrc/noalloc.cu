@@ -16,6 +16,11 @@
 // call's partial sums in it.  Calls whose kernels overlap on the GPU (two
 // streams, or two threads without ordering between them) race on the array
 // and produce wrong results; order them on one stream.
+//
+// The array's address is looked up once per device and kept for the life of
+// the process.  cudaDeviceReset unloads the library's device code, so this
+// entry point must not be called on a device after cudaDeviceReset has run
+// on it: the kept address would then point at freed memory.
 #include <mutex>
 
 #include "ctx.h"
@@ -52,6 +57,23 @@ int scratch_for_current_device(void** out) {
   return KET_OK;
 }
 
+// The caller's buffers must be device (or managed) memory of the current
+// device: a host pointer, or one on another device, would fault the kernel.
+// cudaPointerGetAttributes only queries; it allocates nothing.
+int check_device_pointer(const void* p, int dev, const char* what) {
+  cudaPointerAttributes at;
+  cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear the sticky query error
+    return fail(KET_ERR_TYPE, std::string(what) + " is not a device pointer");
+  }
+  if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+    return fail(KET_ERR_TYPE, std::string(what) + " is not device or managed memory");
+  if (at.type == cudaMemoryTypeDevice && at.device != dev)
+    return fail(KET_ERR_TYPE, std::string(what) + " lives on another device than the current one");
+  return KET_OK;
+}
+
 }  // namespace
 }  // namespace ket
 
@@ -68,8 +90,14 @@ extern "C" int ket_marginals_noalloc(const void* amp, int nqubits, int precision
     return fail(KET_ERR_RANGE, "marginals of this state need " + std::to_string(need) +
                                    " bytes of scratch, more than the fixed " + std::to_string(kNoallocBytes) +
                                    "-byte array of ket_marginals_noalloc");
+  int dev = -1;
+  cudaError_t ge = cudaGetDevice(&dev);
+  if (ge != cudaSuccess) return cuda_fail(ge, "cudaGetDevice");
+  int rc = check_device_pointer(amp, dev, "amp");
+  if (!rc) rc = check_device_pointer(out, dev, "out");
+  if (rc) return rc;
   void* scratch = nullptr;
-  int rc = scratch_for_current_device(&scratch);
+  rc = scratch_for_current_device(&scratch);
   if (rc) return rc;
   // every partial the reduction reads is written by this call's first kernel,
   // so the array needs no clearing

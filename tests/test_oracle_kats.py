@@ -308,3 +308,14 @@ def test_dm_noise_ordering_oracle():
     harmony = _ocirc(2, BELL).dm(0.001, 0.015).purity()
     assert forte > harmony
     assert _ocirc(2, BELL).dm(0.0003, 0.005).purity() < _ocirc(2, BELL).dm().purity()
+
+
+def test_sparse_oracle_agrees_with_dense_prune_on_the_family():
+    """DENSE_PRUNE is the reference's pruning on a dense array: on the
+    workload's family it gives the sparse map's amplitudes, so it stands in
+    for the sparse mode where a Map of 2^26 entries is too slow."""
+    from oracle import oracle as O
+    oc, _ = O.brickwork(16, 20, 42, with_qft=True)
+    a = oc.simulate(mode=O.SPARSE).dense()
+    b = oc.simulate(mode=O.DENSE_PRUNE).dense()
+    assert np.array_equal(a, b)
