@@ -101,7 +101,11 @@ typedef struct ket_exec_opts {
                           5 below 26 qubits, 4 from there on), 4 or 5 = that count at any size, so
                           that the programs large states run can be checked on small ones.  The
                           interpreter always uses 5.  No counterpart in the reference. */
-  int32_t reserved[4];
+  int32_t stage;       /* compiled kernels' tile loads: 1 = staged in shared memory by TMA copies
+                          (one CTA per SM, a copy warp keeps the next tiles in flight), -1 = loads
+                          into registers (two CTAs per SM), 0 = automatic.  Results are identical
+                          either way.  No counterpart in the reference. */
+  int32_t reserved[3];
 } ket_exec_opts;
 
 /* NoiseParams (circuit.ts:213-221): depolarizing probability per single-qubit
@@ -135,6 +139,11 @@ KET_API int ket_ctx_profile_read(ket_ctx* ctx, int* kinds, float* ms, size_t cap
  * own work or record timing events against the engine's launches.  No
  * counterpart in the reference. */
 KET_API int ket_ctx_stream(const ket_ctx* ctx, void** stream);
+/* The device's FP64 fused-multiply-add rate (FMAs per second), measured by a
+ * register-only kernel timed with CUDA events on the context's stream: the
+ * FP64 roofline denominator of shared-memory-resident work (batched circuits,
+ * small states).  No counterpart in the reference. */
+KET_API int ket_measure_fp64(ket_ctx* ctx, double* fma_per_s);
 /* Kernel launches made by the context so far. */
 KET_API int ket_ctx_launch_count(const ket_ctx* ctx, uint64_t* count);
 /* Bytes the context has copied host->device and device->host so far. */
@@ -149,6 +158,11 @@ KET_API int ket_debug_fail_alloc(int after);
  * returns KET_ERR_TIMEOUT (0 = the default, 2^24); drop_item = -1 disables.
  * No counterpart in the reference (which has no device waits). */
 KET_API int ket_debug_batch_hook(int drop_item, uint32_t spin_limit);
+/* Test hook for ket_adjoint_gradient's checkpoints: at most device_bytes of
+ * device memory go to checkpoints of psi, the rest to pinned host memory
+ * (a negative value: whatever free device memory allows, keeping 2 GiB
+ * spare -- the default).  No counterpart in the reference. */
+KET_API int ket_debug_adjoint_budget(int64_t device_bytes);
 
 /* Dense state of 2^nqubits amplitudes, resident in device memory, set to |0..0>
  * (zero(n), statevector.ts:16).  precision: KET_C128 or KET_C64. */
@@ -356,7 +370,10 @@ typedef struct ket_param_binding {
  * ops carry placeholder matrices for bound ops; H is a PauliTerm list (see
  * ket_expect_pauli_sum).  energy[b] and grad[b*nparams + k] are written.
  * checkpoint_every: 0 = automatic (about sqrt(#ops)), -1 = none; the forward state is
- * stored every that many ops and restored during the reverse sweep. */
+ * stored every that many ops and restored during the reverse sweep, in device
+ * memory while free memory holds it and in pinned host memory beyond that.  The
+ * vectors of a batch are queued without host waits, and a batch of 8 or more
+ * runs its passes on kernels compiled for their programs. */
 KET_API int ket_adjoint_gradient(ket_ctx* ctx, int nqubits, uint64_t init, const ket_op* ops, size_t nops,
                          const double* mats, size_t nmat, const ket_param_binding* binds, size_t nbinds,
                          const double* params, int nparams, int batch, int nterms, const double* coeffs,
@@ -387,6 +404,32 @@ KET_API int ket_shift_gradient(ket_ctx* ctx, int nqubits, uint64_t init, const k
 KET_API int ket_batch_config(ket_ctx* ctx, int block_threads, int tile_bits);
 KET_API int ket_batch_qaoa(ket_ctx* ctx, int ninst, const int* n, const int* ne, const int64_t* eoff, const int* edges,
                    int p, const double* gamma, const double* beta, int use_graph, double* out);
+
+/* A circuit template of ket_batch_vqe: ops[op_first .. op_first + nops) on
+ * nqubits qubits (1..13), its parametric ops bound by binds[bind_first ..
+ * bind_first + nbinds) (op indices relative to op_first, placeholder matrices
+ * in the op list as for ket_adjoint_gradient), and its Hamiltonian: nterms
+ * PauliTerms with coefficients coeffs[term_first ..] and strings of nqubits
+ * characters each at pauli[pauli_first ..] (ops[0] acts on qubit n-1). */
+typedef struct ket_batch_template {
+  int32_t nqubits, nops, nbinds, nterms;
+  int64_t op_first, bind_first, term_first, pauli_first;
+} ket_batch_template;
+
+/* vqe() (algorithms.ts:301-336) over a batch of parameterised circuits: instance
+ * i runs template inst_template[i] at parameters theta[i*nparams ..] from
+ * |0...0> with the reference's per-gate pruning and returns
+ * energy[i] = sum_t coeff_t <psi_i|P_t|psi_i>, as a parameter sweep of
+ * vqe(ansatz(params), H) would, one call per instance.  Templates may differ in
+ * qubit count, gates and Hamiltonian.  All instances run in one persistent
+ * launch (one CTA per instance with its state in shared memory, widest first);
+ * with use_graph = 1 the launch is captured in a CUDA graph that later calls of
+ * the same shape replay.  Ops: single, controlled, two, unitary of 1-2 qubits,
+ * cnot, swap, toffoli, cswap, csrswap, barrier. */
+KET_API int ket_batch_vqe(ket_ctx* ctx, int ntemplates, const ket_batch_template* templates, const ket_op* ops,
+                          const double* mats, size_t nmat, const ket_param_binding* binds, const double* coeffs,
+                          const char* pauli, int ninst, const int* inst_template, const double* theta, int nparams,
+                          int use_graph, double* energy);
 
 #ifdef __cplusplus
 }

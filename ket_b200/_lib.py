@@ -49,7 +49,13 @@ class ket_noise(C.Structure):
 
 class ket_exec_opts(C.Structure):
     _fields_ = [("fusion", C.c_int32), ("prune", C.c_int32), ("specialize", C.c_int32), ("reg_bits", C.c_int32),
-                ("reserved", C.c_int32 * 4)]
+                ("stage", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+
+class ket_batch_template(C.Structure):
+    _fields_ = [("nqubits", C.c_int32), ("nops", C.c_int32), ("nbinds", C.c_int32), ("nterms", C.c_int32),
+                ("op_first", C.c_int64), ("bind_first", C.c_int64), ("term_first", C.c_int64),
+                ("pauli_first", C.c_int64)]
 
 
 class ket_param_binding(C.Structure):
@@ -79,6 +85,7 @@ def lib():
             "ket_exec_opts_default": (None, [P(ket_exec_opts)]),
             "ket_debug_fail_alloc": (i32, [i32]),
             "ket_debug_batch_hook": (i32, [i32, C.c_uint32]),
+            "ket_debug_adjoint_budget": (i32, [C.c_int64]),
             "ket_batch_config": (i32, [vp, i32, i32]),
             "ket_ctx_create": (i32, [i32, P(vp)]),
             "ket_ctx_destroy": (i32, [vp]),
@@ -86,6 +93,7 @@ def lib():
             "ket_ctx_profile": (i32, [vp, i32]),
             "ket_ctx_profile_read": (i32, [vp, P(i32), P(C.c_float), sz, P(sz)]),
             "ket_ctx_launch_count": (i32, [vp, P(u64)]),
+            "ket_measure_fp64": (i32, [vp, P(dbl)]),
             "ket_ctx_stream": (i32, [vp, P(vp)]),
             "ket_marginals_noalloc": (i32, [vp, i32, i32, vp, vp]),
             "ket_state_compare": (i32, [vp, vp, P(dbl), P(dbl)]),
@@ -132,6 +140,8 @@ def lib():
                                            P(dbl), i32, i32, i32, P(dbl), C.c_char_p, i32, P(dbl), P(dbl)]),
             "ket_shift_gradient": (i32, [vp, i32, u64, P(ket_op), sz, P(dbl), sz, P(ket_param_binding), sz,
                                          P(dbl), i32, i32, i32, P(dbl), C.c_char_p, i32, P(dbl), P(dbl)]),
+            "ket_batch_vqe": (i32, [vp, i32, P(ket_batch_template), P(ket_op), P(dbl), sz, P(ket_param_binding),
+                                    P(dbl), C.c_char_p, i32, P(i32), P(dbl), i32, i32, P(dbl)]),
             "ket_batch_qaoa": (i32, [vp, i32, P(i32), P(i32), P(C.c_int64), P(i32), i32, P(dbl), P(dbl), i32,
                                      P(dbl)]),
         }
@@ -181,11 +191,13 @@ def jit_stats() -> dict:
     return {"kernels": out[0], "compiled": out[1], "failed": out[2], "launches": out[3], "compile_s": cs.value}
 
 
-def exec_opts(fusion: int = -1, prune: bool = True, specialize: int = 0, reg_bits: int = 0) -> ket_exec_opts:
+def exec_opts(fusion: int = -1, prune: bool = True, specialize: int = 0, reg_bits: int = 0,
+              stage: int = 0) -> ket_exec_opts:
     o = ket_exec_opts()
     lib().ket_exec_opts_default(C.byref(o))
     o.fusion = fusion
     o.prune = 1 if prune else 0
     o.specialize = specialize
     o.reg_bits = reg_bits
+    o.stage = stage
     return o

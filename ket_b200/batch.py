@@ -1,5 +1,6 @@
-"""Batched QAOA MaxCut: thousands of instances of uneven width in one
-persistent GPU launch (ket_batch_qaoa), replayed from a CUDA graph.
+"""Batched circuits in one persistent GPU launch, replayed from a CUDA graph:
+QAOA MaxCut instances of uneven width (ket_batch_qaoa) and vqe() energies of
+parameterised circuits of uneven width (ket_batch_vqe).
 
 Instance i is (n, edges, gamma[p], beta[p]); the circuit is H on every qubit,
 then per layer exp(-i gamma Z_u Z_v) on every edge and Rx(2 beta) on every
@@ -14,7 +15,7 @@ from typing import Sequence, Tuple
 
 import numpy as np
 
-from ._lib import check, default_ctx, lib
+from ._lib import RangeError, check, default_ctx, ket_batch_template, ket_param_binding, lib
 
 
 def batch_qaoa(instances: Sequence[Tuple[int, Sequence[Tuple[int, int]], Sequence[float], Sequence[float]]],
@@ -56,4 +57,66 @@ def _run(instances, use_graph: bool) -> np.ndarray:
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
     check(lib().ket_batch_qaoa(default_ctx(), N, ip(n_a), ip(ne_a), eo_a.ctypes.data_as(C.POINTER(C.c_int64)),
                                ip(ed_a), p, dp(g_a), dp(b_a), 1 if use_graph else 0, dp(out)))
+    return out
+
+
+def batch_vqe(templates, instances, use_graph: bool = True) -> np.ndarray:
+    """vqe() energies of many parameterised circuits in one launch.
+
+    templates: [(ansatz, hamiltonian)], an ansatz being a function params ->
+    Circuit (AnsatzFn or any callable) on at most 13 qubits and a hamiltonian
+    a PauliTerm list, as vqe(ansatz(params), hamiltonian) takes them
+    (algorithms.ts:301-336).  instances: [(template index, params)].  Returns
+    energy[i] = vqe(ansatz_t(params_i), H_t) for every instance, computed with
+    the reference's per-gate pruning; instances of different templates may
+    differ in width, gates and Hamiltonian."""
+    from .adjoint import trace, _terms
+    from .circuit import ops_to_abi
+    if not instances:
+        return np.zeros(0)
+    nparams = max(len(p) for _, p in instances)
+    first = {}
+    for t, p in instances:
+        if not 0 <= t < len(templates):
+            raise RangeError(f"instance template index {t} out of range")
+        first.setdefault(t, p)
+    tmpl = (ket_batch_template * max(1, len(templates)))()
+    all_ops, all_mats, all_binds, coeffs, pauli = [], [], [], [], []
+    for j, (ansatz, ham) in enumerate(templates):
+        p0 = first.get(j)
+        if p0 is None:
+            p0 = [0.3] * getattr(ansatz, "paramCount", nparams)
+        n, ops, binds = trace(ansatz, [float(v) for v in p0])
+        arr, m, k = ops_to_abi(ops)
+        terms = _terms(ham, n)
+        moff = len(all_mats)
+        tmpl[j].nqubits, tmpl[j].nops, tmpl[j].nbinds, tmpl[j].nterms = n, k, len(binds), len(terms)
+        tmpl[j].op_first, tmpl[j].bind_first = len(all_ops), len(all_binds)
+        tmpl[j].term_first, tmpl[j].pauli_first = len(coeffs), sum(len(x) for x in pauli)
+        for i in range(k):
+            if arr[i].mat >= 0:
+                arr[i].mat += moff
+            all_ops.append(arr[i])
+        all_mats.extend(m.tolist())
+        all_binds.extend(binds)
+        for c, o in terms:
+            coeffs.append(c)
+            pauli.append(o)
+    ops_a = (type(all_ops[0]) * max(1, len(all_ops)))(*all_ops) if all_ops else None
+    mats = np.ascontiguousarray(np.asarray(all_mats or [0j], dtype=np.complex128)).view(np.float64)
+    barr = (ket_param_binding * max(1, len(all_binds)))()
+    for i, (op, gate, prm, scale, shift) in enumerate(all_binds):
+        barr[i].op, barr[i].gate, barr[i].param, barr[i].scale, barr[i].shift = op, gate, prm, scale, shift
+    cf = np.ascontiguousarray(coeffs or [0.0], dtype=np.float64)
+    ps = "".join(pauli).encode()
+    it = np.ascontiguousarray([t for t, _ in instances], dtype=np.int32)
+    th = np.zeros((len(instances), max(nparams, 1)))
+    for i, (_, p) in enumerate(instances):
+        th[i, : len(p)] = p
+    th = np.ascontiguousarray(th.reshape(-1))
+    out = np.zeros(len(instances))
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    check(lib().ket_batch_vqe(default_ctx(), len(templates), tmpl, ops_a, dp(mats), mats.size // 2, barr, dp(cf), ps,
+                              len(instances), it.ctypes.data_as(C.POINTER(C.c_int)), dp(th), max(nparams, 1),
+                              1 if use_graph else 0, dp(out)))
     return out

@@ -917,12 +917,15 @@ class DeviceState:
         o = exec_opts(fusion, prune, specialize)
         check(lib().ket_apply_ops(self.h, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, C.byref(o)))
 
-    def apply_abi(self, arr, m, k, fusion: int = -1, prune: bool = True, specialize: int = 0, reg_bits: int = 0):
+    def apply_abi(self, arr, m, k, fusion: int = -1, prune: bool = True, specialize: int = 0, reg_bits: int = 0,
+                  stage: int = 0):
         """specialize: 0 automatic, 1 run-time compiled pass kernels (compiled
         first where missing), -1 the interpreter only.  reg_bits: register
-        bits of the compiled kernels' programs (0 automatic, 4 or 5)."""
+        bits of the compiled kernels' programs (0 automatic, 4 or 5).  stage:
+        the compiled kernels' tile loads (1 TMA-staged, -1 into registers, 0
+        automatic)."""
         mv = np.ascontiguousarray(m).view(np.float64)
-        o = exec_opts(fusion, prune, specialize, reg_bits)
+        o = exec_opts(fusion, prune, specialize, reg_bits, stage)
         check(lib().ket_apply_ops(self.h, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, C.byref(o)))
 
     def amplitudes_dense(self) -> np.ndarray:

@@ -191,16 +191,19 @@ void daggerize(const ket_op& op, const double* mats, std::vector<double>& out_ma
 
 }  // namespace
 
-int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o);
-
 // Reverse-sweep runner: like run_plan, with gradient probes reduced per pass
 // into slot_out (device, indexed by the probes' global slot).
-static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpart, size_t gpart_cap) {
+// Nothing waits: the probe partials (gpart) and the op images are reused by
+// later passes in stream order, and the caller reads the status word once at
+// the end.
+static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpart, size_t gpart_cap,
+                         int specialize) {
   ket_ctx* c = s->ctx;
   const size_t np = plan.passes.size();
   ket_exec_opts o;
   ket_exec_opts_default(&o);
   o.prune = 0;
+  o.specialize = specialize;
   // Passes without probes use the ordinary runner, one at a time.
   for (size_t i = 0; i < np; i++) {
     const Pass& p = plan.passes[i];
@@ -212,7 +215,7 @@ static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpa
     one.anc = plan.anc;
     one.passes.push_back(p);
     if (nprobe == 0) {
-      int rc = run_plan(s, one, o);
+      int rc = run_plan(s, one, o, false);
       if (rc) return rc;
       continue;
     }
@@ -258,10 +261,7 @@ static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpa
     if (e != cudaSuccess) return cuda_fail(e, "adjoint pass launch");
     e = launch_grad_reduce(gpart, nctas, nprobe, slot_out + slot_lo, c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint reduce launch");
-    rc = ctx_wait(c);  // gpart and the op image are reused by the next pass
-    if (rc) return rc;
-    rc = check_status(c);
-    if (rc) return rc;
+    c->launches += 1;
   }
   return KET_OK;
 }
@@ -316,16 +316,27 @@ int lower_one(int n, const ket_op& op, const double* mats, size_t nmat, std::vec
   return KET_OK;
 }
 
+// A checkpoint of psi: device memory while the budget allows, pinned host
+// memory beyond it.
+struct Ckpt {
+  void* p = nullptr;
+  bool host = false;
+};
+
 struct AdjWork {
   ket_state full;   // 2^(n+1): psi | lambda
   ket_state psi;    // view of the first half
-  std::vector<void*> ckpt;
-  double* slot_out = nullptr;
+  std::vector<Ckpt> ckpt;
+  double* slot_out = nullptr;  // [batch][nbinds] probe sums
   double* gpart = nullptr;
   size_t gpart_cap = 0;
   DevTerm* terms = nullptr;
-  double* epart = nullptr;
+  double* epart = nullptr;     // Hpsi partials, then [batch] energies
 };
+
+// Device bytes the adjoint may spend on checkpoints (ket_debug_adjoint_budget);
+// negative = whatever free memory allows, keeping 2 GiB spare.
+int64_t g_ckpt_device_budget = -1;
 
 }  // namespace
 
@@ -376,44 +387,83 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
   w.psi.ctx = ctx; w.psi.n = n; w.psi.precision = KET_C128; w.psi.amp = buf; w.psi.bytes = half;
   auto cleanup = [&]() {
     ctx_wait(ctx);
-    for (void* p : w.ckpt) cudaFree(p);
+    for (const Ckpt& k : w.ckpt) {
+      if (k.host) cudaFreeHost(k.p);
+      else cudaFree(k.p);
+    }
     if (w.slot_out) cudaFree(w.slot_out);
     if (w.gpart) cudaFree(w.gpart);
     if (w.terms) cudaFree(w.terms);
     if (w.epart) cudaFree(w.epart);
     cudaFree(buf);
   };
-  // checkpoints that fit in free memory (keep 2 GiB spare), else fewer restores
+  // Checkpoints for segments 1..nseg-1: in device memory while it holds
+  // them (2 GiB spare, or the debug budget), then in pinned host memory, so a
+  // state too large to keep more than one device copy still restores psi at
+  // every segment boundary.
   {
     size_t freeb = 0, totb = 0;
     cudaMemGetInfo(&freeb, &totb);
-    size_t spare = size_t(2) << 30;
+    const size_t spare = size_t(2) << 30;
+    size_t dev_room = freeb > spare ? freeb - spare : 0;
+    if (g_ckpt_device_budget >= 0) dev_room = std::min(dev_room, (size_t)g_ckpt_device_budget);
     for (int sgi = 1; sgi < nseg; sgi++) {
-      if (freeb < spare + half) break;
-      void* p = nullptr;
-      if (dev_alloc(&p, half)) { g_err.clear(); break; }
-      w.ckpt.push_back(p);
-      freeb -= half;
+      Ckpt k;
+      if (dev_room >= half) {
+        if (dev_alloc(&k.p, half) == KET_OK) {
+          dev_room -= half;
+          w.ckpt.push_back(k);
+          continue;
+        }
+        g_err.clear();
+        dev_room = 0;
+      }
+      if (cudaHostAlloc(&k.p, half, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        break;  // no room anywhere: later segments are un-applied without a restore
+      }
+      k.host = true;
+      w.ckpt.push_back(k);
     }
   }
   const int nck = (int)w.ckpt.size();  // checkpoints for segments 1..nck
+  auto save = [&](int sg) {            // psi at the start of segment sg
+    const Ckpt& k = w.ckpt[sg - 1];
+    return cudaMemcpyAsync(k.p, buf, half, k.host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream);
+  };
+  auto restore = [&](int sg) {
+    const Ckpt& k = w.ckpt[sg - 1];
+    return cudaMemcpyAsync(buf, k.p, half, k.host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream);
+  };
   std::vector<DevTerm> dterms;
   for (const Term& t : terms) {
     zc ph = std::pow(zc(0, 1), t.ny & 3) * t.coeff;
     dterms.push_back(DevTerm{t.flip, t.zm, ph.real(), ph.imag()});
   }
   const int hblocks = 1024;
-  rc = dev_alloc((void**)&w.slot_out, sizeof(double) * std::max<size_t>(nbinds, 1));
+  const size_t nslot = std::max<size_t>(nbinds, 1);
+  rc = dev_alloc((void**)&w.slot_out, sizeof(double) * nslot * std::max(batch, 1));
   if (!rc) { w.gpart_cap = (size_t)fused2_grid(4) * 8 * 512; rc = dev_alloc((void**)&w.gpart, sizeof(double) * w.gpart_cap); }
   if (!rc) rc = dev_alloc((void**)&w.terms, sizeof(DevTerm) * std::max<size_t>(dterms.size(), 1));
-  if (!rc) rc = dev_alloc((void**)&w.epart, sizeof(double) * (hblocks + 8));
+  if (!rc) rc = dev_alloc((void**)&w.epart, sizeof(double) * (hblocks + 8 + std::max(batch, 1)));
   if (rc) { cleanup(); return rc; }
   if (!dterms.empty())
     cudaMemcpyAsync(w.terms, dterms.data(), sizeof(DevTerm) * dterms.size(), cudaMemcpyHostToDevice, ctx->stream);
+  if (batch > 0) cudaMemsetAsync(w.slot_out, 0, sizeof(double) * nslot * batch, ctx->stream);
+  // Batches run their passes on kernels compiled for each pass's program
+  // (compiled once, on the first vector, and reused by the rest); a single
+  // vector uses compiled kernels that are ready and the interpreter otherwise.
+  const int specialize = batch >= 8 ? 1 : 0;
   ket_exec_opts fo;
   ket_exec_opts_default(&fo);
   fo.prune = 0;
+  fo.specialize = specialize;
+  double* d_energy = w.epart + hblocks + 8;
+  std::vector<int> slot_bind;  // slot -> binding index (the same for every vector)
 
+  // Every vector's passes are queued without a host wait: the host plans
+  // vector b+1 while the GPU runs vector b, and the energies and probe sums
+  // stay on the device until the end.
   for (int b = 0; b < batch; b++) {
     const double* theta = params + (size_t)b * nparams;
     Bound bd;
@@ -421,37 +471,37 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
     if (rc) { cleanup(); return rc; }
     // ---- forward, segment by segment, saving checkpoints
     cudaMemsetAsync(buf, 0, 2 * half, ctx->stream);
-    double one[2] = {1.0, 0.0};
+    static const double one[2] = {1.0, 0.0};
     cudaMemcpyAsync((char*)buf + 16 * init, one, 16, cudaMemcpyHostToDevice, ctx->stream);
     for (int sg = 0; sg < nseg; sg++) {
       size_t lo = (size_t)sg * C, hi = std::min(nops, lo + C);
-      if (sg >= 1 && sg <= nck)
-        cudaMemcpyAsync(w.ckpt[sg - 1], buf, half, cudaMemcpyDeviceToDevice, ctx->stream);
+      if (sg >= 1 && sg <= nck && save(sg) != cudaSuccess) { cleanup(); return cuda_fail(cudaGetLastError(), "checkpoint save"); }
       Plan fp;
       std::string err;
       rc = lower_ops(n, ops + lo, hi - lo, bd.mats.data(), nmat, false, fp.gates, err);
       if (rc) { cleanup(); return fail(rc, err); }
       if (fp.gates.empty()) continue;
       plan_passes(n, KET_C128, -1, false, fp);
-      rc = run_plan(&w.psi, fp, fo);
+      rc = run_plan(&w.psi, fp, fo, false);
       if (rc) { cleanup(); return rc; }
     }
     // ---- lambda = H psi, energy
     prof_begin(ctx);
     k_hpsi<<<hblocks, 256, 0, ctx->stream>>>((const double2*)buf, (double2*)((char*)buf + half), uint64_t(1) << n,
                                              w.terms, (int)dterms.size(), ident, w.epart);
-    k_sum_fixed<<<1, 32, 0, ctx->stream>>>(w.epart, hblocks, w.epart + hblocks);
+    k_sum_fixed<<<1, 32, 0, ctx->stream>>>(w.epart, hblocks, d_energy + b);
     prof_end(ctx, PK_ADJOINT);
-    double e_b = 0.0;
-    cudaMemcpyAsync(&e_b, w.epart + hblocks, 8, cudaMemcpyDeviceToHost, ctx->stream);
-    ctx->d2h_bytes += 8;
+    ctx->launches += 1;
     // ---- reverse sweep
-    if (nbinds) cudaMemsetAsync(w.slot_out, 0, sizeof(double) * nbinds, ctx->stream);
-    std::vector<int> slot_bind;  // slot -> binding index
+    double* slots_b = w.slot_out + (size_t)b * nslot;
+    std::vector<int> sb;
     for (int sg = nseg - 1; sg >= 0; sg--) {
       size_t lo = (size_t)sg * C, hi = std::min(nops, lo + C);
-      if (sg + 1 <= nck && sg + 1 < nseg)  // restore psi at the end of this segment
-        cudaMemcpyAsync(buf, w.ckpt[sg], half, cudaMemcpyDeviceToDevice, ctx->stream);
+      // restore psi at the end of this segment
+      if (sg + 1 <= nck && sg + 1 < nseg && restore(sg + 1) != cudaSuccess) {
+        cleanup();
+        return cuda_fail(cudaGetLastError(), "checkpoint restore");
+      }
       Plan bp;
       bp.anc = n;
       std::vector<double> dmats;
@@ -480,8 +530,8 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
           const ket_op& op = ops[k];
           Gate pr;
           pr.src_op = (int)k;
-          pr.slot = (int)slot_bind.size();
-          slot_bind.push_back(bi);
+          pr.slot = (int)sb.size();
+          sb.push_back(bi);
           const zc* D = &bd.D[(size_t)bi * 16];
           const int d = gate_dim(pb.gate);
           bool diag = true;
@@ -511,24 +561,35 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
       if (bp.gates.empty()) continue;
       plan_passes(n + 1, KET_C128, -1, false, bp);
       // probes must stay in order within each pass: slots are consecutive per pass by construction
-      rc = run_plan_grad(&w.full, bp, w.slot_out, w.gpart, w.gpart_cap);
+      rc = run_plan_grad(&w.full, bp, slots_b, w.gpart, w.gpart_cap, specialize);
       if (rc) { cleanup(); return rc; }
     }
-    std::vector<double> slot_val(slot_bind.size());
-    if (!slot_bind.empty()) {
-      cudaMemcpyAsync(slot_val.data(), w.slot_out, 8 * slot_bind.size(), cudaMemcpyDeviceToHost, ctx->stream);
-      ctx->d2h_bytes += 8 * slot_bind.size();
-    }
-    rc = ctx_wait(ctx);
-    if (rc) { cleanup(); return rc; }
-    energy[b] = e_b;
+    if (b == 0) slot_bind = sb;
+  }
+  std::vector<double> slot_val(nslot * std::max(batch, 1)), e_all(std::max(batch, 1));
+  if (batch > 0) {
+    cudaMemcpyAsync(e_all.data(), d_energy, 8 * (size_t)batch, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(slot_val.data(), w.slot_out, 8 * nslot * batch, cudaMemcpyDeviceToHost, ctx->stream);
+    ctx->d2h_bytes += 8 * (size_t)batch * (nslot + 1);
+  }
+  rc = ctx_wait(ctx);
+  if (!rc) rc = check_status(ctx);
+  if (rc) { cleanup(); return rc; }
+  for (int b = 0; b < batch; b++) {
+    energy[b] = e_all[b];
     double* g = grad + (size_t)b * nparams;
     for (int p = 0; p < nparams; p++) g[p] = 0.0;
     // dE/dtheta = sum over bound ops of 2 Re<lambda|G^dagger dG|psi>; slots were
     // numbered in reverse op order, so add them back in forward order
-    for (size_t sl = slot_bind.size(); sl-- > 0;) g[binds[slot_bind[sl]].param] += 2.0 * slot_val[sl];
+    const double* sv = slot_val.data() + (size_t)b * nslot;
+    for (size_t sl = slot_bind.size(); sl-- > 0;) g[binds[slot_bind[sl]].param] += 2.0 * sv[sl];
   }
   cleanup();
+  return KET_OK;
+}
+
+int ket_debug_adjoint_budget(int64_t device_bytes) {
+  g_ckpt_device_budget = device_bytes;
   return KET_OK;
 }
 

@@ -178,6 +178,8 @@ int ket_ctx_destroy(ket_ctx* c) {
   if (c->scratch2) cudaFree(c->scratch2);
   if (c->d_status) cudaFree(c->d_status);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->vqe_graph_exec) cudaGraphExecDestroy(c->vqe_graph_exec);
+  if (c->vqe_work) cudaFree(c->vqe_work);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   cudaEventDestroy(c->done);
   cudaStreamDestroy(c->stream);
@@ -424,7 +426,8 @@ int ket_jit_compile(int n, int precision, const ket_op* ops, size_t nops, const 
   }
   std::vector<JitPass> jp;
   for (size_t i = 0; i < progs.size(); i++)
-    jp.push_back(JitPass{progs[i].data(), (int)progs[i].size(), n, tiled_nreg(n, o.reg_bits), lps[i].data()});
+    jp.push_back(JitPass{progs[i].data(), (int)progs[i].size(), n, tiled_nreg(n, o.reg_bits), lps[i].data(),
+                         use_staged(n, o.stage)});
   std::string clog;
   rc = jit_compile(jp, precision, kernels, clog);
   if (log && logcap) {
@@ -455,7 +458,7 @@ int ket_apply_ops(ket_state* s, const ket_op* ops, size_t nops, const double* ma
 
 namespace ket {
 
-int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
+int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait) {
   ket_ctx* c = s->ctx;
   cudaSetDevice(c->device);
   const bool prune = o.prune != 0;
@@ -489,7 +492,9 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
   if (o.specialize >= 0) {
     std::vector<JitPass> jp(np);
     for (size_t i = 0; i < np; i++)
-      if (use2[i]) jp[i] = JitPass{progs[i].data(), (int)progs[i].size(), s->n, jit_nr, p2[i].load_pos};
+      if (use2[i])
+        jp[i] = JitPass{progs[i].data(), (int)progs[i].size(), s->n, jit_nr, p2[i].load_pos,
+                        use_staged(s->n, o.stage) && plan.passes[i].L == 5};
     std::string err;
     int rc = jit_prepare(jp, s->precision, o.specialize, c->stream, jf, err);
     if (rc) return fail(rc, err);
@@ -592,6 +597,7 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o) {
     prof_end(c, kind);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   }
+  if (!wait) return KET_OK;
   int rc = ctx_wait(c);
   if (rc) return rc;
   return check_status(c);

@@ -19,8 +19,12 @@ struct ket_ctx {
   size_t scratch_bytes = 0;
   void* scratch2 = nullptr;      // second pool (adjoint states, batch workspace)
   size_t scratch2_bytes = 0;
-  cudaGraphExec_t graph_exec = nullptr;  // last captured batch launch
+  cudaGraphExec_t graph_exec = nullptr;  // last captured batch launch (ket_batch_qaoa)
   uint64_t graph_key = 0;
+  void* vqe_work = nullptr;              // ket_batch_vqe: its device workspace
+  size_t vqe_work_bytes = 0;
+  cudaGraphExec_t vqe_graph_exec = nullptr;  // ket_batch_vqe: last captured launch
+  uint64_t vqe_graph_key = 0;
   // launch accounting and optional per-launch CUDA-event timing
   int* d_status = nullptr;        // device status word written by kernels (bounded waits)
   uint64_t launches = 0;
@@ -49,7 +53,11 @@ int cuda_fail(cudaError_t e, const char* where);
 int dev_alloc(void** p, size_t bytes);
 int ctx_scratch(ket_ctx* ctx, size_t bytes, void** out);
 int ctx_wait(ket_ctx* ctx);
-int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o);
+// Run a plan's passes on the state's stream.  wait = false returns once the
+// launches are queued (the caller waits and reads the status word later);
+// every buffer the passes read is stream-ordered, so queued plans may follow
+// one another.
+int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait = true);
 int check_status(ket_ctx* c);
 // ket_sample with the sequential CDF up to seq_qubits qubits (see read.h).
 int sample_indices(const ket_state* s, const double* r, size_t shots, double thr, int seq_qubits, uint64_t* out);

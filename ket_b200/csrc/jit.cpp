@@ -23,6 +23,7 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -144,16 +145,19 @@ struct Driver {
                      void**, void**);
   CUresult (*global)(CUdeviceptr*, size_t*, CUmodule, const char*);
   CUresult (*copy2d)(const CUDA_MEMCPY2D*, CUstream);
+  CUresult (*encode)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                     const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                     CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 };
 
 Driver& driver() {
   static Driver d = [] {
     Driver r;
-    void* p[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    const char* names[6] = {"cuModuleLoadData", "cuModuleGetFunction", "cuFuncSetAttribute", "cuLaunchKernel",
-                            "cuModuleGetGlobal", "cuMemcpy2DAsync"};
+    void* p[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    const char* names[7] = {"cuModuleLoadData", "cuModuleGetFunction", "cuFuncSetAttribute", "cuLaunchKernel",
+                            "cuModuleGetGlobal", "cuMemcpy2DAsync", "cuTensorMapEncodeTiled"};
     bool ok = true;
-    for (int i = 0; i < 6; i++) {
+    for (int i = 0; i < 7; i++) {
       cudaDriverEntryPointQueryResult q;
       if (cudaGetDriverEntryPoint(names[i], &p[i], cudaEnableDefault, &q) != cudaSuccess ||
           q != cudaDriverEntryPointSuccess || !p[i])
@@ -165,6 +169,7 @@ Driver& driver() {
     r.launch = (decltype(r.launch))p[3];
     r.global = (decltype(r.global))p[4];
     r.copy2d = (decltype(r.copy2d))p[5];
+    r.encode = (decltype(r.encode))p[6];
     r.ok = ok;
     return r;
   }();
@@ -180,18 +185,33 @@ int static_lane(const FOp& f) {
   return (f.opc >= OC_MAT1L && f.opc < OC_MAT1L + 3) || f.opc == OC_X1L || f.opc == OC_DIAGT ? f.a : 0;
 }
 
-std::string make_source(const FOp* prog, int nops, int precision, int NR) {
+// Stages of the staged form: 3 tiles of 64 KB (complex128) or 6 of 32 KB.
+int stage_count(int precision) { return precision == KET_C64 ? 6 : 3; }
+
+std::string make_source(const FOp* prog, int nops, int precision, int NR, bool staged) {
   const char* R = real_name(precision);
   const int NT = 32 << (7 - NR);
   std::string s;
-  s.reserve(200 + 96 * (size_t)nops);
+  s.reserve(300 + 96 * (size_t)nops);
+  if (staged) s += "#define KET_STAGED_THREADS " + std::to_string(NT) + "\n";
   s += "#include \"jit_ops.cuh\"\n";
   s += "__constant__ ket::jit::COp c_ops[" + std::to_string(nops > 0 ? nops : 1) + "];\n";
-  s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(NT) + ", 2) ket_pass(const ket::Pass2Args a) {\n";
+  if (staged) {
+    s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(NT + 32) +
+         ", 1) ket_pass(const ket::Pass2Args a, const __grid_constant__ ket::jit::TMap tm) {\n";
+  } else {
+    s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(NT) +
+         ", 2) ket_pass(const ket::Pass2Args a) {\n";
+  }
   s += "  using namespace ket;\n";
   s += "  const FOp* g = a.ops;\n";
-  s += std::string("  jit::run_tiles<") + R + ", " + std::to_string(NR) + ">(a, [&](cpx<" + R + "> (&x)[" +
-       std::to_string(1 << NR) + "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
+  if (staged)
+    s += std::string("  jit::run_tiles_staged<") + R + ", " + std::to_string(NR) + ", " +
+         std::to_string(stage_count(precision)) + ">(a, &tm, [&](cpx<" + R + "> (&x)[" + std::to_string(1 << NR) +
+         "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
+  else
+    s += std::string("  jit::run_tiles<") + R + ", " + std::to_string(NR) + ">(a, [&](cpx<" + R + "> (&x)[" +
+         std::to_string(1 << NR) + "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
   for (int k = 0; k < nops; k++) {
     const FOp& f = prog[k];
     if (f.type == FO_CONT || f.opc == OC_NOP) continue;
@@ -206,8 +226,8 @@ std::string make_source(const FOp* prog, int nops, int precision, int NR) {
 }
 
 // The shape of a program: what selects code in make_source.
-std::string shape_key(const FOp* prog, int nops, int precision, int nreg) {
-  std::string k = std::string(precision == KET_C64 ? "f" : "d") + std::to_string(nreg);
+std::string shape_key(const FOp* prog, int nops, int precision, int nreg, bool staged) {
+  std::string k = std::string(precision == KET_C64 ? "f" : "d") + std::to_string(nreg) + (staged ? "s" : "r");
   k.reserve(8 * (size_t)nops + 1);
   for (int i = 0; i < nops; i++) {
     const FOp& f = prog[i];
@@ -228,6 +248,7 @@ std::string shape_key(const FOp* prog, int nops, int precision, int nreg) {
 // module instances.
 struct Entry {
   enum { QUEUED, BUSY, READY, FAILED } st = QUEUED;
+  bool staged = false;
   std::string src, log;
   std::vector<char> cubin;
   // (device, stream) -> the kernel loaded for it: each stream owns a module
@@ -317,7 +338,7 @@ std::vector<std::string> enqueue(Cache& C, const std::vector<JitPass>& passes, i
     const JitPass& p = passes[i];
     // the constant op array holds at most 64 KB (512 records)
     if (!p.prog || (size_t)p.nops * sizeof(jit::COp) > 60000) continue;
-    keys[i] = shape_key(p.prog, p.nops, precision, p.nreg);
+    keys[i] = shape_key(p.prog, p.nops, precision, p.nreg, p.staged);
     if (C.map.find(keys[i]) == C.map.end()) {
       // below min_qubits a ready kernel is used but none is compiled
       if (p.nqubits < min_qubits) {
@@ -331,7 +352,8 @@ std::vector<std::string> enqueue(Cache& C, const std::vector<JitPass>& passes, i
         continue;
       }
       Entry& e = C.map[keys[i]];
-      e.src = make_source(p.prog, p.nops, precision, p.nreg);
+      e.src = make_source(p.prog, p.nops, precision, p.nreg, p.staged);
+      e.staged = p.staged;
       if (const char* dir = getenv("KET_JIT_DUMP")) {  // kernel sources, for inspection
         const std::string path = std::string(dir) + "/ket_pass_" + std::to_string(C.map.size()) + ".cu";
         if (FILE* fp = fopen(path.c_str(), "w")) {
@@ -426,12 +448,13 @@ int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cud
         if (mode == 1) return err = "loading a run-time compiled pass kernel failed", KET_ERR_CUDA;
         continue;
       }
-      const int smem = (precision == KET_C64 ? 8 : 16) << KET_T2_BITS;
+      const int smem = pass_smem(precision, e.staged);
       if (D.attr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem) != CUDA_SUCCESS) {
         if (mode == 1) return err = "setting the shared memory of a pass kernel failed", KET_ERR_CUDA;
         continue;
       }
       JitFn j;
+      j.staged = e.staged;
       j.fn = (void*)fn;
       j.cops = (unsigned long long)cops;
       j.cops_bytes = cbytes;
@@ -451,6 +474,42 @@ int tiled_nreg(int nqubits, int reg_bits) {
   return nqubits >= KET_JIT_AUTO_QUBITS ? large : KET_FUSED_NREG;
 }
 
+static_assert(jit::kStageTimeout == KET_ERR_TIMEOUT && jit::kStageMisaligned == KET_ERR_CUDA,
+              "status words of the staged loop");
+static_assert(sizeof(jit::TMap) == sizeof(CUtensorMap), "tensor map size");
+
+int pass_smem(int precision, bool staged) {
+  const int tile = (precision == KET_C64 ? 8 : 16) << KET_T2_BITS;
+  return staged ? stage_count(precision) * tile + 16 * stage_count(precision) : tile;
+}
+
+namespace {
+// The staged form's tensor map over the state (see jit_ops.cuh): rank 2,
+// {64 reals of a row of 2^5 amplitudes, rows}, one row per box.
+bool encode_tile_map(const Pass2Args& a, int precision, jit::TMap& out) {
+  const bool c64 = precision == KET_C64;
+  const uint64_t asz = c64 ? 8 : 16;
+  CUtensorMap m;
+  const CUtensorMapDataType dt = c64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const cuuint32_t es[2] = {1, 1};
+  const cuuint64_t dim[2] = {64, cuuint64_t(1) << (a.n - 5)};
+  const cuuint64_t str[1] = {32 * asz};
+  const cuuint32_t box[2] = {64, 1};
+  if (driver().encode(&m, dt, 2, a.amp, dim, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  memcpy(&out, &m, sizeof(m));
+  return true;
+}
+}  // namespace
+
+bool use_staged(int n, int stage) {
+  if (n < KET_T2_BITS) return false;
+  if (stage != 0) return stage > 0;
+  static const int env = getenv("KET_STAGE") ? atoi(getenv("KET_STAGE")) : 0;
+  return env > 0;
+}
+
 cudaError_t jit_launch(const JitFn& f, const Pass2Args& in, int precision, cudaStream_t s) {
   Pass2Args a = in;
   fill_pass2_offsets(a, precision);
@@ -468,13 +527,23 @@ cudaError_t jit_launch(const JitFn& f, const Pass2Args& in, int precision, cudaS
   cp.WidthInBytes = sizeof(jit::COp);
   cp.Height = (size_t)a.nops;
   if (a.nops > 0 && driver().copy2d(&cp, (CUstream)s) != CUDA_SUCCESS) return cudaErrorLaunchFailure;
-  const int smem = (precision == KET_C64 ? 8 : 16) << KET_T2_BITS;
+  const int smem = pass_smem(precision, f.staged);
   const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
-  // two CTAs per SM at either register-bit count (__launch_bounds__(NT, 2))
-  const unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)2 * num_sms());
-  void* params[1] = {&a};
-  const CUresult r = driver().launch((CUfunction)f.fn, blocks, 1, 1, 32 << (7 - a.nreg), 1, 1, smem,
-                                     (CUstream)s, params, nullptr);
+  CUresult r;
+  if (f.staged) {
+    // one CTA per SM: the tile's threads plus the copy warp
+    jit::TMap tm;
+    if (!encode_tile_map(a, precision, tm)) return cudaErrorInvalidValue;
+    const unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)num_sms());
+    void* params[2] = {&a, &tm};
+    r = driver().launch((CUfunction)f.fn, blocks, 1, 1, (32 << (7 - a.nreg)) + 32, 1, 1, smem, (CUstream)s, params,
+                        nullptr);
+  } else {
+    // two CTAs per SM at either register-bit count (__launch_bounds__(NT, 2))
+    const unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)2 * num_sms());
+    void* params[1] = {&a};
+    r = driver().launch((CUfunction)f.fn, blocks, 1, 1, 32 << (7 - a.nreg), 1, 1, smem, (CUstream)s, params, nullptr);
+  }
   {
     std::lock_guard<std::mutex> g(cache().mu);
     cache().launches++;

@@ -24,6 +24,7 @@ struct JitPass {
   int nqubits = 0;
   int nreg = KET_FUSED_NREG;  // register bits of the program's layouts (4 or 5)
   const uint8_t* load_pos = nullptr;  // the program's load layout (role -> tile bit)
+  bool staged = false;        // tiles staged in shared memory by TMA copies (jit_ops.cuh)
 };
 
 // Register bits of the programs of compiled pass kernels for an n-qubit
@@ -38,6 +39,7 @@ struct JitPass {
 // forces that count at any size; 0 leaves the choice above.
 int tiled_nreg(int nqubits, int reg_bits = 0);
 struct JitFn {
+  bool staged = false;              // the staged form (one CTA per SM, TMA copy warp)
   void* fn = nullptr;               // CUfunction, null = run the interpreter
   unsigned long long cops = 0;      // device address of the kernel's constant op array
   size_t cops_bytes = 0;
@@ -50,6 +52,11 @@ struct JitFn {
 int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cudaStream_t stream,
                 std::vector<JitFn>& out, std::string& err);
 cudaError_t jit_launch(const JitFn& f, const Pass2Args& a, int precision, cudaStream_t s);
+// Dynamic shared memory of a pass kernel.
+int pass_smem(int precision, bool staged);
+// Whether a pass of n qubits with these options runs the staged form
+// (ket_exec_opts.stage: 1 always, -1 never, 0 automatic).
+bool use_staged(int n, int stage);
 // Wait until no compile is queued or running.
 int jit_wait_all();
 // Drop queued compiles and wait for running ones.  A host calls this before it

@@ -23,6 +23,17 @@
 namespace ket {
 namespace jit {
 
+// The barrier among the threads that hold a tile.  In the staged form
+// (KET_STAGED_THREADS defined: the tile's threads plus one copy warp) only the
+// tile's threads take part, on named barrier 1; otherwise the whole CTA.
+__device__ __forceinline__ void tile_sync() {
+#ifdef KET_STAGED_THREADS
+  asm volatile("bar.sync 1, %0;" ::"n"(KET_STAGED_THREADS) : "memory");
+#else
+  __syncthreads();
+#endif
+}
+
 template <int NS>
 __host__ __device__ constexpr uint32_t slotmask(int creg) {
   uint32_t v = 0;
@@ -92,9 +103,9 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
   const int oa = (h.x >> 8) & 0xff, ob = (int)(h2.w & 0xffu);
   const double* M = op->m;
   const uint32_t smb = t.smb;
-  __syncthreads();
+  tile_sync();
   write_tile<R, NR>(smb, sl, x);
-  __syncthreads();
+  tile_sync();
   if constexpr (OPC == OC_X1S) {
     for (uint32_t g = t.tid; g < (1u << (KET_T2_BITS - 1)); g += NT) {
       const uint32_t i0 = insert0_32(g, ob);
@@ -151,7 +162,7 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
       }
     }
   }
-  __syncthreads();
+  tile_sync();
   read_tile<R, NR>(smb, sl, x);
 }
 
@@ -165,9 +176,9 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   constexpr int NS = 1 << NR;
   constexpr double thr = 1e-14, qthr = 1e-7;
   if constexpr (OPC == OC_EXCH) {
-    __syncthreads();
+    tile_sync();
     write_tile<R, NR>(t.smb, sl, x);
-    __syncthreads();
+    tile_sync();
     sl = exch_slay_c<NR>(c, t.lane, t.warp);
     read_tile<R, NR>(t.smb, sl, x);
     return;
@@ -304,6 +315,184 @@ __device__ __forceinline__ void run_tiles(const Pass2Args& a, Body body) {
           if (j & (1 << k)) o += a.sgb[5 + NW + k];
         st_amp<R>(reinterpret_cast<V*>(p + o), x[j]);
       }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- staged tile loop
+// The same pass with every tile staged in shared memory by the tensor-memory
+// accelerator.  One CTA per SM: NT tile threads plus one copy warp whose lane
+// 0 keeps NSTAGE tiles in flight.  A tile lands in shared memory in its
+// natural order -- byte offset = tile index x amplitude size, tile bits 0-4
+// the 5 contiguous low qubits, bits 5-11 the pass's high qubits -- as 128
+// boxes of a 2-D tensor map over the state, {the 2^5 amplitudes of a row (as
+// 2 x 32 reals), rows}: box j is the row at the tile's context plus the high
+// qubits set in j.
+//
+// Per tile and stage s: the copy lane waits for `empty[s]` (the tile threads
+// released the stage), arms `full[s]` with the tile's byte count and issues
+// the boxes; the tile threads wait for `full[s]`, read the tile into
+// registers in the load layout, run the ops -- exchanges and shared-memory
+// ops use the stage itself as their buffer -- release the stage (after a
+// proxy fence, since the next copy into it comes from the async proxy) and
+// store their registers straight to the state.  Every wait is bounded in
+// time: past KET_STAGE_WAIT_NS the status word gets KET_ERR_TIMEOUT, the tile
+// threads (all together, by a barrier vote) stop, and the copy lane waits
+// for its copies in flight before the CTA exits.
+struct __align__(64) TMap {
+  unsigned long long w[16];
+};
+
+#define KET_STAGE_WAIT_NS 2000000000ull
+// Status words the staged loop writes: KET_ERR_TIMEOUT and KET_ERR_CUDA of
+// ket_sv.h (the run-time compiler sees only these headers; jit.cpp checks that
+// the values agree).
+constexpr int kStageTimeout = 5, kStageMisaligned = 4;
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for the phase of `parity` to complete; false once KET_STAGE_WAIT_NS has
+// passed without it.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try(bar, parity))
+    if (global_ns() - t0 > KET_STAGE_WAIT_NS) return false;
+  return true;
+}
+__device__ __forceinline__ void tma_load2(uint32_t dst, const TMap* m, int row, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"((unsigned long long)m), "r"(0), "r"(row), "r"(bar)
+      : "memory");
+}
+// AND of v over the NT tile threads (named barrier 1).
+template <int NT>
+__device__ __forceinline__ bool all_tile_threads(bool v) {
+  uint32_t r;
+  asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(r)
+               : "r"((uint32_t)v), "n"(NT)
+               : "memory");
+  return r != 0;
+}
+
+template <typename R, int NR, int NSTAGE, typename Body>
+__device__ __forceinline__ void run_tiles_staged(const Pass2Args& a, const TMap* tm, Body body) {
+  constexpr int NW = 7 - NR, NS = 1 << NR, NT = 32 << NW;
+  typedef typename Vec2<R>::T V;
+  constexpr uint32_t TB = (uint32_t)sizeof(V) << KET_T2_BITS;  // bytes per tile
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  const uint32_t sm0 = (uint32_t)__cvta_generic_to_shared(smraw);
+  const uint32_t full0 = sm0 + NSTAGE * TB, empty0 = full0 + 8 * NSTAGE;
+  const int tid = threadIdx.x;
+  if (sm0 & 1023u) {  // the copies need aligned stages: refuse rather than misalign
+    if (tid == 0) atomicExch(a.status, kStageMisaligned);
+    return;
+  }
+  if (tid == 0) {
+    for (int s = 0; s < NSTAGE; s++) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, NT / 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
+  if (tid >= NT) {
+    // ---- copy lane
+    if (tid != NT) return;
+    constexpr int nbox = 1 << (KET_T2_BITS - 5);  // one box per row of 2^5 amplitudes
+    constexpr uint32_t boxb = TB / (uint32_t)nbox;
+    uint32_t k = 0;
+    bool ok = true;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
+      const uint32_t s = k % NSTAGE;
+      if (k >= NSTAGE && !mbar_wait(empty0 + 8 * s, ((k / NSTAGE) - 1) & 1)) {
+        ok = false;
+        break;
+      }
+      const uint64_t ctx0 = ctx_of(a, tile);
+      mbar_expect_tx(full0 + 8 * s, TB);
+      for (int j = 0; j < nbox; j++) {
+        uint64_t idx = ctx0;
+#pragma unroll
+        for (int e = 0; e < KET_T2_BITS - 5; e++)
+          if ((j >> e) & 1) idx |= uint64_t(1) << a.hbits[e];
+        tma_load2(sm0 + s * TB + (uint32_t)j * boxb, tm, (int)(idx >> 5), full0 + 8 * s);
+      }
+    }
+    if (!ok) atomicExch(a.status, kStageTimeout);
+    // every copy in flight lands before the CTA may exit
+    for (uint32_t kk = k > NSTAGE ? k - NSTAGE : 0; kk < k; kk++)
+      if (!mbar_wait(full0 + 8 * (kk % NSTAGE), (kk / NSTAGE) & 1)) atomicExch(a.status, kStageTimeout);
+    return;
+  }
+  // ---- tile threads
+  Tile t;
+  t.tid = tid;
+  t.lane = tid & 31;
+  t.warp = tid >> 5;
+  char* const amp = reinterpret_cast<char*>(a.amp);
+  uint64_t gs = 0;
+#pragma unroll
+  for (int r = 0; r < 5; r++)
+    if ((t.lane >> r) & 1) gs += a.sgb[r];
+#pragma unroll
+  for (int r = 0; r < NW; r++)
+    if ((t.warp >> r) & 1) gs += a.sgb[5 + r];
+  // the staged tile in the load layout: role r's tile bit at byte sizeof(V) << bit
+  uint32_t nbx[KET_T2_BITS];
+#pragma unroll
+  for (int r = 0; r < KET_T2_BITS; r++) nbx[r] = (uint32_t)sizeof(V) << a.load_pos[r];
+  const SLay<NR> nat = make_slay<NR>(nbx, t.lane, t.warp);
+  cpx<R> x[NS];
+  uint32_t k = 0;
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
+    const uint32_t s = k % NSTAGE;
+    if (!all_tile_threads<NT>(mbar_wait(full0 + 8 * s, (k / NSTAGE) & 1))) {
+      if (tid == 0) atomicExch(a.status, kStageTimeout);
+      break;
+    }
+    t.ctx0 = ctx_of(a, tile);
+    t.smb = sm0 + s * TB;
+    read_tile<R, NR>(t.smb, nat, x);
+    SLay<NR> sl = make_slay<NR>(a.lbx, t.lane, t.warp);
+    body(x, sl, t);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (t.lane == 0) mbar_arrive(empty0 + 8 * s);
+    char* p = amp + t.ctx0 * sizeof(V) + gs;
+#pragma unroll
+    for (int j = 0; j < NS; j++) {
+      uint64_t o = 0;
+#pragma unroll
+      for (int q = 0; q < NR; q++)
+        if (j & (1 << q)) o += a.sgb[5 + NW + q];
+      st_amp<R>(reinterpret_cast<V*>(p + o), x[j]);
     }
   }
 }

@@ -14,6 +14,9 @@ with 42, in a fixed draw order:
   gamma = rng()*pi, beta = rng()*pi.
 * tfim_vqe: fields h_i = 0.5 + rng() for i = 0..n-1, then batch parameter
   vectors theta = rng()*2*pi.
+* vqe_batch: per template width n (ascending), fields h_i = 0.5 + rng() for
+  the TFIM; then per instance a template t = floor(rng()*T) and its
+  parameters theta = rng()*2*pi.
 * midcircuit_brickwork(n, layers): brickwork(n, layers), measure q0 into c[0],
   reset q0, then brickwork(n, layers // 2) on the same stream (run() with
   noise exercises the per-shot path on it).
@@ -167,3 +170,21 @@ def tfim_vqe(n: int = 24, layers: int = 8, batch: int = 64, seed: int = 42):
     ansatz = hea_ladder(n, layers)
     params = [[rng() * 2 * math.pi for _ in range(ansatz.paramCount)] for _ in range(batch)]
     return ansatz, tfim_hamiltonian(n, h), params
+
+
+def vqe_batch(ninst: int = 1024, sizes: Sequence[int] = (8, 9, 10, 11, 12, 13), layers: int = 4, seed: int = 42):
+    """The batched VQE workload: templates [(hea_ladder(n, layers), TFIM(n))] for
+    every n in sizes, and ninst instances (template index, parameters) drawn
+    uniformly over the templates -- a parameter sweep over circuits of uneven
+    width."""
+    rng = Xorshift32(seed)
+    templates = []
+    for n in sizes:
+        h = [0.5 + rng() for _ in range(n)]
+        templates.append((hea_ladder(n, layers), tfim_hamiltonian(n, h)))
+    inst = []
+    for _ in range(ninst):
+        t = math.floor(rng() * len(sizes))
+        pc = templates[t][0].paramCount
+        inst.append((t, [rng() * 2 * math.pi for _ in range(pc)]))
+    return templates, inst
