@@ -163,6 +163,12 @@ KET_API int ket_debug_batch_hook(int drop_item, uint32_t spin_limit);
  * (a negative value: whatever free device memory allows, keeping 2 GiB
  * spare -- the default).  No counterpart in the reference. */
 KET_API int ket_debug_adjoint_budget(int64_t device_bytes);
+/* Test hook for the bounded waits of the staged pass kernels
+ * (ket_exec_opts.stage = 1): tile >= 0 makes each such kernel's copy warp skip
+ * the copies of that tile, so the tile threads' wait for it runs out (about
+ * two seconds) and the call returns KET_ERR_TIMEOUT with the context still
+ * usable; -1 disables.  No counterpart in the reference. */
+KET_API int ket_debug_stage_drop(int64_t tile);
 
 /* Dense state of 2^nqubits amplitudes, resident in device memory, set to |0..0>
  * (zero(n), statevector.ts:16).  precision: KET_C128 or KET_C64. */

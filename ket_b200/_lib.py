@@ -86,6 +86,7 @@ def lib():
             "ket_debug_fail_alloc": (i32, [i32]),
             "ket_debug_batch_hook": (i32, [i32, C.c_uint32]),
             "ket_debug_adjoint_budget": (i32, [C.c_int64]),
+            "ket_debug_stage_drop": (i32, [C.c_int64]),
             "ket_batch_config": (i32, [vp, i32, i32]),
             "ket_ctx_create": (i32, [i32, P(vp)]),
             "ket_ctx_destroy": (i32, [vp]),

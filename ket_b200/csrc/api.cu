@@ -385,6 +385,11 @@ int ket_plan_program_stats(int n, int precision, const ket_op* ops, size_t nops,
   return KET_OK;
 }
 
+int ket_debug_stage_drop(int64_t tile) {
+  jit_debug_stage_drop(tile);
+  return KET_OK;
+}
+
 int ket_jit_wait(void) {
   const int rc = jit_wait_all();
   return rc ? fail(rc, "a run-time compile of a pass kernel failed") : KET_OK;

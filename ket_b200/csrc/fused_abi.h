@@ -155,6 +155,7 @@ struct Pass2Args {
   uint64_t lgb[KET_T2_BITS];       // byte offset in the state of each role's tile bit, load layout
   uint64_t sgb[KET_T2_BITS];       // same, store layout
   uint32_t lbx[KET_T2_BITS];       // exchange-buffer offset of each role's tile bit, load layout
+  int64_t drop_tile;               // staged form, test hook: the copy lane skips this tile (-1 = none)
 };
 
 }  // namespace ket

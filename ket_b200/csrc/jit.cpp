@@ -484,6 +484,8 @@ int pass_smem(int precision, bool staged) {
 }
 
 namespace {
+int64_t g_stage_drop = -1;  // ket_debug_stage_drop
+
 // The staged form's tensor map over the state (see jit_ops.cuh): rank 2,
 // {64 reals of a row of 2^5 amplitudes, rows}, one row per box.
 bool encode_tile_map(const Pass2Args& a, int precision, jit::TMap& out) {
@@ -502,6 +504,8 @@ bool encode_tile_map(const Pass2Args& a, int precision, jit::TMap& out) {
   return true;
 }
 }  // namespace
+
+void jit_debug_stage_drop(int64_t tile) { g_stage_drop = tile; }
 
 bool use_staged(int n, int stage) {
   if (n < KET_T2_BITS) return false;
@@ -534,6 +538,7 @@ cudaError_t jit_launch(const JitFn& f, const Pass2Args& in, int precision, cudaS
     // one CTA per SM: the tile's threads plus the copy warp
     jit::TMap tm;
     if (!encode_tile_map(a, precision, tm)) return cudaErrorInvalidValue;
+    a.drop_tile = g_stage_drop;
     const unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)num_sms());
     void* params[2] = {&a, &tm};
     r = driver().launch((CUfunction)f.fn, blocks, 1, 1, (32 << (7 - a.nreg)) + 32, 1, 1, smem, (CUstream)s, params,

@@ -57,6 +57,8 @@ int pass_smem(int precision, bool staged);
 // Whether a pass of n qubits with these options runs the staged form
 // (ket_exec_opts.stage: 1 always, -1 never, 0 automatic).
 bool use_staged(int n, int stage);
+// Test hook of the staged form's bounded waits (ket_debug_stage_drop).
+void jit_debug_stage_drop(int64_t tile);
 // Wait until no compile is queued or running.
 int jit_wait_all();
 // Drop queued compiles and wait for running ones.  A host calls this before it

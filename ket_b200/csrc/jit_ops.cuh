@@ -435,6 +435,7 @@ __device__ __forceinline__ void run_tiles_staged(const Pass2Args& a, const TMap*
         ok = false;
         break;
       }
+      if ((int64_t)tile == a.drop_tile) continue;  // test hook: the tile threads' wait for it runs out
       const uint64_t ctx0 = ctx_of(a, tile);
       mbar_expect_tx(full0 + 8 * s, TB);
       for (int j = 0; j < nbox; j++) {

@@ -6,7 +6,9 @@
 * The batched QAOA kernel waits on other CTAs with a bounded spin; the test
   hook drops one work item so that the tiles depending on it wait in vain.
   The wait gives up after a short limit, the call reports KET_ERR_TIMEOUT
-  through the context's status word, and the next call runs normally."""
+  through the context's status word, and the next call runs normally.
+* The staged pass kernels' wait for a tile's copies is bounded in time; the
+  test hook skips one tile's copies and the call reports KET_ERR_TIMEOUT."""
 import math
 
 import numpy as np
@@ -57,3 +59,33 @@ def test_batch_wait_times_out_and_recovers():
     for u, v in edges:
         cut += ((x >> u) ^ (x >> v)) & 1
     assert abs(got[0] - float(np.dot(p, cut))) < 1e-11
+
+
+def test_staged_pass_wait_times_out_and_recovers():
+    """The staged pass kernels' tile threads wait for each tile's copies with a
+    bounded wait.  The test hook makes the copy warp skip one tile, so that wait
+    runs out (about two seconds), every tile thread stops together, the copy
+    warp drains its copies in flight, and the call reports KET_ERR_TIMEOUT; the
+    next call on the same context runs normally and matches the other form."""
+    import ket_b200 as K
+    from ket_b200 import _lib
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import DeviceState, flatten_ops, ops_to_abi
+    L = _lib.lib()
+    c, _ = W.brickwork_circuit(16, 4, 3)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    st = DeviceState(16)
+    st.set_basis(0)
+    L.ket_debug_stage_drop(5)
+    try:
+        with pytest.raises(K.KetError) as ei:
+            st.apply_abi(arr, m, k, specialize=1, stage=1)
+        assert ei.value.code == _lib.KET_ERR_TIMEOUT
+    finally:
+        L.ket_debug_stage_drop(-1)
+    st.set_basis(0)
+    st.apply_abi(arr, m, k, specialize=1, stage=1)
+    a = st.amplitudes_dense()
+    st.set_basis(0)
+    st.apply_abi(arr, m, k, specialize=1, stage=-1)
+    assert np.array_equal(a, st.amplitudes_dense())
