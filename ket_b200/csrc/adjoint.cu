@@ -28,6 +28,7 @@
 #include "ctx.h"
 #include "launch.h"
 #include "read.h"
+#include "jit.h"
 
 namespace ket {
 
@@ -253,10 +254,21 @@ static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpa
     a.status = c->d_status;
     a.gpart = gpart;
     a.nslots = nprobe;
-    const int nctas = std::min<int>(fused2_grid(4), 1 << (s->n - KET_T2_BITS));
+    // the probe pass on a kernel compiled for its program where one is ready
+    // (or, with specialize = 1, after compiling it), else on the interpreter
+    JitFn jf;
+    if (specialize >= 0 && nprobe <= KET_JIT_MAX_PROBES) {
+      std::vector<JitPass> jp{JitPass{prog.data(), (int)prog.size(), s->n, 4, a.load_pos, false}};
+      std::vector<JitFn> fns;
+      std::string err;
+      rc = jit_prepare(jp, s->precision, specialize, c->stream, fns, err);
+      if (rc) return fail(rc, err);
+      jf = fns[0];
+    }
+    const int nctas = jf.fn ? (int)jit_grid(s->n) : std::min<int>(fused2_grid(4), 1 << (s->n - KET_T2_BITS));
     if ((size_t)nctas * nprobe * 8 > gpart_cap) return fail(KET_ERR_UNSUPPORTED, "too many gradient probes in a pass");
     prof_begin(c);
-    e = launch_fused2(a, s->precision, c->stream);
+    e = jf.fn ? jit_launch(jf, a, s->precision, c->stream) : launch_fused2(a, s->precision, c->stream);
     prof_end(c, PK_ADJOINT);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint pass launch");
     e = launch_grad_reduce(gpart, nctas, nprobe, slot_out + slot_lo, c->stream);
@@ -443,7 +455,10 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
   const int hblocks = 1024;
   const size_t nslot = std::max<size_t>(nbinds, 1);
   rc = dev_alloc((void**)&w.slot_out, sizeof(double) * nslot * std::max(batch, 1));
-  if (!rc) { w.gpart_cap = (size_t)fused2_grid(4) * 8 * 512; rc = dev_alloc((void**)&w.gpart, sizeof(double) * w.gpart_cap); }
+  if (!rc) {
+    w.gpart_cap = (size_t)2 * num_sms() * 8 * KET_JIT_MAX_PROBES;  // CTAs x warps x probes of one pass
+    rc = dev_alloc((void**)&w.gpart, sizeof(double) * w.gpart_cap);
+  }
   if (!rc) rc = dev_alloc((void**)&w.terms, sizeof(DevTerm) * std::max<size_t>(dterms.size(), 1));
   if (!rc) rc = dev_alloc((void**)&w.epart, sizeof(double) * (hblocks + 8 + std::max(batch, 1)));
   if (rc) { cleanup(); return rc; }

@@ -308,6 +308,44 @@ __device__ __forceinline__ uint64_t ctx_of(const Pass2Args& a, uint64_t tile) {
   return cb;
 }
 
+// ---------------------------------------------------------------- adjoint probes
+// Adjoint passes use 16 slots per thread: register bit 3 selects psi (0) / lambda (1).
+// Re<lambda| D |psi> with D 2x2 on register bit A.
+template <typename R, int A>
+__device__ __forceinline__ double grad_m(const cpx<R>* x, const R* d, uint32_t smask) {
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    if ((j >> A) & 1) continue;
+    if (!((smask >> j) & 1)) continue;
+    const int j1 = j | (1 << A);
+    cpx<R> u0 = mac2<R>(d[0], d[1], x[j], d[2], d[3], x[j1]);
+    cpx<R> u1 = mac2<R>(d[4], d[5], x[j], d[6], d[7], x[j1]);
+    acc += (double)x[j + 8].re * u0.re + (double)x[j + 8].im * u0.im + (double)x[j1 + 8].re * u1.re +
+           (double)x[j1 + 8].im * u1.im;
+  }
+  return acc;
+}
+// Re<lambda| diag(d0, d1) on register bit A |psi>; A = -1: one factor (d0) for all.
+template <typename R, int A>
+__device__ __forceinline__ double grad_d(const cpx<R>* x, R d0r, R d0i, R d1r, R d1i, uint32_t smask) {
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    if (!((smask >> j) & 1)) continue;
+    const bool one = A >= 0 && ((j >> (A < 0 ? 0 : A)) & 1);
+    cpx<R> u = cmul<R>(one ? d1r : d0r, one ? d1i : d0i, x[j]);
+    acc += (double)x[j + 8].re * u.re + (double)x[j + 8].im * u.im;
+  }
+  return acc;
+}
+
+// Warp-sum v and add it to the CTA's gradient accumulator for (slot, warp).
+__device__ __forceinline__ void grad_accum(double* sgrad, int slot, int warp, int lane, double v) {
+  v = warp_sum(v);
+  if (lane == 0) sgrad[slot * 8 + warp] += v;
+}
+
 // ---------------------------------------------------------------- phase fans
 // FO_CPHASE on register bit A for the TT tiles of a thread; tile t's context is
 // ctx0 | (t ? pairq : 0).

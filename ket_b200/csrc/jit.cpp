@@ -188,6 +188,13 @@ int static_lane(const FOp& f) {
 // Stages of the staged form: 3 tiles of 64 KB (complex128) or 6 of 32 KB.
 int stage_count(int precision) { return precision == KET_C64 ? 6 : 3; }
 
+// A program with adjoint probes: its kernel keeps per-CTA probe sums.
+bool has_probes(const FOp* prog, int nops) {
+  for (int k = 0; k < nops; k++)
+    if (prog[k].type != FO_CONT && prog[k].opc >= OC_GRADM && prog[k].opc <= OC_GRADM2) return true;
+  return false;
+}
+
 std::string make_source(const FOp* prog, int nops, int precision, int NR, bool staged) {
   const char* R = real_name(precision);
   const int NT = 32 << (7 - NR);
@@ -201,7 +208,8 @@ std::string make_source(const FOp* prog, int nops, int precision, int NR, bool s
          ", 1) ket_pass(const ket::Pass2Args a, const __grid_constant__ ket::jit::TMap tm) {\n";
   } else {
     s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(NT) +
-         ", 2) ket_pass(const ket::Pass2Args a) {\n";
+         (has_probes(prog, nops) ? ", 2) ket_probe_pass(const ket::Pass2Args a) {\n"
+                                 : ", 2) ket_pass(const ket::Pass2Args a) {\n");
   }
   s += "  using namespace ket;\n";
   s += "  const FOp* g = a.ops;\n";
@@ -210,8 +218,9 @@ std::string make_source(const FOp* prog, int nops, int precision, int NR, bool s
          std::to_string(stage_count(precision)) + ">(a, &tm, [&](cpx<" + R + "> (&x)[" + std::to_string(1 << NR) +
          "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
   else
-    s += std::string("  jit::run_tiles<") + R + ", " + std::to_string(NR) + ">(a, [&](cpx<" + R + "> (&x)[" +
-         std::to_string(1 << NR) + "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
+    s += std::string("  jit::run_tiles<") + R + ", " + std::to_string(NR) +
+         (has_probes(prog, nops) ? ", true" : ", false") + ">(a, [&](cpx<" + R + "> (&x)[" + std::to_string(1 << NR) +
+         "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
   for (int k = 0; k < nops; k++) {
     const FOp& f = prog[k];
     if (f.type == FO_CONT || f.opc == OC_NOP) continue;
@@ -249,6 +258,7 @@ std::string shape_key(const FOp* prog, int nops, int precision, int nreg, bool s
 struct Entry {
   enum { QUEUED, BUSY, READY, FAILED } st = QUEUED;
   bool staged = false;
+  bool grad = false;  // adjoint probe pass (per-CTA probe sums after the exchange buffer)
   std::string src, log;
   std::vector<char> cubin;
   // (device, stream) -> the kernel loaded for it: each stream owns a module
@@ -354,6 +364,7 @@ std::vector<std::string> enqueue(Cache& C, const std::vector<JitPass>& passes, i
       Entry& e = C.map[keys[i]];
       e.src = make_source(p.prog, p.nops, precision, p.nreg, p.staged);
       e.staged = p.staged;
+      e.grad = !p.staged && has_probes(p.prog, p.nops);
       if (const char* dir = getenv("KET_JIT_DUMP")) {  // kernel sources, for inspection
         const std::string path = std::string(dir) + "/ket_pass_" + std::to_string(C.map.size()) + ".cu";
         if (FILE* fp = fopen(path.c_str(), "w")) {
@@ -443,18 +454,19 @@ int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cud
       CUfunction fn;
       CUdeviceptr cops = 0;
       size_t cbytes = 0;
-      if (D.load(&mod, e.cubin.data()) != CUDA_SUCCESS || D.get(&fn, mod, "ket_pass") != CUDA_SUCCESS ||
+      if (D.load(&mod, e.cubin.data()) != CUDA_SUCCESS || D.get(&fn, mod, e.grad ? "ket_probe_pass" : "ket_pass") != CUDA_SUCCESS ||
           D.global(&cops, &cbytes, mod, "c_ops") != CUDA_SUCCESS) {
         if (mode == 1) return err = "loading a run-time compiled pass kernel failed", KET_ERR_CUDA;
         continue;
       }
-      const int smem = pass_smem(precision, e.staged);
+      const int smem = pass_smem(precision, e.staged) + (e.grad ? 64 * KET_JIT_MAX_PROBES : 0);
       if (D.attr(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem) != CUDA_SUCCESS) {
         if (mode == 1) return err = "setting the shared memory of a pass kernel failed", KET_ERR_CUDA;
         continue;
       }
       JitFn j;
       j.staged = e.staged;
+      j.grad = e.grad;
       j.fn = (void*)fn;
       j.cops = (unsigned long long)cops;
       j.cops_bytes = cbytes;
@@ -477,6 +489,10 @@ int tiled_nreg(int nqubits, int reg_bits) {
 static_assert(jit::kStageTimeout == KET_ERR_TIMEOUT && jit::kStageMisaligned == KET_ERR_CUDA,
               "status words of the staged loop");
 static_assert(sizeof(jit::TMap) == sizeof(CUtensorMap), "tensor map size");
+
+unsigned jit_grid(int n) {
+  return (unsigned)std::min<uint64_t>(uint64_t(1) << (n - KET_T2_BITS), (uint64_t)2 * num_sms());
+}
 
 int pass_smem(int precision, bool staged) {
   const int tile = (precision == KET_C64 ? 8 : 16) << KET_T2_BITS;
@@ -544,10 +560,13 @@ cudaError_t jit_launch(const JitFn& f, const Pass2Args& in, int precision, cudaS
     r = driver().launch((CUfunction)f.fn, blocks, 1, 1, (32 << (7 - a.nreg)) + 32, 1, 1, smem, (CUstream)s, params,
                         nullptr);
   } else {
-    // two CTAs per SM at either register-bit count (__launch_bounds__(NT, 2))
-    const unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)2 * num_sms());
+    // two CTAs per SM at either register-bit count (__launch_bounds__(NT, 2));
+    // probe passes add their per-(slot, warp) sums after the exchange buffer
+    if (f.grad && (a.nslots < 1 || a.nslots > KET_JIT_MAX_PROBES)) return cudaErrorInvalidValue;
+    const unsigned blocks = jit_grid(a.n);
     void* params[1] = {&a};
-    r = driver().launch((CUfunction)f.fn, blocks, 1, 1, 32 << (7 - a.nreg), 1, 1, smem, (CUstream)s, params, nullptr);
+    r = driver().launch((CUfunction)f.fn, blocks, 1, 1, 32 << (7 - a.nreg), 1, 1, smem + (f.grad ? 64 * a.nslots : 0),
+                        (CUstream)s, params, nullptr);
   }
   {
     std::lock_guard<std::mutex> g(cache().mu);

@@ -38,8 +38,12 @@ struct JitPass {
 // rounding rather than bit for bit.  reg_bits (ket_exec_opts.reg_bits) 4 or 5
 // forces that count at any size; 0 leaves the choice above.
 int tiled_nreg(int nqubits, int reg_bits = 0);
+// Probes a compiled adjoint pass holds at most (its shared-memory sums).
+#define KET_JIT_MAX_PROBES 512
+
 struct JitFn {
   bool staged = false;              // the staged form (one CTA per SM, TMA copy warp)
+  bool grad = false;                // an adjoint probe pass
   void* fn = nullptr;               // CUfunction, null = run the interpreter
   unsigned long long cops = 0;      // device address of the kernel's constant op array
   size_t cops_bytes = 0;
@@ -52,8 +56,10 @@ struct JitFn {
 int jit_prepare(const std::vector<JitPass>& passes, int precision, int mode, cudaStream_t stream,
                 std::vector<JitFn>& out, std::string& err);
 cudaError_t jit_launch(const JitFn& f, const Pass2Args& a, int precision, cudaStream_t s);
-// Dynamic shared memory of a pass kernel.
+// Dynamic shared memory of a pass kernel (without probe sums).
 int pass_smem(int precision, bool staged);
+// CTAs of a register-load pass kernel on an n-qubit state (two per SM at most).
+unsigned jit_grid(int n);
 // Whether a pass of n qubits with these options runs the staged form
 // (ket_exec_opts.stage: 1 always, -1 never, 0 automatic).
 bool use_staged(int n, int stage);

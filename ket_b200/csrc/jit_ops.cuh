@@ -90,6 +90,7 @@ struct Tile {
   uint32_t smb;   // exchange buffer (shared-memory address)
   int tid, lane, warp;
   uint64_t ctx0;  // global index bits of the tile outside its 12 bits
+  double* sgrad;  // adjoint probe passes: the CTA's partial sums [slot][warp] in shared memory
 };
 
 // Rare ops on the shared-memory copy of the tile, as in k_fused2.
@@ -106,7 +107,37 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
   tile_sync();
   write_tile<R, NR>(smb, sl, x);
   tile_sync();
-  if constexpr (OPC == OC_X1S) {
+  if constexpr (OPC == OC_GRADM2) {
+    // Re<lambda| D |psi> with D 4x4 on tile bits a (MSB), b; the ancilla tile
+    // bit selects psi (0) / lambda (1).  Read-only: the registers keep the tile.
+    const int slot = (int16_t)(h2.z & 0xffff), anc = (int16_t)(h2.z >> 16);
+    int b3[3] = {oa, ob, anc};
+    for (int u = 1; u < 3; u++)
+      for (int v = u; v > 0 && b3[v - 1] > b3[v]; v--) {
+        const int w = b3[v];
+        b3[v] = b3[v - 1];
+        b3[v - 1] = w;
+      }
+    double acc = 0.0;
+    for (uint32_t g = t.tid; g < (1u << (KET_T2_BITS - 3)); g += NT) {
+      const uint32_t b0 = insert0_32(insert0_32(insert0_32(g, b3[0]), b3[1]), b3[2]);
+      if ((b0 & ct) != ct) continue;
+      const uint32_t idx[4] = {b0, b0 | (1u << ob), b0 | (1u << oa), b0 | (1u << oa) | (1u << ob)};
+      cpx<R> v[4];
+      for (int c = 0; c < 4; c++) lds(smb + swz<R>(idx[c]), v[c]);
+      for (int r = 0; r < 4; r++) {
+        cpx<R> s0 = mac2<R>((R)__ldg(M + 8 * r), (R)__ldg(M + 8 * r + 1), v[0], (R)__ldg(M + 8 * r + 2),
+                            (R)__ldg(M + 8 * r + 3), v[1]);
+        cpx<R> s1 = mac2<R>((R)__ldg(M + 8 * r + 4), (R)__ldg(M + 8 * r + 5), v[2], (R)__ldg(M + 8 * r + 6),
+                            (R)__ldg(M + 8 * r + 7), v[3]);
+        cpx<R> lam;
+        lds(smb + swz<R>(idx[r] | (1u << anc)), lam);
+        acc += (double)lam.re * (s0.re + s1.re) + (double)lam.im * (s0.im + s1.im);
+      }
+    }
+    grad_accum(t.sgrad, slot, t.warp, t.lane, acc);
+    return;
+  } else if constexpr (OPC == OC_X1S) {
     for (uint32_t g = t.tid; g < (1u << (KET_T2_BITS - 1)); g += NT) {
       const uint32_t i0 = insert0_32(g, ob);
       if ((i0 & ct) != ct) continue;
@@ -186,8 +217,35 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   if constexpr (CCTX) {
     if ((t.ctx0 & c.cctx) != c.cctx) return;  // uniform over the CTA
   }
-  if constexpr (OPC == OC_SWAPS || OPC == OC_MAT2S || OPC == OC_DIAG || OPC == OC_X1S) {
+  if constexpr (OPC == OC_SWAPS || OPC == OC_MAT2S || OPC == OC_DIAG || OPC == OC_X1S || OPC == OC_GRADM2) {
     smem_op<R, NR, OPC, FL>(x, sl, g, t);
+    return;
+  }
+  if constexpr ((OPC >= OC_GRADM && OPC < OC_GRADM + 4) || OPC == OC_GRADD) {
+    // adjoint probe <lambda|D|psi> over this thread's amplitudes (register bit
+    // 3 selects psi / lambda); every lane takes part in the warp sum, so
+    // threads whose thread-bit controls fail add zero
+    bool thr_ok = true;
+    if constexpr (CTHR != 0) thr_ok = ((uint32_t)t.tid & CTHR) == CTHR;
+    const uint32_t smask = thr_ok ? (slotmask<NS>(CREG) & full_mask<NS>()) : 0u;
+    double acc;
+    if constexpr (OPC == OC_GRADD) {
+      const R d0r = (R)c.m[0], d0i = (R)c.m[1], d1r = (R)c.m[2], d1i = (R)c.m[3];
+      if (c.flags & (FOF_TGT_THR | FOF_TGT_CTX)) {
+        const bool one = (c.flags & FOF_TGT_CTX) ? (t.ctx0 & c.dg0) != 0 : (bool)((t.tid >> c.a) & 1);
+        acc = grad_d<R, -1>(x, one ? d1r : d0r, one ? d1i : d0i, one ? d1r : d0r, one ? d1i : d0i, smask);
+      } else if (c.a == 0) {
+        acc = grad_d<R, 0>(x, d0r, d0i, d1r, d1i, smask);
+      } else if (c.a == 1) {
+        acc = grad_d<R, 1>(x, d0r, d0i, d1r, d1i, smask);
+      } else {
+        acc = grad_d<R, 2>(x, d0r, d0i, d1r, d1i, smask);
+      }
+    } else {
+      const R d[8] = {(R)c.m[0], (R)c.m[1], (R)c.m[2], (R)c.m[3], (R)c.m[4], (R)c.m[5], (R)c.m[6], (R)c.m[7]};
+      acc = grad_m<R, OPC - OC_GRADM>(x, d, smask);
+    }
+    grad_accum(t.sgrad, c.slot, t.warp, t.lane, acc);
     return;
   }
   if constexpr (CTHR != 0) {
@@ -255,7 +313,7 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   } else {
     // handled above (the exchange and the shared-memory ops return early)
     static_assert(OPC == OC_NOP || OPC == OC_EXCH || OPC == OC_SWAPS || OPC == OC_MAT2S || OPC == OC_DIAG ||
-                      OPC == OC_X1S,
+                      OPC == OC_X1S || (OPC >= OC_GRADM && OPC <= OC_GRADM2),
                   "op code without a compiled form");
     return;
   }
@@ -264,9 +322,12 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
 
 // The tile loop around a program: load each tile in the load layout, run the
 // ops, store it in the store layout -- the same addressing as k_fused2.
-template <typename R, int NR, typename Body>
+// GRAD: an adjoint probe pass; its probes add into per-(slot, warp) partial
+// sums in shared memory after the exchange buffer, written to a.gpart per CTA
+// at the end (k_grad_reduce adds them in a fixed order).
+template <typename R, int NR, bool GRAD = false, typename Body>
 __device__ __forceinline__ void run_tiles(const Pass2Args& a, Body body) {
-  constexpr int NW = 7 - NR, NS = 1 << NR;
+  constexpr int NW = 7 - NR, NS = 1 << NR, NT = 32 << NW;
   typedef typename Vec2<R>::T V;
   extern __shared__ __align__(128) unsigned char smraw[];
   Tile t;
@@ -274,6 +335,11 @@ __device__ __forceinline__ void run_tiles(const Pass2Args& a, Body body) {
   t.tid = threadIdx.x;
   t.lane = t.tid & 31;
   t.warp = t.tid >> 5;
+  t.sgrad = reinterpret_cast<double*>(smraw + ((size_t)sizeof(V) << KET_T2_BITS));
+  if constexpr (GRAD) {
+    for (int i = t.tid; i < a.nslots * 8; i += NT) t.sgrad[i] = 0.0;
+    __syncthreads();
+  }
   char* const amp = reinterpret_cast<char*>(a.amp);
   const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
   uint64_t gl = 0, gs = 0;
@@ -316,6 +382,10 @@ __device__ __forceinline__ void run_tiles(const Pass2Args& a, Body body) {
         st_amp<R>(reinterpret_cast<V*>(p + o), x[j]);
       }
     }
+  }
+  if constexpr (GRAD) {
+    __syncthreads();
+    for (int i = t.tid; i < a.nslots * 8; i += NT) a.gpart[(size_t)blockIdx.x * a.nslots * 8 + i] = t.sgrad[i];
   }
 }
 

@@ -228,9 +228,8 @@ __global__ void k_marginal_dist(const typename Vec2<R>::T* a, int c, MarginalSpe
 // probabilities and write chunk c-1's running sums to cum, all coalesced.  An
 // entry that is not kept is stored as -0.0: adding it leaves a non-negative
 // sum unchanged, so the chain equals the reference's conditional sum bit for
-// bit, and its sign bit tells it apart from a kept p = +0.0 (a threshold
-// below zero keeps those).  The last kept index stays on the device for the
-// sampler.
+// bit.  The loading threads note the last kept index, reduced over the
+// block at the end; it stays on the device for the sampler.
 constexpr int kCdfChunk = 2048;
 constexpr int kCdfThreads = 1024;
 
@@ -243,34 +242,35 @@ __global__ void __launch_bounds__(kCdfThreads) k_cdf_sequential(const typename V
   const int tid = threadIdx.x;
   const int wtid = tid - 32;  // worker index (warps 1..)
   const int nwork = kCdfThreads - 32;
+  // the last kept index: each thread's largest among the entries it loaded,
+  // then the block's largest
+  long long lk = -1;
   // chunk 0 by every thread
   for (uint64_t i = tid; i < CH; i += kCdfThreads) {
     const double p = pref<R>(a, i);
-    buf[0][i] = p > thr ? p : -0.0;
+    const bool keep = p > thr;
+    buf[0][i] = keep ? p : -0.0;
+    if (keep) lk = (long long)i;
   }
   double acc = 0.0;
-  long long lk = -1;
   __syncthreads();
   for (uint64_t c = 0; c <= nch; c++) {
     if (tid == 0 && c < nch) {
+      // the chain: one load, one add, one store per entry, loads 16 ahead
       double* b = buf[c % 3];
-      const long long base = (long long)(c * CH);
       int i = 0;
-      for (; i + 8 <= (int)CH; i += 8) {
-        double v[8];
+      for (; i + 16 <= (int)CH; i += 16) {
+        double v[16];
 #pragma unroll
-        for (int j = 0; j < 8; j++) v[j] = b[i + j];
+        for (int j = 0; j < 16; j++) v[j] = b[i + j];
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
+        for (int j = 0; j < 16; j++) {
           acc += v[j];
-          if (__double_as_longlong(v[j]) >= 0) lk = base + i + j;
           b[i + j] = acc;
         }
       }
-      for (; i < (int)CH; i++) {  // states of fewer than 8 amplitudes
-        const double v = b[i];
-        acc += v;
-        if (__double_as_longlong(v) >= 0) lk = base + i;
+      for (; i < (int)CH; i++) {  // states of fewer than 16 amplitudes
+        acc += b[i];
         b[i] = acc;
       }
     } else if (tid >= 32) {
@@ -283,15 +283,28 @@ __global__ void __launch_bounds__(kCdfThreads) k_cdf_sequential(const typename V
         const uint64_t base = (c + 1) * CH;
         for (int i = wtid; i < (int)CH; i += nwork) {
           const double p = pref<R>(a, base + i);
-          b[i] = p > thr ? p : -0.0;
+          const bool keep = p > thr;
+          b[i] = keep ? p : -0.0;
+          if (keep) lk = (long long)(base + i);
         }
       }
     }
     __syncthreads();
   }
-  if (tid == 0) buf[0][0] = __longlong_as_double(lk);  // the chunks are spent: broadcast through them
+  // block maximum of lk through the spent chunks
+  long long* red = reinterpret_cast<long long*>(buf[0]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lk = max(lk, __shfl_xor_sync(0xffffffffu, lk, o));
+  if ((tid & 31) == 0) red[tid >> 5] = lk;
   __syncthreads();
-  const uint64_t l = (uint64_t)__double_as_longlong(buf[0][0]);
+  if (tid < 32) {
+    long long v = red[tid];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (tid == 0) red[32] = v;
+  }
+  __syncthreads();
+  const uint64_t l = (uint64_t)red[32];
   if (tid == 0) *last = l;
   // the reference sets the last kept entry's cumP to 1.0; entries after it
   // are never kept, so the search treats them alike
