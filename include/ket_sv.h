@@ -375,7 +375,7 @@ typedef struct ket_param_binding {
  * shift (algorithms.ts:536-547), which costs 2*nparams energy evaluations.  The template
  * ops carry placeholder matrices for bound ops; H is a PauliTerm list (see
  * ket_expect_pauli_sum).  energy[b] and grad[b*nparams + k] are written.
- * checkpoint_every: 0 = automatic (about sqrt(#ops)), -1 = none; the forward state is
+ * checkpoint_every: 0 = automatic (8 sqrt(#ops)), -1 = none; the forward state is
  * stored every that many ops and restored during the reverse sweep, in device
  * memory while free memory holds it and in pinned host memory beyond that.  The
  * vectors of a batch are queued without host waits, and a batch of 8 or more

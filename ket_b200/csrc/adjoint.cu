@@ -18,7 +18,10 @@
 // default) and restored at the matching point of the reverse sweep, which
 // bounds the drift of un-applying gates in floating point.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <complex>
 #include <cstring>
 #include <map>
@@ -385,8 +388,14 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
     bind_of[binds[i].op] = (int)i;
   }
   // checkpoint spacing
+  // The reverse sweep recomputes psi by un-applying each gate (exact inverses
+  // in FP64), so checkpoints only bound the rounding drift, about 1e-16 per
+  // gate; a few suffice.  Automatic spacing: 8 sqrt(#ops) ops, i.e. about
+  // sqrt(#ops)/8 segments (3 for the 568-gate, 8-layer ansatz: one every
+  // three layers).  Each segment costs at least one pass over the state, so
+  // fewer, longer segments also mean fuller passes.
   int C = checkpoint_every;
-  if (C == 0) C = std::max(1, (int)std::lround(std::sqrt((double)std::max<size_t>(nops, 1))));
+  if (C == 0) C = std::max(1, 8 * (int)std::ceil(std::sqrt((double)std::max<size_t>(nops, 1))));
   if (C < 0) C = (int)nops + 1;
   const int nseg = std::max(1, (int)((nops + C - 1) / C));
   const size_t half = size_t(16) << n;
@@ -479,6 +488,9 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
   // Every vector's passes are queued without a host wait: the host plans
   // vector b+1 while the GPU runs vector b, and the energies and probe sums
   // stay on the device until the end.
+  // KET_ADJ_TIMING=1: host seconds spent queueing the batch and waiting for it, to stderr
+  static const bool timing = getenv("KET_ADJ_TIMING") != nullptr;
+  const auto t_start = std::chrono::steady_clock::now();
   for (int b = 0; b < batch; b++) {
     const double* theta = params + (size_t)b * nparams;
     Bound bd;
@@ -587,8 +599,15 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
     cudaMemcpyAsync(slot_val.data(), w.slot_out, 8 * nslot * batch, cudaMemcpyDeviceToHost, ctx->stream);
     ctx->d2h_bytes += 8 * (size_t)batch * (nslot + 1);
   }
+  const auto t_queued = std::chrono::steady_clock::now();
   rc = ctx_wait(ctx);
   if (!rc) rc = check_status(ctx);
+  if (timing) {
+    const auto t_done = std::chrono::steady_clock::now();
+    fprintf(stderr, "ket_adjoint_gradient: %d vectors, %d segments: queued in %.3f s, then waited %.3f s\n", batch,
+            nseg, std::chrono::duration<double>(t_queued - t_start).count(),
+            std::chrono::duration<double>(t_done - t_queued).count());
+  }
   if (rc) { cleanup(); return rc; }
   for (int b = 0; b < batch; b++) {
     energy[b] = e_all[b];

@@ -41,6 +41,7 @@ namespace {
 struct QInst {
   int n, ne, p, ntiles;     // ntiles = 2^(n - tile) for split instances, 1 otherwise
   int64_t state;            // offset (amplitudes) of the instance's state in the workspace (split only)
+  int64_t cut;              // offset (bytes) of the instance's cut values in the cut area (split only)
   int64_t edge_off;         // first edge in the edge array
   int64_t part_off;         // first <C> partial of the instance
 };
@@ -58,6 +59,7 @@ struct QArgs {
   const double* gamma;      // [inst * p + l]
   const double* beta;
   double2* work;            // split-instance states
+  uint8_t* cutw;            // split-instance cut(x) per amplitude, written by pass 0
   double* part;             // <C> partials
   unsigned int* next;       // queue head
   unsigned int* done;       // per instance: tiles finished (pass-major)
@@ -102,6 +104,7 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
   double2* tab = s + (1u << a.tile);                             // phase table (<= 65 entries)
   uint64_t* em = reinterpret_cast<uint64_t*>(tab + KQ_MAX_EDGES + 1);
   double* red = reinterpret_cast<double*>(em + KQ_MAX_EDGES);     // 32 doubles
+  uint8_t* cutb = reinterpret_cast<uint8_t*>(red + 32);           // whole instances: cut(x) per amplitude
   __shared__ int item_sh;
   const int T = a.tile;
   for (;;) {
@@ -118,13 +121,18 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
       // ---- whole instance in shared memory
       const uint32_t N = 1u << n;
       const double amp0 = 1.0 / sqrt((double)N);
-      for (uint32_t i = threadIdx.x; i < N; i += NT) s[i] = make_double2(amp0, 0.0);
+      __syncthreads();  // edge masks in
+      // cut(x) depends on x only: computed once, read by every layer and <C>
+      for (uint32_t i = threadIdx.x; i < N; i += NT) {
+        s[i] = make_double2(amp0, 0.0);
+        cutb[i] = (uint8_t)cut_of(i, em, I.ne);
+      }
       for (int l = 0; l < I.p; l++) {
         __syncthreads();
         fill_phase<NT>(tab, a.gamma[w.inst * I.p + l], I.ne);
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < N; i += NT) {
-          const double2 ph = tab[cut_of(i, em, I.ne)];
+          const double2 ph = tab[cutb[i]];
           const double2 v = s[i];
           s[i] = make_double2(fma(ph.x, v.x, -ph.y * v.y), fma(ph.x, v.y, ph.y * v.x));
         }
@@ -139,7 +147,7 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
       double acc = 0.0;
       for (uint32_t i = threadIdx.x; i < N; i += NT) {
         const double2 v = s[i];
-        acc += (v.x * v.x + v.y * v.y) * (double)cut_of(i, em, I.ne);
+        acc += (v.x * v.x + v.y * v.y) * (double)cutb[i];
       }
       acc = block_sum<NT>(acc, red);
       if (threadIdx.x == 0) a.part[I.part_off] = acc;
@@ -199,8 +207,19 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
       __syncthreads();
       fill_phase<NT>(tab, a.gamma[w.inst * I.p + layer], I.ne);
       __syncthreads();
+      // pass A tiles are contiguous: layer 0 computes cut(x) and keeps it,
+      // later layers read it back (written by other CTAs: bypass L1)
+      uint8_t* cw = a.cutw + I.cut;
       for (uint32_t i = threadIdx.x; i < TN; i += NT) {
-        const double2 ph = tab[cut_of(gidx(i), em, I.ne)];
+        const uint64_t x = gidx(i);
+        int cx;
+        if (layer == 0) {
+          cx = cut_of(x, em, I.ne);
+          cw[x] = (uint8_t)cx;
+        } else {
+          cx = __ldcg(cw + x);
+        }
+        const double2 ph = tab[cx];
         const double2 v = s[i];
         s[i] = make_double2(fma(ph.x, v.x, -ph.y * v.y), fma(ph.x, v.y, ph.y * v.x));
       }
@@ -264,7 +283,7 @@ static cudaError_t run_batch(ket_ctx* c, const QArgs& a, size_t smem, int ninst,
   static std::atomic<uint64_t> attr_set{0};
   const uint64_t bit = uint64_t(1) << (c->device & 63);
   if (!(attr_set.load() & bit)) {
-    const size_t smax = (16u << 12) + 16 * (KQ_MAX_EDGES + 1) + 8 * KQ_MAX_EDGES + 8 * 32;
+    const size_t smax = (17u << 12) + 16 * (KQ_MAX_EDGES + 1) + 8 * KQ_MAX_EDGES + 8 * 32;
     cudaError_t e = cudaFuncSetAttribute(k_batch_qaoa<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
     if (e != cudaSuccess) return e;
     attr_set.fetch_or(bit);
@@ -361,6 +380,7 @@ extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne
     const bool split = I.n > T && p > 0;
     I.ntiles = split ? (1 << (I.n - T)) : 1;
     I.state = split ? work : 0;
+    I.cut = split ? work : 0;  // the cut bytes sit at the same index offset in their own area
     if (split) work += int64_t(1) << I.n;
     I.part_off = parts;
     parts += I.ntiles;
@@ -389,7 +409,8 @@ extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne
   size_t off_out = off_part + al(8 * (size_t)parts);
   size_t off_cnt = off_out + al(8 * (size_t)ninst);
   size_t off_work = off_cnt + al(4 * ((size_t)ninst + 2));
-  size_t total = off_work + 16 * (size_t)work + 256;
+  size_t off_cut = off_work + al(16 * (size_t)work);
+  size_t total = off_cut + (size_t)work + 256;
   if (c->scratch2_bytes < total) {
     int rc = ctx_wait(c);
     if (rc) return rc;
@@ -424,9 +445,10 @@ extern "C" int ket_batch_qaoa(ket_ctx* c, int ninst, const int* n, const int* ne
   a.status = c->d_status;
   a.spin_limit = g_spin_limit;
   a.work = (double2*)(base + off_work);
+  a.cutw = (uint8_t*)(base + off_cut);
   a.nitems = (int)items.size();
   a.tile = T;
-  const size_t smem = (16u << T) + 16 * (KQ_MAX_EDGES + 1) + 8 * KQ_MAX_EDGES + 8 * 32;
+  const size_t smem = (17u << T) + 16 * (KQ_MAX_EDGES + 1) + 8 * KQ_MAX_EDGES + 8 * 32;  // state, table, masks, sums, cuts
   double* dout = (double*)(base + off_out);
   prof_begin(c);
   cudaError_t e;
