@@ -548,7 +548,7 @@ def vqe24_measure():
     from ket_b200.adjoint import adjoint_gradient, shift_gradient
     ans, H, P = W.tfim_vqe(24, 8, 64)
     P = np.array(P)
-    adjoint_gradient(ans, H, P[:2])
+    adjoint_gradient(ans, H, P[:8])  # a batch of 8 compiles the pass kernels the timed batch reuses
     with Profiled() as pf:
         t = time.perf_counter()
         e, g = adjoint_gradient(ans, H, P)
