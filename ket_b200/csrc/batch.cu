@@ -84,16 +84,78 @@ __device__ void fill_phase(double2* tab, double gamma, int ne) {
   }
 }
 
-// Rx(2 beta) on local bit q of a shared-memory array of 2^m amplitudes.
+// Shared-memory position of local amplitude i: the three low index bits are
+// XORed with bits 3-5.  For every group of rotated bits below, the eight
+// threads of a quarter warp then touch eight distinct 16-byte slots of a
+// 128-byte row (conflict-free), whichever bits the group holds.
+__device__ __forceinline__ uint32_t sw(uint32_t i) { return i ^ ((i >> 3) & 7u); }
+
+// Rx(2 beta) = [[c, -i s], [-i s, c]] on one pair, in registers.
+__device__ __forceinline__ void rx_pair(double2& a, double2& b, double cb, double sb) {
+  const double2 x = a, y = b;
+  a = make_double2(fma(cb, x.x, sb * y.y), fma(cb, x.y, -sb * y.x));
+  b = make_double2(fma(cb, y.x, sb * x.y), fma(cb, y.y, -sb * x.x));
+}
+
+// Rx(2 beta) on the K local bits g[0] < ... < g[K-1] of a shared-memory block
+// of 2^m amplitudes: each thread loads the 2^K amplitudes of a subcube into
+// registers, rotates every bit of the group there (lowest first), and stores
+// them back -- one shared-memory round trip per group instead of one per
+// bit.  Per amplitude the rotations run in the same order as bit by bit, so
+// results are the same.
+template <int NT, int K>
+__device__ void rx_group(double2* s, int m, uint32_t gp, double cb, double sb) {
+  int g[K];  // the group's bits, packed one per byte of gp (kept in registers)
+#pragma unroll
+  for (int q = 0; q < K; q++) g[q] = (int)((gp >> (8 * q)) & 0xffu);
+  const uint32_t nsub = 1u << (m - K);
+  for (uint32_t u = threadIdx.x; u < nsub; u += NT) {
+    uint32_t b = u;
+#pragma unroll
+    for (int q = 0; q < K; q++) b = insert0_32(b, g[q]);
+    double2 v[1 << K];
+#pragma unroll
+    for (int j = 0; j < (1 << K); j++) {
+      uint32_t o = b;
+#pragma unroll
+      for (int q = 0; q < K; q++)
+        if ((j >> q) & 1) o |= 1u << g[q];
+      v[j] = s[sw(o)];
+    }
+#pragma unroll
+    for (int q = 0; q < K; q++)
+#pragma unroll
+      for (int j = 0; j < (1 << K); j++)
+        if (!((j >> q) & 1)) rx_pair(v[j], v[j | (1 << q)], cb, sb);
+#pragma unroll
+    for (int j = 0; j < (1 << K); j++) {
+      uint32_t o = b;
+#pragma unroll
+      for (int q = 0; q < K; q++)
+        if ((j >> q) & 1) o |= 1u << g[q];
+      s[sw(o)] = v[j];
+    }
+  }
+}
+
+// Rx(2 beta) on every local bit set in `bits`, in ascending order, four bits
+// per shared-memory round trip.
 template <int NT>
-__device__ void rx_smem(double2* s, int m, int q, double cb, double sb) {
-  const uint32_t half = 1u << (m - 1);
-  for (uint32_t p = threadIdx.x; p < half; p += NT) {
-    uint32_t i0 = insert0_32(p, q), i1 = i0 | (1u << q);
-    double2 a = s[i0], b = s[i1];
-    // [[c, -i s], [-i s, c]]
-    s[i0] = make_double2(fma(cb, a.x, sb * b.y), fma(cb, a.y, -sb * b.x));
-    s[i1] = make_double2(fma(cb, b.x, sb * a.y), fma(cb, b.y, -sb * a.x));
+__device__ void rx_bits(double2* s, int m, uint32_t bits, double cb, double sb) {
+  while (bits) {
+    uint32_t gp = 0;
+    int k = 0;
+    while (bits && k < 4) {
+      gp |= (uint32_t)(__ffs(bits) - 1) << (8 * k++);
+      bits &= bits - 1;
+    }
+    __syncthreads();
+    switch (k) {
+      case 4: rx_group<NT, 4>(s, m, gp, cb, sb); break;
+      case 3: rx_group<NT, 3>(s, m, gp, cb, sb); break;
+      case 2: rx_group<NT, 2>(s, m, gp, cb, sb); break;
+      default: rx_group<NT, 1>(s, m, gp, cb, sb); break;
+    }
   }
 }
 
@@ -124,7 +186,7 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
       __syncthreads();  // edge masks in
       // cut(x) depends on x only: computed once, read by every layer and <C>
       for (uint32_t i = threadIdx.x; i < N; i += NT) {
-        s[i] = make_double2(amp0, 0.0);
+        s[sw(i)] = make_double2(amp0, 0.0);
         cutb[i] = (uint8_t)cut_of(i, em, I.ne);
       }
       for (int l = 0; l < I.p; l++) {
@@ -133,20 +195,17 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < N; i += NT) {
           const double2 ph = tab[cutb[i]];
-          const double2 v = s[i];
-          s[i] = make_double2(fma(ph.x, v.x, -ph.y * v.y), fma(ph.x, v.y, ph.y * v.x));
+          const double2 v = s[sw(i)];
+          s[sw(i)] = make_double2(fma(ph.x, v.x, -ph.y * v.y), fma(ph.x, v.y, ph.y * v.x));
         }
         double sb, cb;
         sincos(a.beta[w.inst * I.p + l], &sb, &cb);
-        for (int q = 0; q < n; q++) {
-          __syncthreads();
-          rx_smem<NT>(s, n, q, cb, sb);
-        }
+        rx_bits<NT>(s, n, (1u << n) - 1u, cb, sb);
       }
       __syncthreads();
       double acc = 0.0;
       for (uint32_t i = threadIdx.x; i < N; i += NT) {
-        const double2 v = s[i];
+        const double2 v = s[sw(i)];
         acc += (v.x * v.x + v.y * v.y) * (double)cutb[i];
       }
       acc = block_sum<NT>(acc, red);
@@ -197,9 +256,9 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
     const uint32_t TN = 1u << T;
     if (w.pass == 0) {
       const double amp0 = 1.0 / sqrt((double)(uint64_t(1) << n));
-      for (uint32_t i = threadIdx.x; i < TN; i += NT) s[i] = make_double2(amp0, 0.0);
+      for (uint32_t i = threadIdx.x; i < TN; i += NT) s[sw(i)] = make_double2(amp0, 0.0);
     } else {
-      for (uint32_t i = threadIdx.x; i < TN; i += NT) s[i] = __ldcg(g + gidx(i));  // written by other CTAs: bypass L1
+      for (uint32_t i = threadIdx.x; i < TN; i += NT) s[sw(i)] = __ldcg(g + gidx(i));  // written by other CTAs: bypass L1
     }
     double sb, cb;
     sincos(a.beta[w.inst * I.p + layer], &sb, &cb);
@@ -220,31 +279,25 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
           cx = __ldcg(cw + x);
         }
         const double2 ph = tab[cx];
-        const double2 v = s[i];
-        s[i] = make_double2(fma(ph.x, v.x, -ph.y * v.y), fma(ph.x, v.y, ph.y * v.x));
+        const double2 v = s[sw(i)];
+        s[sw(i)] = make_double2(fma(ph.x, v.x, -ph.y * v.y), fma(ph.x, v.y, ph.y * v.x));
       }
-      for (int q = 0; q < T; q++) {
-        __syncthreads();
-        rx_smem<NT>(s, T, q, cb, sb);
-      }
+      rx_bits<NT>(s, T, (1u << T) - 1u, cb, sb);
     } else {
-      for (int q = lowB; q < T; q++) {
-        __syncthreads();
-        rx_smem<NT>(s, T, q, cb, sb);
-      }
+      rx_bits<NT>(s, T, ((1u << T) - 1u) & ~((1u << lowB) - 1u), cb, sb);
     }
     __syncthreads();
     const bool last = w.pass == 2 * I.p - 1;
     if (last) {
       double acc = 0.0;
       for (uint32_t i = threadIdx.x; i < TN; i += NT) {
-        const double2 v = s[i];
+        const double2 v = s[sw(i)];
         acc += (v.x * v.x + v.y * v.y) * (double)cut_of(gidx(i), em, I.ne);
       }
       acc = block_sum<NT>(acc, red);
       if (threadIdx.x == 0) a.part[I.part_off + w.tile] = acc;
     } else {
-      for (uint32_t i = threadIdx.x; i < TN; i += NT) g[gidx(i)] = s[i];
+      for (uint32_t i = threadIdx.x; i < TN; i += NT) g[gidx(i)] = s[sw(i)];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
