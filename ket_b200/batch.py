@@ -11,6 +11,7 @@ terms that is vqe(qaoa(n, edges, -2*gamma, beta), maxCutHamiltonian(n, edges))
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from typing import Sequence, Tuple
 
 import numpy as np
@@ -69,9 +70,10 @@ def batch_vqe(templates, instances, use_graph: bool = True) -> np.ndarray:
     (algorithms.ts:301-336).  instances: [(template index, params)].  Returns
     energy[i] = vqe(ansatz_t(params_i), H_t) for every instance, computed with
     the reference's per-gate pruning; instances of different templates may
-    differ in width, gates and Hamiltonian."""
-    from .adjoint import trace, _terms
-    from .circuit import ops_to_abi
+    differ in width, gates and Hamiltonian.  Each ansatz is traced once and
+    kept while the ansatz object lives, so it must build the same gate list
+    on every call (as the adjoint's trace requires)."""
+    from .adjoint import _terms
     if not instances:
         return np.zeros(0)
     nparams = max(len(p) for _, p in instances)
@@ -86,8 +88,7 @@ def batch_vqe(templates, instances, use_graph: bool = True) -> np.ndarray:
         p0 = first.get(j)
         if p0 is None:
             p0 = [0.3] * getattr(ansatz, "paramCount", nparams)
-        n, ops, binds = trace(ansatz, [float(v) for v in p0])
-        arr, m, k = ops_to_abi(ops)
+        n, arr, m, k, binds = _traced(ansatz, p0)
         terms = _terms(ham, n)
         moff = len(all_mats)
         tmpl[j].nqubits, tmpl[j].nops, tmpl[j].nbinds, tmpl[j].nterms = n, k, len(binds), len(terms)
@@ -110,13 +111,45 @@ def batch_vqe(templates, instances, use_graph: bool = True) -> np.ndarray:
     cf = np.ascontiguousarray(coeffs or [0.0], dtype=np.float64)
     ps = "".join(pauli).encode()
     it = np.ascontiguousarray([t for t, _ in instances], dtype=np.int32)
-    th = np.zeros((len(instances), max(nparams, 1)))
-    for i, (_, p) in enumerate(instances):
-        th[i, : len(p)] = p
-    th = np.ascontiguousarray(th.reshape(-1))
+    if all(len(p) == nparams for _, p in instances):
+        th = np.ascontiguousarray(np.asarray([p for _, p in instances], dtype=np.float64).reshape(-1))
+    else:
+        th = np.zeros((len(instances), max(nparams, 1)))
+        for i, (_, p) in enumerate(instances):
+            th[i, : len(p)] = p
+        th = np.ascontiguousarray(th.reshape(-1))
     out = np.zeros(len(instances))
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
     check(lib().ket_batch_vqe(default_ctx(), len(templates), tmpl, ops_a, dp(mats), mats.size // 2, barr, dp(cf), ps,
                               len(instances), it.ctypes.data_as(C.POINTER(C.c_int)), dp(th), max(nparams, 1),
                               1 if use_graph else 0, dp(out)))
     return out
+
+
+# Traced templates, kept per ansatz function while it lives: a parameter sweep
+# calls batch_vqe again and again with the same ansatze, and tracing (two
+# builds of the circuit) costs more host time than the batch's kernel.
+_TRACE_CACHE = weakref.WeakKeyDictionary()
+
+
+def _traced(ansatz, p0):
+    """(n, ket_op array, matrices, count, bindings) of an ansatz, traced once."""
+    from .adjoint import trace
+    from .circuit import ops_to_abi
+    key = len(p0)
+    try:
+        hit = _TRACE_CACHE.get(ansatz, {}).get(key)
+    except TypeError:  # not weak-referenceable: trace every time
+        hit = None
+    if hit is None:
+        n, ops, binds = trace(ansatz, [float(v) for v in p0])
+        arr, m, k = ops_to_abi(ops)
+        hit = (n, arr, m, k, binds)
+        try:
+            _TRACE_CACHE.setdefault(ansatz, {})[key] = hit
+        except TypeError:
+            pass
+    n, arr, m, k, binds = hit
+    arr2 = (type(arr[0]) * max(1, k))()
+    C.memmove(arr2, arr, C.sizeof(arr2))  # the caller shifts matrix offsets in its copy
+    return n, arr2, m, k, binds

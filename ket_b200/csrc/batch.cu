@@ -138,20 +138,31 @@ __device__ void rx_group(double2* s, int m, uint32_t gp, double cb, double sb) {
   }
 }
 
-// Rx(2 beta) on every local bit set in `bits`, in ascending order, four bits
-// per shared-memory round trip.
+// Bits per group: three at 256 threads per CTA, so that the registers of three
+// resident CTAs (the shared-memory limit) hold a group's 8 amplitudes without
+// spills; four at 128 and 512 threads.
+template <int NT>
+constexpr int rx_group_bits() { return NT == 256 ? 3 : 4; }
+template <int NT>
+constexpr int batch_min_blocks() { return NT == 512 ? 1 : 3; }
+
+// Rx(2 beta) on every local bit set in `bits`, in ascending order, a group of
+// bits per shared-memory round trip.
 template <int NT>
 __device__ void rx_bits(double2* s, int m, uint32_t bits, double cb, double sb) {
+  constexpr int KM = rx_group_bits<NT>();
   while (bits) {
     uint32_t gp = 0;
     int k = 0;
-    while (bits && k < 4) {
+    while (bits && k < KM) {
       gp |= (uint32_t)(__ffs(bits) - 1) << (8 * k++);
       bits &= bits - 1;
     }
     __syncthreads();
+    if constexpr (KM == 4) {
+      if (k == 4) { rx_group<NT, 4>(s, m, gp, cb, sb); continue; }
+    }
     switch (k) {
-      case 4: rx_group<NT, 4>(s, m, gp, cb, sb); break;
       case 3: rx_group<NT, 3>(s, m, gp, cb, sb); break;
       case 2: rx_group<NT, 2>(s, m, gp, cb, sb); break;
       default: rx_group<NT, 1>(s, m, gp, cb, sb); break;
@@ -160,7 +171,7 @@ __device__ void rx_bits(double2* s, int m, uint32_t bits, double cb, double sb) 
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
+__global__ void __launch_bounds__(NT, batch_min_blocks<NT>()) k_batch_qaoa(QArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* s = reinterpret_cast<double2*>(smraw);
   double2* tab = s + (1u << a.tile);                             // phase table (<= 65 entries)
@@ -258,7 +269,17 @@ __global__ void __launch_bounds__(NT) k_batch_qaoa(QArgs a) {
       const double amp0 = 1.0 / sqrt((double)(uint64_t(1) << n));
       for (uint32_t i = threadIdx.x; i < TN; i += NT) s[sw(i)] = make_double2(amp0, 0.0);
     } else {
-      for (uint32_t i = threadIdx.x; i < TN; i += NT) s[sw(i)] = __ldcg(g + gidx(i));  // written by other CTAs: bypass L1
+      // four loads in flight per thread before any lands in shared memory
+      // (written by other CTAs: bypass L1)
+      for (uint32_t i0 = threadIdx.x; i0 < TN; i0 += 4 * NT) {
+        double2 v[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (i0 + j * NT < TN) v[j] = __ldcg(g + gidx(i0 + j * NT));
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (i0 + j * NT < TN) s[sw(i0 + j * NT)] = v[j];
+      }
     }
     double sb, cb;
     sincos(a.beta[w.inst * I.p + layer], &sb, &cb);

@@ -140,11 +140,25 @@ __device__ __forceinline__ double2 prune2(double2 v) {
   return norm2_ref(v.x, v.y) < 1e-14 ? make_double2(0.0, 0.0) : v;
 }
 
+// Shared-memory position of amplitude i: the three low index bits XORed with
+// bits 3-5, so that pairs and quads on low qubits spread over the banks.
+__device__ __forceinline__ uint32_t swz3(uint32_t i) { return i ^ ((i >> 3) & 7u); }
+
+// The matrix of op k into m: formed from the instance's parameter, or copied.
+__device__ __forceinline__ void op_matrix(const BArgs& a, const BOp& op, const double* th, double2* m) {
+  if (op.fam >= 0) {
+    param_matrix(op.fam, op.scale * th[op.param] + op.shift, m);
+  } else {
+    const int ne = op.kind == BK_M1 ? 4 : 16;
+    for (int e = 0; e < ne; e++) m[e] = a.mats[op.moff + e];
+  }
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT) k_batch_vqe(BArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* s = reinterpret_cast<double2*>(smraw);
-  __shared__ double2 gm[16];
+  __shared__ double2 gm[2][16];  // the current op's matrix and the next one's
   __shared__ double red[32];
   __shared__ int item_sh;
   const int tid = threadIdx.x;
@@ -159,18 +173,21 @@ __global__ void __launch_bounds__(NT) k_batch_vqe(BArgs a) {
     const int n = T.n;
     const uint32_t N = 1u << n;
     const double* th = a.theta + (size_t)inst * a.nparams;
-    for (uint32_t i = tid; i < N; i += NT) s[i] = make_double2(i == 0 ? 1.0 : 0.0, 0.0);
+    for (uint32_t i = tid; i < N; i += NT) s[swz3(i)] = make_double2(i == 0 ? 1.0 : 0.0, 0.0);
+    if (tid == 0 && T.nops > 0) {
+      const BOp op0 = a.ops[T.op_first];
+      if (op0.kind == BK_M1 || op0.kind == BK_M2) op_matrix(a, op0, th, gm[0]);
+    }
     for (int k = 0; k < T.nops; k++) {
       const BOp op = a.ops[T.op_first + k];
-      __syncthreads();  // the previous op is done with s and gm
-      if (op.kind == BK_M1 || op.kind == BK_M2) {
-        if (op.fam >= 0) {
-          if (tid == 0) param_matrix(op.fam, op.scale * th[op.param] + op.shift, gm);
-        } else if (tid < (op.kind == BK_M1 ? 4 : 16)) {
-          gm[tid] = a.mats[op.moff + tid];
-        }
-        __syncthreads();
+      // one barrier per op: op k-1 is done with s and with gm[(k+1)&1], and
+      // gm[k&1] (written during op k-1) is ready
+      __syncthreads();
+      if (tid == 0 && k + 1 < T.nops) {  // the next op's matrix, while this op runs
+        const BOp nx = a.ops[T.op_first + k + 1];
+        if (nx.kind == BK_M1 || nx.kind == BK_M2) op_matrix(a, nx, th, gm[(k + 1) & 1]);
       }
+      const double2* M = gm[k & 1];
       const uint32_t cm = (uint32_t)op.cmask;
       const bool pr = op.prune != 0;
       if (op.kind == BK_M1 || op.kind == BK_X) {
@@ -178,16 +195,17 @@ __global__ void __launch_bounds__(NT) k_batch_vqe(BArgs a) {
         for (uint32_t p = tid; p < N / 2; p += NT) {
           const uint32_t i0 = insert0_32(p, t), i1 = i0 | (1u << t);
           if ((i0 & cm) != cm) continue;
-          const double2 x0 = s[i0], x1 = s[i1];
+          const uint32_t a0 = swz3(i0), a1 = swz3(i1);
+          const double2 x0 = s[a0], x1 = s[a1];
           if (op.kind == BK_X) {
-            s[i0] = x1;
-            s[i1] = x0;
+            s[a0] = x1;
+            s[a1] = x0;
           } else {
-            double2 y0 = cmac(cmac(make_double2(0, 0), gm[0], x0), gm[1], x1);
-            double2 y1 = cmac(cmac(make_double2(0, 0), gm[2], x0), gm[3], x1);
+            double2 y0 = cmac(cmac(make_double2(0, 0), M[0], x0), M[1], x1);
+            double2 y1 = cmac(cmac(make_double2(0, 0), M[2], x0), M[3], x1);
             if (pr) { y0 = prune2(y0); y1 = prune2(y1); }
-            s[i0] = y0;
-            s[i1] = y1;
+            s[a0] = y0;
+            s[a1] = y1;
           }
         }
       } else {
@@ -198,17 +216,17 @@ __global__ void __launch_bounds__(NT) k_batch_vqe(BArgs a) {
           if ((b0 & cm) != cm) continue;
           const uint32_t i1 = b0 | (1u << qb), i2 = b0 | (1u << qa), i3 = i1 | i2;
           if (op.kind == BK_SWAP) {
-            const double2 t1 = s[i1];
-            s[i1] = s[i2];
-            s[i2] = t1;
+            const double2 t1 = s[swz3(i1)];
+            s[swz3(i1)] = s[swz3(i2)];
+            s[swz3(i2)] = t1;
           } else {
-            const double2 x[4] = {s[b0], s[i1], s[i2], s[i3]};
-            const uint32_t idx[4] = {b0, i1, i2, i3};
+            const uint32_t idx[4] = {swz3(b0), swz3(i1), swz3(i2), swz3(i3)};
+            const double2 x[4] = {s[idx[0]], s[idx[1]], s[idx[2]], s[idx[3]]};
 #pragma unroll
             for (int r = 0; r < 4; r++) {
               double2 y = make_double2(0, 0);
 #pragma unroll
-              for (int c = 0; c < 4; c++) y = cmac(y, gm[4 * r + c], x[c]);
+              for (int c = 0; c < 4; c++) y = cmac(y, M[4 * r + c], x[c]);
               s[idx[r]] = pr ? prune2(y) : y;
             }
           }
@@ -221,7 +239,7 @@ __global__ void __launch_bounds__(NT) k_batch_vqe(BArgs a) {
       const BTerm tm = a.terms[T.term_first + t];
       for (uint32_t y = tid; y < N; y += NT) {
         const uint32_t x = y ^ (uint32_t)tm.flip;
-        const double2 v = s[x], p = s[y];
+        const double2 v = s[swz3(x)], p = s[swz3(y)];
         const double sg = (__popc(x & (uint32_t)tm.zm) & 1) ? -1.0 : 1.0;
         const double lr = sg * (tm.cre * v.x - tm.cim * v.y), li = sg * (tm.cre * v.y + tm.cim * v.x);
         e += p.x * lr + p.y * li;
