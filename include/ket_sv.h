@@ -222,7 +222,9 @@ KET_API int ket_plan_stats(int nqubits, int precision, const ket_op* ops, size_t
  * (0 layout exchange, 1/2 2x2 on a register/lane bit, 3/4 X on a register/lane
  * bit, 5 register swap, 6 4x4, 7-10 diagonal forms, 11 merged phase fans), counts[12] / counts[13] =
  * 2x2 ops with a general / a real or Rx-like matrix, counts[14] = tiled passes,
- * counts[15] = other passes.  No counterpart in the reference. */
+ * counts[15] = other passes.  Programs use the register bits a run with these
+ * options would (opts->reg_bits, else the automatic choice for nqubits).  No
+ * counterpart in the reference. */
 KET_API int ket_plan_program_stats(int nqubits, int precision, const ket_op* ops, size_t nops, const double* mats,
                                    size_t nmat, const ket_exec_opts* opts, int64_t counts[16]);
 

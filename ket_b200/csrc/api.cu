@@ -375,7 +375,7 @@ int ket_plan_program_stats(int n, int precision, const ket_op* ops, size_t nops,
     if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) { counts[15]++; continue; }
     std::vector<FOp> prog;
     uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
-    plan_program(plan, p, precision, o.prune != 0, KET_FUSED_NREG, prog, lp, sp);
+    plan_program(plan, p, precision, o.prune != 0, tiled_nreg(n, o.reg_bits), prog, lp, sp);
     for (const FOp& f : prog) {
       if (f.type != FO_CONT) counts[f.type]++;
       if (f.type == FO_MAT1R || f.type == FO_MAT1L) counts[(f.flags & (FOF_REAL | FOF_RXFORM)) ? 13 : 12]++;
