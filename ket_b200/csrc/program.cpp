@@ -6,13 +6,10 @@
 //
 // Layout choice looks ahead: the tile bits needed soonest become register
 // and lane bits, the ones needed latest become warp bits.  The first and last
-// layouts keep lane bit l on tile bit l for l < 3: every 8 lanes then cover 8
-// contiguous amplitudes (128 bytes at complex128), so each warp's global load
-// and store touch four whole 128-byte lines, as with all five low bits on
-// lanes; lanes 3 and 4 are free for the bits the program needs.
+// layouts keep lane bit l on tile bit l (l < 5) so the global load and store
+// of each warp touch contiguous 128-byte lines.
 #include <algorithm>
 #include <cmath>
-#include <cstdlib>
 #include <cstring>
 
 #include "launch.h"
@@ -37,19 +34,8 @@ void fill_roles(Lay& l) {
   for (int r = 0; r < NB; r++) l.role[l.pos[r]] = r;
 }
 
-// Lanes pinned to the tile's lowest bits in the load and store layouts (3;
-// KET_PINNED_LANES=2..5 in the environment, for experiments).
-int pinned_lanes() {
-  static const int v = [] {
-    const char* e = getenv("KET_PINNED_LANES");
-    const int k = e ? atoi(e) : 3;
-    return k < 2 ? 2 : (k > 5 ? 5 : k);
-  }();
-  return v;
-}
-
 bool a0_compatible(const Lay& l) {
-  for (int i = 0; i < pinned_lanes(); i++)
+  for (int i = 0; i < 5; i++)
     if (l.pos[i] != i) return false;
   return true;
 }
@@ -116,10 +102,9 @@ Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision)
   std::vector<int> regs, lanes, warps;
   auto take_reg = [&](int b) { regs.push_back(b); used[b] = true; };
   if (a0) {
-    for (int b = 0; b < pinned_lanes(); b++) { lanes.push_back(b); used[b] = true; }
+    for (int b = 0; b < 5; b++) { lanes.push_back(b); used[b] = true; }
     for (int b : must) if (!used[b] && (int)regs.size() < NRg()) take_reg(b);
     for (int b : order) if (!used[b] && (int)regs.size() < NRg() && b >= 5) take_reg(b);
-    for (int b : order) if (!used[b] && (int)lanes.size() < 5) { lanes.push_back(b); used[b] = true; }
     for (int b : order) if (!used[b]) { warps.push_back(b); used[b] = true; }
   } else {
     for (int b : must) if (!used[b] && (int)regs.size() < NRg()) take_reg(b);
