@@ -220,95 +220,213 @@ __global__ void k_marginal_dist(const typename Vec2<R>::T* a, int c, MarginalSpe
 }
 
 // ------------------------------------------------------------------ sampling
-// Exact reference order (small states): the running FP64 sum over kept
-// entries in ascending index order (circuit.ts:3429-3436).  The sum itself is
-// one dependent chain of additions and stays on one thread; what surrounds it
-// is spread over the block.  The state streams through three shared-memory
-// chunks: while thread 0 sums chunk c, warps 1.. load chunk c+1 as kept
-// probabilities and write chunk c-1's running sums to cum, all coalesced.  An
-// entry that is not kept is stored as -0.0: adding it leaves a non-negative
-// sum unchanged, so the chain equals the reference's conditional sum bit for
-// bit.  The loading threads note the last kept index, reduced over the
-// block at the end; it stays on the device for the sampler.
-constexpr int kCdfChunk = 2048;
+// Exact reference order (small states): cum[i] = the running FP64 sum over
+// kept entries in ascending index order, rounded after every addition as
+// the reference's loop does (circuit.ts:3429-3436) -- computed in parallel,
+// bit for bit.
+//
+// While the running sum s stays in one binade [2^(e-1), 2^e), every value it
+// takes is a multiple of u = 2^(e-53), s = S u with S an integer in
+// [2^52, 2^53).  Adding p then rounds to the nearest multiple of u, so
+// s + p = (S + d) u with d = round(p / u) -- an increment that does not
+// depend on s, except when p / u lies exactly halfway (the tie goes to the
+// even S + d) or when S + d reaches 2^53 (the sum leaves the binade and
+// rounds on the next grid).  So a chunk of entries is an integer prefix sum
+// of the d's, done by the whole block, up to the first tie or binade
+// crossing; thread 0 takes that one entry with the FP64 addition itself, and
+// the next chunk starts after it.  Entries that are not kept add nothing.
+// Before the first kept entry the sum is +0.0.  A binade is crossed about
+// once per doubling of s, so the single-entry steps are few.
 constexpr int kCdfThreads = 1024;
+constexpr int kCdfPer = 4;                          // entries per thread per chunk
+constexpr int kCdfChunk = kCdfThreads * kCdfPer;    // 4096
+
+// Inclusive block scan of v (NT = kCdfThreads); `wsum` holds 32 partials.
+__device__ __forceinline__ long long block_scan_incl(long long v, long long* wsum) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  if (lane == 31) wsum[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    long long x = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += t;
+    }
+    wsum[lane] = x;
+  }
+  __syncthreads();
+  const long long r = v + (w > 0 ? wsum[w - 1] : 0);
+  __syncthreads();  // wsum is reused by the next scan
+  return r;
+}
+
+// Block minimum of v; every thread gets it.
+__device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v, unsigned long long* wred) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (lane == 0) wred[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    unsigned long long x = wred[lane];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = min(x, __shfl_xor_sync(0xffffffffu, x, o));
+    if (lane == 0) wred[32] = x;
+  }
+  __syncthreads();
+  const unsigned long long r = wred[32];
+  __syncthreads();
+  return r;
+}
 
 template <typename R>
 __global__ void __launch_bounds__(kCdfThreads) k_cdf_sequential(const typename Vec2<R>::T* a, uint64_t N, double thr,
                                                                 double* cum, uint64_t* last) {
-  __shared__ __align__(16) double buf[3][kCdfChunk];  // 48 KB, the static limit
-  const uint64_t CH = N < (uint64_t)kCdfChunk ? N : (uint64_t)kCdfChunk;
-  const uint64_t nch = N / CH;
+  __shared__ long long wsum[32];
+  __shared__ unsigned long long wred[33];
+  __shared__ double s_sh;            // the running sum after entry c - 1 (exact)
+  __shared__ unsigned long long c_sh;  // next entry
   const int tid = threadIdx.x;
-  const int wtid = tid - 32;  // worker index (warps 1..)
-  const int nwork = kCdfThreads - 32;
-  // the last kept index: each thread's largest among the entries it loaded,
-  // then the block's largest
-  long long lk = -1;
-  // chunk 0 by every thread
-  for (uint64_t i = tid; i < CH; i += kCdfThreads) {
-    const double p = pref<R>(a, i);
-    const bool keep = p > thr;
-    buf[0][i] = keep ? p : -0.0;
-    if (keep) lk = (long long)i;
-  }
-  double acc = 0.0;
+  const uint64_t NONE = ~0ull;
+  long long lk = -1;  // the last kept entry this thread loaded
+  if (tid == 0) { s_sh = 0.0; c_sh = 0; }
   __syncthreads();
-  for (uint64_t c = 0; c <= nch; c++) {
-    if (tid == 0 && c < nch) {
-      // the chain: one load, one add, one store per entry, loads 16 ahead
-      double* b = buf[c % 3];
-      int i = 0;
-      for (; i + 16 <= (int)CH; i += 16) {
-        double v[16];
+  for (;;) {
+    const uint64_t c = c_sh;
+    const double s = s_sh;
+    if (c >= N) break;
+    // this thread's entries c + kCdfPer*tid + k
+    const uint64_t i0 = c + (uint64_t)kCdfPer * tid;
+    double pv[kCdfPer];
 #pragma unroll
-        for (int j = 0; j < 16; j++) v[j] = b[i + j];
+    for (int k = 0; k < kCdfPer; k++) {
+      const uint64_t i = i0 + k;
+      double p = -0.0;  // not kept (or past the end): adds nothing
+      if (i < N) {
+        const double q = pref<R>(a, i);
+        if (q > thr) { p = q; lk = (long long)i; }
+      }
+      pv[k] = p;
+    }
+    if (s == 0.0) {
+      // before the first kept entry the sum is +0.0; that entry sets it exactly
+      unsigned long long f = NONE;
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-          acc += v[j];
-          b[i + j] = acc;
+      for (int k = 0; k < kCdfPer; k++)
+        if (f == NONE && i0 + k < N && __double_as_longlong(pv[k]) > 0) f = i0 + k;
+      f = block_min_u64(f, wred);
+#pragma unroll
+      for (int k = 0; k < kCdfPer; k++) {
+        const uint64_t i = i0 + k;
+        if (i < N && i < f) cum[i] = 0.0;
+      }
+      if (tid == 0) {
+        if (f != NONE) {
+          const double p0 = pref<R>(a, f);
+          s_sh = 0.0 + p0;
+          cum[f] = s_sh;
+          c_sh = f + 1;
+        } else {
+          c_sh = c + kCdfChunk;
         }
       }
-      for (; i < (int)CH; i++) {  // states of fewer than 16 amplitudes
-        acc += b[i];
-        b[i] = acc;
+      __syncthreads();
+      continue;
+    }
+    // s in [2^(e-1), 2^e): u = 2^(e-53), S = s / u
+    int e;
+    frexp(s, &e);
+    const long long S0 = (long long)ldexp(s, 53 - e);
+    unsigned long long special = NONE;  // first entry that is a tie or crosses for sure
+    long long d[kCdfPer];
+    long long tsum = 0;
+#pragma unroll
+    for (int k = 0; k < kCdfPer; k++) {
+      const uint64_t i = i0 + k;
+      d[k] = 0;
+      if (i >= N) continue;
+      const double q = ldexp(pv[k], 53 - e);  // p / u, exact
+      if (q >= 9007199254740992.0) {          // 2^53: the sum leaves the binade
+        if (special == NONE) special = i;
+        continue;
       }
-    } else if (tid >= 32) {
-      if (c >= 1) {  // running sums of chunk c-1 out
-        const double* b = buf[(c - 1) % 3];
-        for (int i = wtid; i < (int)CH; i += nwork) cum[(c - 1) * CH + i] = b[i];
+      const double fl = floor(q);
+      if (q - fl == 0.5) {                    // a tie: the rounding depends on S
+        if (special == NONE) special = i;
+        continue;
       }
-      if (c + 1 < nch) {  // kept probabilities of chunk c+1 in
-        double* b = buf[(c + 1) % 3];
-        const uint64_t base = (c + 1) * CH;
-        for (int i = wtid; i < (int)CH; i += nwork) {
-          const double p = pref<R>(a, base + i);
-          const bool keep = p > thr;
-          b[i] = keep ? p : -0.0;
-          if (keep) lk = (long long)(base + i);
-        }
+      if (special == NONE) {
+        d[k] = (long long)rint(q);
+        tsum += d[k];
       }
+    }
+    special = block_min_u64(special, wred);
+    // entries at or after the first special one do not count in the scan
+    if (special != NONE && i0 >= special) tsum = 0;
+    if (special != NONE && i0 < special) {
+      tsum = 0;
+#pragma unroll
+      for (int k = 0; k < kCdfPer; k++)
+        if (i0 + k < special) tsum += d[k];
+    }
+    const long long incl = block_scan_incl(tsum, wsum);
+    long long Sr = S0 + incl - tsum;  // S before this thread's first entry
+    unsigned long long cross = NONE;  // first entry whose sum reaches 2^53 u
+#pragma unroll
+    for (int k = 0; k < kCdfPer; k++) {
+      const uint64_t i = i0 + k;
+      if (i >= N || (special != NONE && i >= special)) break;
+      const long long Sn = Sr + d[k];
+      if (Sn >= 9007199254740992ll) { cross = i; break; }
+      Sr = Sn;
+    }
+    cross = block_min_u64(cross, wred);
+    const uint64_t lim = c + (uint64_t)kCdfChunk < N ? c + (uint64_t)kCdfChunk : N;
+    uint64_t stop = special < cross ? (uint64_t)special : (uint64_t)cross;
+    if (stop > lim) stop = lim;
+    // write the exact sums of the entries before `stop`
+    Sr = S0 + incl - tsum;
+#pragma unroll
+    for (int k = 0; k < kCdfPer; k++) {
+      const uint64_t i = i0 + k;
+      if (i >= stop) break;
+      Sr += d[k];
+      cum[i] = ldexp((double)Sr, e - 53);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      // the sum just before `stop`: the running S (all entries < stop are in range)
+      double sp = s;
+      if (stop > c) sp = cum[stop - 1];
+      if (stop < lim) {
+        // the special entry, by the reference's own FP64 addition
+        const double q = pref<R>(a, stop);
+        const double p = q > thr ? q : -0.0;
+        sp = sp + p;
+        cum[stop] = sp;
+        c_sh = stop + 1;
+      } else {
+        c_sh = stop;
+      }
+      s_sh = sp;
     }
     __syncthreads();
   }
-  // block maximum of lk through the spent chunks
-  long long* red = reinterpret_cast<long long*>(buf[0]);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) lk = max(lk, __shfl_xor_sync(0xffffffffu, lk, o));
-  if ((tid & 31) == 0) red[tid >> 5] = lk;
-  __syncthreads();
-  if (tid < 32) {
-    long long v = red[tid];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if (tid == 0) red[32] = v;
-  }
-  __syncthreads();
-  const uint64_t l = (uint64_t)red[32];
+  // the last kept entry: the block's largest
+  unsigned long long nl = lk < 0 ? NONE : ~(unsigned long long)lk;  // min of ~x is max of x
+  nl = block_min_u64(nl, wred);
+  const uint64_t l = nl == NONE ? NONE : ~nl;
   if (tid == 0) *last = l;
+  __syncthreads();
   // the reference sets the last kept entry's cumP to 1.0; entries after it
   // are never kept, so the search treats them alike
-  if (l != ~uint64_t(0))
+  if (l != NONE)
     for (uint64_t i = l + tid; i < N; i += kCdfThreads) cum[i] = 1.0;
 }
 

@@ -163,3 +163,49 @@ def test_shots_sequential_cdf_vs_oracle(n, layers):
     for i in want.tolist():
         counts[i] = counts.get(i, 0) + 1
     assert dist.probs == {format(i, "b").zfill(n)[::-1]: c / 4096 for i, c in counts.items()}
+
+
+def _sample_vs_numpy_cdf(n, amps, draws_at=None, rng_seed=0):
+    """Shots from ket_sample against a lower bound on numpy's sequential
+    cumulative sum (np.cumsum adds left to right, rounding each step, as the
+    reference's loop does).  Draws sit exactly on CDF values and one ulp above
+    them, so any last-bit difference in the device CDF changes an index."""
+    from ket_b200.circuit import DeviceState
+    st = DeviceState(n)
+    st.set_amplitudes(amps)
+    p = amps.real * amps.real + amps.imag * amps.imag
+    kept = p > 1e-14
+    cum = np.cumsum(np.where(kept, p, 0.0))
+    last = np.nonzero(kept)[0][-1]
+    cum[last:] = 1.0
+    idx = draws_at if draws_at is not None else np.arange(1 << n)
+    r = np.concatenate([cum[idx], np.nextafter(cum[idx], np.inf),
+                        np.random.default_rng(rng_seed).random(4096) * cum[last - 1]])
+    r = r[r <= 1.0]
+    want = np.searchsorted(cum, r, side="left")
+    got = st.sample(r)
+    assert np.array_equal(got, want)
+
+
+def test_sequential_cdf_ties_and_binades():
+    """Entries whose probability lies exactly halfway between two multiples of
+    the running sum's ulp (a tie the reference's rounding breaks by the sum's
+    parity), a binade crossing at the start, entries below the pruning
+    threshold and exact zeros."""
+    n = 14
+    a = np.zeros(1 << n, dtype=np.complex128)
+    a[0] = 0.6 ** 0.5                      # the sum starts in [0.5, 1): ulp 2^-53
+    a[1:] = 2.0 ** -23 + 1j * 2.0 ** -27   # p = 2^-46 + 2^-54: every addition is a tie
+    a[5::7] = 1e-8                         # p = 1e-16: below the threshold, not kept
+    a[9::11] = 0.0
+    _sample_vs_numpy_cdf(n, a)
+
+
+@pytest.mark.parametrize("n", [10, 16, 20])
+def test_sequential_cdf_random_states(n):
+    rng = np.random.default_rng(n)
+    a = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    a[rng.random(1 << n) < 0.1] = 0.0
+    a /= np.linalg.norm(a)
+    sel = np.unique(rng.integers(0, 1 << n, 20000))
+    _sample_vs_numpy_cdf(n, a, draws_at=sel, rng_seed=n)
