@@ -287,10 +287,11 @@ KET_API int ket_state_compare(const ket_state* a, const ket_state* b, double* ov
 /* Sum of |a|^2 (FP64 accumulation). */
 KET_API int ket_norm2(const ket_state* st, double* out);
 /* run() pure fast path sampler (circuit.ts:3424-3453): r[s] are the caller's
- * uniform draws (makePrng, circuit.ts:813-819); out_idx[s] = the first index, in
- * ascending order over entries with p > threshold, whose running FP64 sum is >= r[s]
- * (the last such entry's running sum is taken as 1.0).  For 2^n <= 2^22 the running
- * sum is accumulated in ascending index order, exactly as the reference does. */
+ * uniform draws (makePrng, circuit.ts:813-819), each in [0, 1] (KET_ERR_RANGE
+ * otherwise); out_idx[s] = the first index, in ascending order over entries with
+ * p > threshold, whose running FP64 sum is >= r[s] (the last such entry's running sum
+ * is taken as 1.0).  The running sum is the reference's, rounded after every
+ * addition in ascending index order, bit for bit at every state size. */
 KET_API int ket_sample(const ket_state* st, const double* r, size_t shots, double threshold, uint64_t* out_idx);
 /* circuitMatrix() (circuit.ts:1462-1485): the 2^n x 2^n matrix of ops on
  * nqubits <= 12 (KET_ERR_RANGE above, as the reference), out[row * 2^n + col]

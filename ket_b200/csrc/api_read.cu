@@ -181,28 +181,28 @@ int ket_marginal_dist(const ket_state* s, const int* qubits, int m, double* out)
 }
 
 int ket_sample(const ket_state* s, const double* r, size_t shots, double thr, uint64_t* out) {
-  return ket::sample_indices(s, r, shots, thr, KET_SEQ_CDF_QUBITS, out);
+  return ket::sample_indices(s, r, shots, thr, out);
 }
 
 }  // extern "C"
 
 namespace ket {
 
-int sample_indices(const ket_state* s, const double* r, size_t shots, double thr, int seq_qubits, uint64_t* out) {
+int sample_indices(const ket_state* s, const double* r, size_t shots, double thr, uint64_t* out) {
   TRY(check_state(s));
   if (shots && (!r || !out)) return fail(KET_ERR_TYPE, "null argument");
   if (!shots) return KET_OK;
-  size_t need = sample_scratch(s->n, seq_qubits) + 16 * shots + 1024;
+  for (size_t i = 0; i < shots; i++)
+    if (!(r[i] >= 0.0 && r[i] <= 1.0)) return fail(KET_ERR_RANGE, "a draw outside [0, 1]");
+  size_t need = sample_scratch(s->n) + 16 * shots + 1024;
   void* scr;
   TRY(ctx_scratch(s->ctx, need, &scr));
   double* dr = (double*)scr;
   uint64_t* dout = (uint64_t*)align_up((char*)(dr + shots), 256);
   void* work = align_up((char*)(dout + shots), 256);
   TRY(h2d(s->ctx, dr, r, 8 * shots));
-  // the sequential CDF path runs two kernels, the chunked one three
-  s->ctx->launches += (s->n <= seq_qubits || s->n < 10) ? 1 : 2;
-  TRY(LAUNCH_READ(s->ctx, launch_sample(s->amp, s->n, s->precision, thr, seq_qubits, dr, shots, work, dout,
-                                         s->ctx->stream)));
+  s->ctx->launches += sample_launches() - 1;  // LAUNCH_READ counts one
+  TRY(LAUNCH_READ(s->ctx, launch_sample(s->amp, s->n, s->precision, thr, dr, shots, work, dout, s->ctx->stream)));
   TRY(d2h(s->ctx, out, dout, 8 * shots));
   return ctx_wait(s->ctx);
 }

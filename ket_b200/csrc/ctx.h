@@ -60,7 +60,7 @@ int ctx_wait(ket_ctx* ctx);
 int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait = true);
 int check_status(ket_ctx* c);
 // ket_sample with the sequential CDF up to seq_qubits qubits (see read.h).
-int sample_indices(const ket_state* s, const double* r, size_t shots, double thr, int seq_qubits, uint64_t* out);
+int sample_indices(const ket_state* s, const double* r, size_t shots, double thr, uint64_t* out);
 
 // Launch kinds reported by ket_ctx_profile_read.
 enum { PK_FUSED2 = 0, PK_FUSED1 = 1, PK_GATE = 2, PK_READ = 3, PK_ADJOINT = 4, PK_BATCH = 5 };

@@ -220,53 +220,83 @@ __global__ void k_marginal_dist(const typename Vec2<R>::T* a, int c, MarginalSpe
 }
 
 // ------------------------------------------------------------------ sampling
-// Exact reference order (small states): cum[i] = the running FP64 sum over
-// kept entries in ascending index order, rounded after every addition as
-// the reference's loop does (circuit.ts:3429-3436) -- computed in parallel,
-// bit for bit.
+// The sampling CDF is the reference's running FP64 sum over kept entries in
+// ascending index order, rounded after every addition (circuit.ts:3429-3436),
+// reproduced bit for bit at every state size.  It is kept as checkpoints:
+// ck[k] = the running sum before entry 32k, ck[nk] = the total.  A draw finds
+// its 32-entry sub-chunk by binary search over ck and finishes with the
+// reference's own FP64 additions from ck[k].
 //
 // While the running sum s stays in one binade [2^(e-1), 2^e), every value it
-// takes is a multiple of u = 2^(e-53), s = S u with S an integer in
-// [2^52, 2^53).  Adding p then rounds to the nearest multiple of u, so
+// takes is a multiple of u = 2^(e-53): s = S u with S an integer in
+// [2^52, 2^53).  Adding p rounds to the nearest multiple of u, so
 // s + p = (S + d) u with d = round(p / u) -- an increment that does not
 // depend on s, except when p / u lies exactly halfway (the tie goes to the
-// even S + d) or when S + d reaches 2^53 (the sum leaves the binade and
-// rounds on the next grid).  So a chunk of entries is an integer prefix sum
-// of the d's, done by the whole block, up to the first tie or binade
-// crossing; thread 0 takes that one entry with the FP64 addition itself, and
-// the next chunk starts after it.  Entries that are not kept add nothing.
-// Before the first kept entry the sum is +0.0.  A binade is crossed about
-// once per doubling of s, so the single-entry steps are few.
+// even S + d) or when S + d reaches 2^53 (the sum leaves the binade and rounds
+// on the next grid).  A run of entries inside one binade is therefore an
+// integer prefix sum of the d's.  Five kernels build the checkpoints:
+//   k_cdf_block_sums    per block of 4096 entries, the plain sum of the kept
+//                       p's and the first and last kept index;
+//   k_cdf_block_prefix  an approximate exclusive prefix of those sums -- it
+//                       only guesses the binade each block starts in -- and
+//                       the first and last kept index of the state;
+//   k_cdf_block_d       per block, in the guessed binade, the d's, their sum D
+//                       and their exclusive prefix at every 32-entry
+//                       sub-chunk; a block holding a tie or an oversized d, or
+//                       with nothing kept before it, is marked unclean;
+//   k_cdf_walk          one CTA carries the exact running sum across windows
+//                       of blocks.  A block is taken whole when nothing in it
+//                       is kept, or when it is clean in the binade the exact
+//                       sum is in and S + D stays below 2^53 -- its integer
+//                       prefix is then exact.  Any other block runs entry by
+//                       entry (cdf_exact_range): integer prefix sums up to the
+//                       next tie or crossing, which takes the FP64 addition
+//                       itself;
+//   k_cdf_fill          the checkpoints of the blocks taken whole, from their
+//                       exact start and the sub-chunk prefixes.
+// Only blocks holding a binade crossing, a tie or the first kept entry run
+// entry by entry: a crossing happens about once per doubling of s.
 constexpr int kCdfThreads = 1024;
 constexpr int kCdfPer = 4;                          // entries per thread per chunk
 constexpr int kCdfChunk = kCdfThreads * kCdfPer;    // 4096
+constexpr int kCdfBlock = 4096;                     // entries per block
+constexpr int kCdfSub = 32;                         // entries per checkpoint
+constexpr int kCdfSubPerBlock = kCdfBlock / kCdfSub;
+constexpr int kCdfWalkPer = 4;                      // blocks per walker thread per window
+constexpr long long kTwo52 = 4503599627370496ll;
+constexpr long long kTwo53 = 9007199254740992ll;
+static_assert(kCdfChunk == kCdfBlock, "an entry-by-entry block is one chunk");
 
-// Inclusive block scan of v (NT = kCdfThreads); `wsum` holds 32 partials.
-__device__ __forceinline__ long long block_scan_incl(long long v, long long* wsum) {
+enum : int { kBlkUnclean = 0, kBlkClean = 1, kBlkEmpty = 2, kBlkExact = 3 };
+
+// Inclusive block scan of v over NT threads; `wsum` holds 32 partials.
+template <int NT, typename T>
+__device__ __forceinline__ T block_scan_incl(T v, T* wsum) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const long long t = __shfl_up_sync(0xffffffffu, v, o);
+    const T t = __shfl_up_sync(0xffffffffu, v, o);
     if (lane >= o) v += t;
   }
   if (lane == 31) wsum[w] = v;
   __syncthreads();
   if (w == 0) {
-    long long x = wsum[lane];
+    T x = lane < NT / 32 ? wsum[lane] : T(0);
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const long long t = __shfl_up_sync(0xffffffffu, x, o);
+      const T t = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= o) x += t;
     }
     wsum[lane] = x;
   }
   __syncthreads();
-  const long long r = v + (w > 0 ? wsum[w - 1] : 0);
+  const T r = v + (w > 0 ? wsum[w - 1] : T(0));
   __syncthreads();  // wsum is reused by the next scan
   return r;
 }
 
-// Block minimum of v; every thread gets it.
+// Block minimum of v over NT threads; every thread gets it.
+template <int NT>
 __device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v, unsigned long long* wred) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -274,7 +304,7 @@ __device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v
   if (lane == 0) wred[w] = v;
   __syncthreads();
   if (w == 0) {
-    unsigned long long x = wred[lane];
+    unsigned long long x = lane < NT / 32 ? wred[lane] : ~0ull;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x = min(x, __shfl_xor_sync(0xffffffffu, x, o));
     if (lane == 0) wred[32] = x;
@@ -285,55 +315,173 @@ __device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v
   return r;
 }
 
+// The kept probability of entry i: p when p > thr, else +0.0 (adds nothing).
 template <typename R>
-__global__ void __launch_bounds__(kCdfThreads) k_cdf_sequential(const typename Vec2<R>::T* a, uint64_t N, double thr,
-                                                                double* cum, uint64_t* last) {
-  __shared__ long long wsum[32];
+__device__ __forceinline__ double kept_p(const typename Vec2<R>::T* a, uint64_t i, double thr) {
+  const double p = pref<R>(a, i);
+  return p > thr ? p : 0.0;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_cdf_block_sums(const typename Vec2<R>::T* a, uint64_t N, double thr,
+                                                        double* bsum, unsigned long long* bfirst,
+                                                        unsigned long long* blast) {
+  __shared__ double red[32];
   __shared__ unsigned long long wred[33];
-  __shared__ double s_sh;            // the running sum after entry c - 1 (exact)
-  __shared__ unsigned long long c_sh;  // next entry
+  const uint64_t lo = (uint64_t)blockIdx.x * kCdfBlock;
+  double acc = 0.0;
+  unsigned long long f = ~0ull, l = ~0ull;  // l holds ~index, so the minimum is the largest index
+#pragma unroll 4
+  for (int k = 0; k < kCdfBlock / 256; k++) {
+    const uint64_t i = lo + (uint64_t)k * 256 + threadIdx.x;
+    if (i < N) {
+      const double p = pref<R>(a, i);
+      if (p > thr) {
+        acc += p;
+        if (f == ~0ull) f = i;
+        l = ~(unsigned long long)i;
+      }
+    }
+  }
+  const double t = block_sum<256>(acc, red);
+  f = block_min_u64<256>(f, wred);
+  l = block_min_u64<256>(l, wred);
+  if (threadIdx.x == 0) {
+    bsum[blockIdx.x] = t;
+    bfirst[blockIdx.x] = f;
+    blast[blockIdx.x] = l;
+  }
+}
+
+// bsum[0..nb) -> its exclusive prefix, bsum[nb] = the total; fl[0] = the
+// first kept index, fl[1] = the last (~0: nothing kept).
+__global__ void __launch_bounds__(kCdfThreads) k_cdf_block_prefix(double* bsum, const unsigned long long* bfirst,
+                                                                  const unsigned long long* blast, uint64_t nb,
+                                                                  unsigned long long* fl) {
+  __shared__ double wsd[32];
+  __shared__ unsigned long long wred[33];
+  const uint64_t per = (nb + kCdfThreads - 1) / kCdfThreads;
+  const uint64_t lo = min(nb, (uint64_t)threadIdx.x * per), hi = min(nb, lo + per);
+  double t = 0.0;
+  unsigned long long f = ~0ull, l = ~0ull;
+  for (uint64_t b = lo; b < hi; b++) {
+    t += bsum[b];
+    f = min(f, bfirst[b]);
+    l = min(l, blast[b]);
+  }
+  const double incl = block_scan_incl<kCdfThreads>(t, wsd);
+  double x = incl - t;
+  for (uint64_t b = lo; b < hi; b++) {
+    const double v = bsum[b];
+    bsum[b] = x;
+    x += v;
+  }
+  f = block_min_u64<kCdfThreads>(f, wred);
+  l = block_min_u64<kCdfThreads>(l, wred);
+  if (threadIdx.x == kCdfThreads - 1) bsum[nb] = incl;
+  if (threadIdx.x == 0) {
+    fl[0] = f;
+    fl[1] = l == ~0ull ? ~0ull : ~l;
+  }
+}
+
+// Warp w handles sub-chunks 16w .. 16w + 15; lane l reads entry 32j + l of
+// sub-chunk j, so every load is 32 consecutive amplitudes.
+template <typename R>
+__global__ void __launch_bounds__(256) k_cdf_block_d(const typename Vec2<R>::T* a, uint64_t N, double thr,
+                                                     const double* bstart_approx, long long* ckd, long long* bd,
+                                                     int* bst, int* be) {
+  static_assert(kCdfSubPerBlock == 8 * 16, "8 warps of 16 sub-chunks");
+  __shared__ long long wsum[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint64_t b = blockIdx.x, lo = b * kCdfBlock;
+  const double A = bstart_approx[b];
+  int e = 0;
+  if (A > 0.0) frexp(A, &e);
+  const bool guess = A > 0.0;
+  bool pos = false, bad = false;
+  long long mine = 0;  // lane k < 16: the d-sum of sub-chunk 16w + k
+#pragma unroll 4
+  for (int k = 0; k < 16; k++) {
+    const uint64_t i = lo + (uint64_t)(16 * w + k) * kCdfSub + lane;
+    const double p = i < N ? kept_p<R>(a, i, thr) : 0.0;
+    pos |= p > 0.0;
+    long long d = 0;
+    if (guess) {
+      const double q = ldexp(p, 53 - e);  // p / u, exact
+      if (q >= 4503599627370496.0) bad = true;  // 2^52: S + d would leave the binade
+      else if (q - floor(q) == 0.5) bad = true;   // a tie: the rounding depends on S
+      else d = (long long)rint(q);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    if (lane == k) mine = d;
+  }
+  const bool any_pos = __syncthreads_or(pos);
+  const bool any_bad = __syncthreads_or(bad);
+  // a sub-chunk sum is below 2^57; clamped at 2^53 the block total stays exact
+  // below 2^53 and cannot overflow
+  const long long v = lane < 16 ? (mine < kTwo53 ? mine : kTwo53) : 0;
+  const long long incl = block_scan_incl<256>(v, wsum);
+  __shared__ long long total;
+  if (threadIdx.x == 255) total = incl;
+  __syncthreads();
+  const uint64_t j = 16 * w + lane;
+  if (lane < 16 && lo + j * kCdfSub < N) ckd[b * kCdfSubPerBlock + j] = incl - v;
+  if (threadIdx.x == 0) {
+    int st;
+    if (!any_pos) st = kBlkEmpty;
+    else if (!guess || any_bad || total >= kTwo53) st = kBlkUnclean;
+    else st = kBlkClean;
+    bst[b] = st;
+    be[b] = e;
+    bd[b] = total;
+  }
+}
+
+// The running sum over entries [lo, hi) (hi - lo <= kCdfChunk) in the
+// reference's rounding, from the exact sum *s_io before lo.  Writes the
+// checkpoints ck[(i + 1) / 32] for entries i with (i + 1) % 32 == 0 and
+// i + 1 < hi, and leaves the sum after entry hi - 1 in *s_io.  Called by the
+// whole CTA of kCdfThreads threads.
+template <typename R>
+__device__ void cdf_exact_range(const typename Vec2<R>::T* a, uint64_t lo, uint64_t hi, double thr, double* ck,
+                                double* s_io, unsigned long long* c_io, long long* wsum, unsigned long long* wred) {
   const int tid = threadIdx.x;
-  const uint64_t NONE = ~0ull;
-  long long lk = -1;  // the last kept entry this thread loaded
-  if (tid == 0) { s_sh = 0.0; c_sh = 0; }
+  const unsigned long long NONE = ~0ull;
+  if (tid == 0) *c_io = lo;
   __syncthreads();
   for (;;) {
-    const uint64_t c = c_sh;
-    const double s = s_sh;
-    if (c >= N) break;
+    const uint64_t c = *c_io;
+    const double s = *s_io;
+    if (c >= hi) break;
     // this thread's entries c + kCdfPer*tid + k
     const uint64_t i0 = c + (uint64_t)kCdfPer * tid;
     double pv[kCdfPer];
 #pragma unroll
-    for (int k = 0; k < kCdfPer; k++) {
-      const uint64_t i = i0 + k;
-      double p = -0.0;  // not kept (or past the end): adds nothing
-      if (i < N) {
-        const double q = pref<R>(a, i);
-        if (q > thr) { p = q; lk = (long long)i; }
-      }
-      pv[k] = p;
-    }
+    for (int k = 0; k < kCdfPer; k++) pv[k] = i0 + k < hi ? kept_p<R>(a, i0 + k, thr) : 0.0;
     if (s == 0.0) {
-      // before the first kept entry the sum is +0.0; that entry sets it exactly
+      // before the first positive kept entry the sum is +0.0; that entry sets
+      // it exactly
       unsigned long long f = NONE;
 #pragma unroll
       for (int k = 0; k < kCdfPer; k++)
-        if (f == NONE && i0 + k < N && __double_as_longlong(pv[k]) > 0) f = i0 + k;
-      f = block_min_u64(f, wred);
+        if (f == NONE && pv[k] > 0.0) f = i0 + k;
+      f = block_min_u64<kCdfThreads>(f, wred);
+      const uint64_t z = f == NONE ? hi : f;
 #pragma unroll
       for (int k = 0; k < kCdfPer; k++) {
         const uint64_t i = i0 + k;
-        if (i < N && i < f) cum[i] = 0.0;
+        if (i < z && ((i + 1) & (kCdfSub - 1)) == 0 && i + 1 < hi) ck[(i + 1) / kCdfSub] = 0.0;
       }
       if (tid == 0) {
         if (f != NONE) {
-          const double p0 = pref<R>(a, f);
-          s_sh = 0.0 + p0;
-          cum[f] = s_sh;
-          c_sh = f + 1;
+          const double sn = 0.0 + kept_p<R>(a, f, thr);
+          if (((f + 1) & (kCdfSub - 1)) == 0 && f + 1 < hi) ck[(f + 1) / kCdfSub] = sn;
+          *s_io = sn;
+          *c_io = f + 1;
         } else {
-          c_sh = c + kCdfChunk;
+          *c_io = hi;
         }
       }
       __syncthreads();
@@ -350,14 +498,13 @@ __global__ void __launch_bounds__(kCdfThreads) k_cdf_sequential(const typename V
     for (int k = 0; k < kCdfPer; k++) {
       const uint64_t i = i0 + k;
       d[k] = 0;
-      if (i >= N) continue;
+      if (i >= hi) continue;
       const double q = ldexp(pv[k], 53 - e);  // p / u, exact
       if (q >= 9007199254740992.0) {          // 2^53: the sum leaves the binade
         if (special == NONE) special = i;
         continue;
       }
-      const double fl = floor(q);
-      if (q - fl == 0.5) {                    // a tie: the rounding depends on S
+      if (q - floor(q) == 0.5) {              // a tie: the rounding depends on S
         if (special == NONE) special = i;
         continue;
       }
@@ -366,164 +513,188 @@ __global__ void __launch_bounds__(kCdfThreads) k_cdf_sequential(const typename V
         tsum += d[k];
       }
     }
-    special = block_min_u64(special, wred);
+    special = block_min_u64<kCdfThreads>(special, wred);
     // entries at or after the first special one do not count in the scan
-    if (special != NONE && i0 >= special) tsum = 0;
-    if (special != NONE && i0 < special) {
+    if (special != NONE) {
       tsum = 0;
 #pragma unroll
       for (int k = 0; k < kCdfPer; k++)
         if (i0 + k < special) tsum += d[k];
     }
-    const long long incl = block_scan_incl(tsum, wsum);
+    const long long incl = block_scan_incl<kCdfThreads>(tsum, wsum);
     long long Sr = S0 + incl - tsum;  // S before this thread's first entry
     unsigned long long cross = NONE;  // first entry whose sum reaches 2^53 u
 #pragma unroll
     for (int k = 0; k < kCdfPer; k++) {
       const uint64_t i = i0 + k;
-      if (i >= N || (special != NONE && i >= special)) break;
+      if (i >= hi || i >= special) break;
       const long long Sn = Sr + d[k];
-      if (Sn >= 9007199254740992ll) { cross = i; break; }
+      if (Sn >= kTwo53) { cross = i; break; }
       Sr = Sn;
     }
-    cross = block_min_u64(cross, wred);
-    const uint64_t lim = c + (uint64_t)kCdfChunk < N ? c + (uint64_t)kCdfChunk : N;
+    cross = block_min_u64<kCdfThreads>(cross, wred);
+    const uint64_t lim = c + (uint64_t)kCdfChunk < hi ? c + (uint64_t)kCdfChunk : hi;
     uint64_t stop = special < cross ? (uint64_t)special : (uint64_t)cross;
     if (stop > lim) stop = lim;
-    // write the exact sums of the entries before `stop`
+    // the exact sums of the entries before `stop`
     Sr = S0 + incl - tsum;
 #pragma unroll
     for (int k = 0; k < kCdfPer; k++) {
       const uint64_t i = i0 + k;
       if (i >= stop) break;
       Sr += d[k];
-      cum[i] = ldexp((double)Sr, e - 53);
+      const double v = ldexp((double)Sr, e - 53);
+      if (((i + 1) & (kCdfSub - 1)) == 0 && i + 1 < hi) ck[(i + 1) / kCdfSub] = v;
+      if (i + 1 == stop) *s_io = v;
     }
     __syncthreads();
     if (tid == 0) {
-      // the sum just before `stop`: the running S (all entries < stop are in range)
-      double sp = s;
-      if (stop > c) sp = cum[stop - 1];
+      double sp = *s_io;  // the sum before `stop` (s itself when stop == c)
       if (stop < lim) {
         // the special entry, by the reference's own FP64 addition
-        const double q = pref<R>(a, stop);
-        const double p = q > thr ? q : -0.0;
-        sp = sp + p;
-        cum[stop] = sp;
-        c_sh = stop + 1;
+        sp = sp + kept_p<R>(a, stop, thr);
+        if (((stop + 1) & (kCdfSub - 1)) == 0 && stop + 1 < hi) ck[(stop + 1) / kCdfSub] = sp;
+        *s_io = sp;
+        *c_io = stop + 1;
       } else {
-        c_sh = stop;
+        *c_io = stop;
       }
-      s_sh = sp;
     }
     __syncthreads();
   }
-  // the last kept entry: the block's largest
-  unsigned long long nl = lk < 0 ? NONE : ~(unsigned long long)lk;  // min of ~x is max of x
-  nl = block_min_u64(nl, wred);
-  const uint64_t l = nl == NONE ? NONE : ~nl;
-  if (tid == 0) *last = l;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kCdfThreads) k_cdf_walk(const typename Vec2<R>::T* a, uint64_t N, double thr,
+                                                          uint64_t nb, uint64_t nk, double* ck, const long long* bd,
+                                                          int* bst, const int* be, double* bstart) {
+  __shared__ long long wsum[32];
+  __shared__ unsigned long long wred[33];
+  __shared__ double s_sh;              // the exact running sum before block c
+  __shared__ unsigned long long c_sh;  // the next block
+  __shared__ unsigned long long x_sh;  // cdf_exact_range's position
+  const int tid = threadIdx.x;
+  const unsigned long long NONE = ~0ull;
+  if (tid == 0) { s_sh = 0.0; c_sh = 0; }
   __syncthreads();
-  // the reference sets the last kept entry's cumP to 1.0; entries after it
-  // are never kept, so the search treats them alike
-  if (l != NONE)
-    for (uint64_t i = l + tid; i < N; i += kCdfThreads) cum[i] = 1.0;
+  for (;;) {
+    const uint64_t c = c_sh;
+    const double s = s_sh;
+    if (c >= nb) break;
+    int e = 0;
+    long long S0 = 0;
+    if (s > 0.0) {
+      frexp(s, &e);
+      S0 = (long long)ldexp(s, 53 - e);
+    }
+    // this thread's blocks c + kCdfWalkPer*tid + k
+    const uint64_t b0 = c + (uint64_t)kCdfWalkPer * tid;
+    long long dv[kCdfWalkPer];
+    unsigned long long fail = NONE;  // first block that is not taken whole
+#pragma unroll
+    for (int k = 0; k < kCdfWalkPer; k++) {
+      const uint64_t b = b0 + k;
+      dv[k] = 0;
+      if (b >= nb || fail != NONE) continue;
+      const int st = bst[b];
+      if (st == kBlkEmpty) continue;
+      if (st == kBlkClean && s > 0.0 && be[b] == e) dv[k] = bd[b];
+      else fail = b;
+    }
+    fail = block_min_u64<kCdfThreads>(fail, wred);
+    long long tsum = 0;
+#pragma unroll
+    for (int k = 0; k < kCdfWalkPer; k++)
+      if (b0 + k < fail) tsum += dv[k];
+    const long long incl = block_scan_incl<kCdfThreads>(tsum, wsum);  // each D < 2^53: no overflow
+    long long Sr = S0 + incl - tsum;
+    unsigned long long cross = NONE;  // first block whose sum reaches 2^53 u
+#pragma unroll
+    for (int k = 0; k < kCdfWalkPer; k++) {
+      const uint64_t b = b0 + k;
+      if (b >= nb || b >= fail) break;
+      if (Sr + dv[k] >= kTwo53) { cross = b; break; }
+      Sr += dv[k];
+    }
+    cross = block_min_u64<kCdfThreads>(cross, wred);
+    const uint64_t lim = c + (uint64_t)kCdfWalkPer * kCdfThreads < nb ? c + (uint64_t)kCdfWalkPer * kCdfThreads : nb;
+    uint64_t stop = fail < cross ? (uint64_t)fail : (uint64_t)cross;
+    if (stop > lim) stop = lim;
+    // blocks before `stop` are taken whole
+    Sr = S0 + incl - tsum;
+#pragma unroll
+    for (int k = 0; k < kCdfWalkPer; k++) {
+      const uint64_t b = b0 + k;
+      if (b >= stop) break;
+      bstart[b] = s > 0.0 ? ldexp((double)Sr, e - 53) : 0.0;
+      Sr += dv[k];
+      if (b + 1 == stop) s_sh = s > 0.0 ? ldexp((double)Sr, e - 53) : 0.0;
+    }
+    __syncthreads();
+    if (stop < lim) {
+      // block `stop` entry by entry
+      if (tid == 0) {
+        const double sb = s_sh;
+        bstart[stop] = sb;
+        bst[stop] = kBlkExact;
+        ck[stop * kCdfSubPerBlock] = sb;
+      }
+      const uint64_t lo = stop * kCdfBlock;
+      const uint64_t hi = lo + kCdfBlock < N ? lo + kCdfBlock : N;
+      cdf_exact_range<R>(a, lo, hi, thr, ck, &s_sh, &x_sh, wsum, wred);
+      if (tid == 0) c_sh = stop + 1;
+    } else if (tid == 0) {
+      c_sh = stop;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) ck[nk] = s_sh;
 }
 
-__global__ void k_sample_dense(const double* cum, uint64_t N, const double* r, uint64_t shots, const uint64_t* lastp,
-                               uint64_t* out) {
-  const uint64_t last = *lastp;
+// Checkpoints of the blocks taken whole: the exact start plus the sub-chunk's
+// d prefix, in the block's binade (ck holds the prefixes as integers until now).
+__global__ void k_cdf_fill(double* ck, uint64_t nk, const int* bst, const int* be, const double* bstart) {
+  long long* ckd = (long long*)ck;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nk; k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t b = k / kCdfSubPerBlock;
+    const int st = bst[b];
+    if (st == kBlkEmpty) {
+      ck[k] = bstart[b];
+    } else if (st == kBlkClean) {
+      const int e = be[b];
+      const long long S = (long long)ldexp(bstart[b], 53 - e);
+      ck[k] = ldexp((double)(S + ckd[k]), e - 53);
+    }
+  }
+}
+
+// One draw per thread: the first kept entry whose running sum is >= r, the
+// last kept entry's sum taken as 1.0 (circuit.ts:3438-3451).  The host checks
+// 0 <= r <= 1, so the walk ends inside one sub-chunk.
+template <typename R>
+__global__ void k_sample_ck(const typename Vec2<R>::T* a, uint64_t N, double thr, const double* ck, uint64_t nk,
+                            const double* r, uint64_t shots, const unsigned long long* fl, uint64_t* out) {
+  const uint64_t first = fl[0], last = fl[1];
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < shots; s += (uint64_t)gridDim.x * blockDim.x) {
     if (last == ~uint64_t(0)) { out[s] = 0; continue; }
-    double rv = r[s];
-    uint64_t lo = 0, hi = N - 1;
+    const double rv = r[s];
+    if (ck[nk] < rv) { out[s] = last; continue; }
+    uint64_t lo = 0, hi = nk;  // the first checkpoint >= r
     while (lo < hi) {
-      uint64_t mid = (lo + hi) >> 1;
-      if (cum[mid] < rv) lo = mid + 1; else hi = mid;
+      const uint64_t mid = (lo + hi) >> 1;
+      if (ck[mid] < rv) lo = mid + 1; else hi = mid;
     }
-    out[s] = lo;
-  }
-}
-
-// Chunked CDF for large states: lane l of warp c sums sub-chunk (c*32 + l) of
-// 32 entries sequentially; the warp then combines its 32 sub-chunk sums
-// sequentially.  chunk_sum[c] and last_kept[c] are written.
-template <typename R>
-__global__ void k_chunk_sums(const typename Vec2<R>::T* a, uint64_t nchunks, double thr, double* chunk_sum,
-                             uint64_t* last_kept) {
-  uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (warp >= nchunks) return;
-  uint64_t base = warp * 1024 + (uint64_t)lane * 32;
-  double s = 0.0;
-  long long lk = -1;
-  for (int j = 0; j < 32; j++) {
-    double p = pref<R>(a, base + j);
-    if (p > thr) { s += p; lk = (long long)(base + j); }
-  }
-  double tot = 0.0;
-  long long l2 = -1;
-  for (int j = 0; j < 32; j++) {
-    double v = __shfl_sync(0xffffffffu, s, j);
-    long long lj = __shfl_sync(0xffffffffu, lk, j);
-    tot += v;
-    if (lj >= 0) l2 = lj;
-  }
-  if (lane == 0) { chunk_sum[warp] = tot; last_kept[warp] = (uint64_t)l2; }
-}
-
-// Exclusive prefix E[0..nchunks] (sequential, one thread) and the last kept index.
-__global__ void k_chunk_prefix(const double* chunk_sum, const uint64_t* last_kept, uint64_t nchunks, double* E,
-                               uint64_t* last) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  double acc = 0.0;
-  uint64_t lk = ~uint64_t(0);
-  for (uint64_t c = 0; c < nchunks; c++) {
-    E[c] = acc;
-    acc += chunk_sum[c];
-    if (last_kept[c] != ~uint64_t(0)) lk = last_kept[c];
-  }
-  E[nchunks] = acc;
-  *last = lk;
-}
-
-template <typename R>
-__global__ void k_sample_chunked(const typename Vec2<R>::T* a, const double* E, uint64_t nchunks, double thr,
-                                 const double* r, uint64_t shots, const uint64_t* lastp, uint64_t* out) {
-  const uint64_t last = *lastp;
-  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < shots; s += (uint64_t)gridDim.x * blockDim.x) {
-    if (last == ~uint64_t(0)) { out[s] = 0; continue; }
-    double rv = r[s];
-    if (E[nchunks] < rv) { out[s] = last; continue; }  // the reference's last.cumP = 1.0
-    uint64_t lo = 0, hi = nchunks - 1;                // first chunk c with E[c+1] >= r
-    while (lo < hi) {
-      uint64_t mid = (lo + hi) >> 1;
-      if (E[mid + 1] < rv) lo = mid + 1; else hi = mid;
-    }
-    const uint64_t c = lo;
-    const double ec = E[c];
+    const uint64_t k = lo > 0 ? lo - 1 : 0;
+    double acc = ck[k];
+    uint64_t i = k * kCdfSub;
+    if (i < first) i = first;
     uint64_t res = last;
-    double W = 0.0;
-    bool found = false;
-    for (int sub = 0; sub < 32 && !found; sub++) {
-      uint64_t b = c * 1024 + (uint64_t)sub * 32;
-      double ps = 0.0;
-      for (int j = 0; j < 32; j++) {
-        double p = pref<R>(a, b + j);
-        if (p > thr) ps += p;
+    for (; i < last; i++) {
+      const double p = pref<R>(a, i);
+      if (p > thr) {
+        acc = acc + p;
+        if (acc >= rv) { res = i; break; }
       }
-      double Wn = W + ps;
-      if (ec + Wn >= rv) {
-        double part = 0.0;
-        for (int j = 0; j < 32; j++) {
-          double p = pref<R>(a, b + j);
-          if (p > thr) {
-            part += p;
-            if (ec + (W + part) >= rv) { res = b + j; found = true; break; }
-          }
-        }
-      }
-      W = Wn;
     }
     out[s] = res;
   }
@@ -659,38 +830,65 @@ cudaError_t launch_marginal_dist(const void* amp, int n, int prec, const Margina
   return prec == KET_C64 ? mdist_t<float>(amp, n, spec, partial, out, s) : mdist_t<double>(amp, n, spec, partial, out, s);
 }
 
+// Scratch layout of the sampler: nk + 1 checkpoints, then per block the
+// approximate prefix (nb + 1), the first and last kept index, D, the exact
+// start, the state and the binade; the state's first and last kept index.
+struct CdfScratch {
+  double* ck;
+  double* bsum;
+  unsigned long long* bfirst;
+  unsigned long long* blast;
+  long long* bd;
+  double* bstart;
+  int* bst;
+  int* be;
+  unsigned long long* fl;
+  size_t bytes;
+};
+static CdfScratch cdf_scratch(int n, void* base) {
+  const uint64_t N = uint64_t(1) << n;
+  const uint64_t nk = (N + kCdfSub - 1) / kCdfSub, nb = (N + kCdfBlock - 1) / kCdfBlock;
+  CdfScratch c;
+  char* p = (char*)base;
+  auto take = [&](size_t bytes) {
+    char* r = p;
+    p += (bytes + 255) & ~size_t(255);
+    return (void*)r;
+  };
+  c.ck = (double*)take(8 * (nk + 1));
+  c.bsum = (double*)take(8 * (nb + 1));
+  c.bfirst = (unsigned long long*)take(8 * nb);
+  c.blast = (unsigned long long*)take(8 * nb);
+  c.bd = (long long*)take(8 * nb);
+  c.bstart = (double*)take(8 * nb);
+  c.bst = (int*)take(4 * nb);
+  c.be = (int*)take(4 * nb);
+  c.fl = (unsigned long long*)take(16);
+  c.bytes = (size_t)(p - (char*)base);
+  return c;
+}
+
 template <typename R>
-static cudaError_t sample_t(const void* amp, int n, double thr, int seq_qubits, const double* r, uint64_t shots,
-                            void* scratch, uint64_t* out, cudaStream_t s) {
+static cudaError_t sample_t(const void* amp, int n, double thr, const double* r, uint64_t shots, void* scratch,
+                            uint64_t* out, cudaStream_t s) {
   const typename Vec2<R>::T* a = (const typename Vec2<R>::T*)amp;
   const uint64_t N = uint64_t(1) << n;
-  if (n <= seq_qubits || n < 10) {
-    double* cum = (double*)scratch;
-    uint64_t* last = (uint64_t*)(cum + N);
-    k_cdf_sequential<R><<<1, kCdfThreads, 0, s>>>(a, N, thr, cum, last);
-    k_sample_dense<<<gridn(shots, 256), 256, 0, s>>>(cum, N, r, shots, last, out);
-  } else {
-    const uint64_t nchunks = N / 1024;
-    double* cs = (double*)scratch;
-    uint64_t* lk = (uint64_t*)(cs + nchunks);
-    double* E = (double*)(lk + nchunks);
-    uint64_t* last = (uint64_t*)(E + nchunks + 1);
-    k_chunk_sums<R><<<(unsigned)((nchunks * 32 + 255) / 256), 256, 0, s>>>(a, nchunks, thr, cs, lk);
-    k_chunk_prefix<<<1, 32, 0, s>>>(cs, lk, nchunks, E, last);
-    k_sample_chunked<R><<<gridn(shots, 128), 128, 0, s>>>(a, E, nchunks, thr, r, shots, last, out);
-  }
+  const uint64_t nk = (N + kCdfSub - 1) / kCdfSub, nb = (N + kCdfBlock - 1) / kCdfBlock;
+  const CdfScratch c = cdf_scratch(n, scratch);
+  k_cdf_block_sums<R><<<(unsigned)nb, 256, 0, s>>>(a, N, thr, c.bsum, c.bfirst, c.blast);
+  k_cdf_block_prefix<<<1, kCdfThreads, 0, s>>>(c.bsum, c.bfirst, c.blast, nb, c.fl);
+  k_cdf_block_d<R><<<(unsigned)nb, 256, 0, s>>>(a, N, thr, c.bsum, (long long*)c.ck, c.bd, c.bst, c.be);
+  k_cdf_walk<R><<<1, kCdfThreads, 0, s>>>(a, N, thr, nb, nk, c.ck, c.bd, c.bst, c.be, c.bstart);
+  k_cdf_fill<<<gridn(nk, 256), 256, 0, s>>>(c.ck, nk, c.bst, c.be, c.bstart);
+  k_sample_ck<R><<<gridn(shots, 128), 128, 0, s>>>(a, N, thr, c.ck, nk, r, shots, c.fl, out);
   return cudaGetLastError();
 }
-size_t sample_scratch(int n, int seq_qubits) {
-  uint64_t N = uint64_t(1) << n;
-  if (n <= seq_qubits || n < 10) return 8 * N + 64;
-  uint64_t nc = N / 1024;
-  return 8 * (3 * nc + 8);
-}
-cudaError_t launch_sample(const void* amp, int n, int prec, double thr, int seq_qubits, const double* r, uint64_t shots,
-                          void* scratch, uint64_t* out, cudaStream_t s) {
-  return prec == KET_C64 ? sample_t<float>(amp, n, thr, seq_qubits, r, shots, scratch, out, s)
-                         : sample_t<double>(amp, n, thr, seq_qubits, r, shots, scratch, out, s);
+size_t sample_scratch(int n) { return cdf_scratch(n, nullptr).bytes; }
+int sample_launches() { return 6; }
+cudaError_t launch_sample(const void* amp, int n, int prec, double thr, const double* r, uint64_t shots, void* scratch,
+                          uint64_t* out, cudaStream_t s) {
+  return prec == KET_C64 ? sample_t<float>(amp, n, thr, r, shots, scratch, out, s)
+                         : sample_t<double>(amp, n, thr, r, shots, scratch, out, s);
 }
 
 cudaError_t launch_gather(const void* amp, int prec, const uint64_t* idx, uint64_t k, double* out, cudaStream_t s) {

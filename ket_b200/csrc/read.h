@@ -8,9 +8,6 @@
 
 namespace ket {
 
-// States with at most this many qubits build the sampling CDF as one running
-// FP64 sum in ascending index order -- the reference's exact summation order.
-#define KET_SEQ_CDF_QUBITS 20
 #define KET_MAX_MARGINAL_QUBITS 12
 #define KET_PAULI_GROUP_TERMS 64
 
@@ -43,11 +40,12 @@ cudaError_t launch_marginals(const void* amp, int n, int prec, double* partial, 
 int mdist_chunk_bits(int n, int m);
 cudaError_t launch_marginal_dist(const void* amp, int n, int prec, const MarginalSpec& spec, double* partial,
                                  double* out, cudaStream_t s);
-// Sampling: a sequential FP64 CDF in index order (the reference's order) for
-// n <= seq_qubits, chunk sums and a per-draw walk inside one chunk above
-// that (seq_qubits >= 10: a chunk is 1024 amplitudes).
-size_t sample_scratch(int n, int seq_qubits);
-cudaError_t launch_sample(const void* amp, int n, int prec, double thr, int seq_qubits, const double* r, uint64_t shots, void* scratch,
+// Sampling: the reference's running FP64 sum over kept entries in ascending
+// index order, bit for bit, kept as one checkpoint per 32 entries; each draw
+// (0 <= r <= 1) searches the checkpoints and adds inside one sub-chunk.
+size_t sample_scratch(int n);
+int sample_launches();
+cudaError_t launch_sample(const void* amp, int n, int prec, double thr, const double* r, uint64_t shots, void* scratch,
                           uint64_t* out, cudaStream_t s);
 cudaError_t launch_gather(const void* amp, int prec, const uint64_t* idx, uint64_t k, double* out, cudaStream_t s);
 cudaError_t launch_pauli_group(const void* amp, int n, int prec, const PauliGroup& g, double* partial, double* out,

@@ -15,9 +15,9 @@
 //   * the final readout is the sampling kernel with no probability
 //     threshold: sampleSV walks every entry of its Map, and the engine's
 //     pruned state holds exactly those entries as its nonzero amplitudes.
-//     One draw per shot does not pay for a whole sequential CDF, so above 12
-//     qubits the draw walks chunk sums and then one chunk; that order of
-//     additions differs from the sequential one only in rounding.
+//     The sampler's running sum is sampleSV's, ascending index order and
+//     rounding included; the in-shared-memory trajectories below walk chunk
+//     sums and then one chunk, which differs from it only in rounding.
 // The device state is the caller's ket_state, reset to |init> per shot.
 #include <algorithm>
 #include <cmath>
@@ -832,7 +832,7 @@ int ket_run_shots(ket_state* st, const ket_op* ops, size_t nops, const double* m
     // sampleSV (circuit.ts:75-83) then the readout flips (:3466-3470)
     const double r = R.draw();
     uint64_t idx = 0;
-    TRY(sample_indices(st, &r, 1, 0.0, 12, &idx));
+    TRY(sample_indices(st, &r, 1, 0.0, &idx));
     if (R.nz.pmeas != 0)
       for (int q = 0; q < st->n; q++)
         if (R.draw() < R.nz.pmeas) idx ^= uint64_t(1) << q;

@@ -192,3 +192,19 @@ def check_pershot(case, probs, cregs, clean=None):
             assert all(abs(v - clean.get(k, 0.0)) < chk[1] for k, v in probs.items()), (case["id"], probs, clean)
         else:
             raise AssertionError(f"unknown check {kind}")
+
+
+def reference_draws(amps, draws_at=None, rng_seed=0):
+    """Draws on and one ulp above the running sums, uniform draws, 0 and 1,
+    and the reference's answer to each: the first kept entry whose running
+    sum is >= r, the last kept entry's sum taken as 1.0."""
+    p = amps.real * amps.real + amps.imag * amps.imag
+    kept = np.nonzero(p > 1e-14)[0]
+    ck = np.cumsum(p[kept])                # ascending index order, rounded each step
+    ck[-1] = 1.0
+    cum = np.cumsum(np.where(p > 1e-14, p, 0.0))
+    idx = draws_at if draws_at is not None else np.arange(p.size)
+    r = np.concatenate([cum[idx], np.nextafter(cum[idx], np.inf), [0.0, 1.0],
+                        np.random.default_rng(rng_seed).random(4096)])
+    r = r[r <= 1.0]
+    return kept[np.searchsorted(ck, r, side="left")], r

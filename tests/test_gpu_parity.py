@@ -148,23 +148,17 @@ def test_readouts_dense_and_sparse_probs():
     assert abs(dst.norm2() - 1.0) < 1e-12
 
 
-def test_sampling_large_state_chunked_cdf():
-    """States above 2^20 use the chunked CDF: every shot lands where the exact
-    ascending-index running sum crosses r (up to summation rounding)."""
+def test_sampling_large_state_reference_order():
+    """A 25-qubit state: every shot equals the reference's, whose running sum
+    numpy's sequential cumsum reproduces bit for bit."""
     from ket_b200 import workloads as W
-    from ket_b200.circuit import prng_draws
-    kc, _ = W.brickwork_circuit(22, 12, 42)
+    from harness import reference_draws
+    kc, _ = W.brickwork_circuit(25, 6, 42)
     st = kc._state()
-    r = prng_draws(1234, 4096)
-    got = st.sample(r)
     a = st.amplitudes_dense()
-    p = a.real * a.real + a.imag * a.imag
-    p[p <= 1e-14] = 0.0
-    cum = np.cumsum(p)
-    want = np.searchsorted(cum, r, side="left")
-    bad = np.nonzero(got != want)[0]
-    for b in bad:  # only boundary cases within summation rounding may differ
-        assert abs(cum[min(want[b], got[b])] - r[b]) < 1e-11
+    sel = np.random.default_rng(25).integers(0, 1 << 25, 20000)
+    want, r = reference_draws(a, draws_at=sel, rng_seed=25)
+    assert np.array_equal(st.sample(r), want)
 
 
 def test_expectation_and_pauli_sum_vs_oracle():

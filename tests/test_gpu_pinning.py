@@ -173,16 +173,8 @@ def _sample_vs_numpy_cdf(n, amps, draws_at=None, rng_seed=0):
     from ket_b200.circuit import DeviceState
     st = DeviceState(n)
     st.set_amplitudes(amps)
-    p = amps.real * amps.real + amps.imag * amps.imag
-    kept = p > 1e-14
-    cum = np.cumsum(np.where(kept, p, 0.0))
-    last = np.nonzero(kept)[0][-1]
-    cum[last:] = 1.0
-    idx = draws_at if draws_at is not None else np.arange(1 << n)
-    r = np.concatenate([cum[idx], np.nextafter(cum[idx], np.inf),
-                        np.random.default_rng(rng_seed).random(4096) * cum[last - 1]])
-    r = r[r <= 1.0]
-    want = np.searchsorted(cum, r, side="left")
+    from harness import reference_draws
+    want, r = reference_draws(amps, draws_at, rng_seed)
     got = st.sample(r)
     assert np.array_equal(got, want)
 
@@ -201,7 +193,29 @@ def test_sequential_cdf_ties_and_binades():
     _sample_vs_numpy_cdf(n, a)
 
 
-@pytest.mark.parametrize("n", [10, 16, 20])
+def test_sampling_rejects_draws_outside_unit_interval():
+    from ket_b200.circuit import DeviceState
+    from ket_b200 import RangeError
+    st = DeviceState(4)
+    for bad in (-1e-300, 1.0000000000000002, float("nan")):
+        with pytest.raises(RangeError):
+            st.sample(np.array([0.5, bad]))
+
+
+def test_sequential_cdf_leading_zeros_and_single_entry():
+    """Nothing kept before the last entry (every draw, 0 included, lands on
+    it), and a block of zeros between two kept entries."""
+    n = 16
+    a = np.zeros(1 << n, dtype=np.complex128)
+    a[-1] = 1.0
+    _sample_vs_numpy_cdf(n, a, draws_at=np.array([0, 1 << 15, (1 << n) - 1]))
+    a[:] = 0.0
+    a[3] = 0.5 ** 0.5
+    a[(1 << n) - 5] = 0.5 ** 0.5
+    _sample_vs_numpy_cdf(n, a, draws_at=np.array([0, 3, 4, 1 << 15, (1 << n) - 5]))
+
+
+@pytest.mark.parametrize("n", [10, 16, 20, 24])
 def test_sequential_cdf_random_states(n):
     rng = np.random.default_rng(n)
     a = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
