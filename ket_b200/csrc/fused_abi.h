@@ -51,7 +51,8 @@ enum FOpType : uint8_t {
   FO_GRADM = 12,  // adjoint probe, D 2x2 on register bit a (ancilla on register bit 3)
   FO_GRADD = 13,  // adjoint probe, D = diag(m0, m1) on target a (register / thread / outside, see flags)
   FO_GRADM2 = 14, // adjoint probe, D 4x4 on tile bits a (MSB), b through shared memory; ancilla tile bit anc
-  FO_CONT = 15    // continuation record of the op before it (data only, never dispatched)
+  FO_CONT = 15,   // continuation record of the op before it (data only, never dispatched)
+  FO_PPOLY = 16   // phases of a run of controlled-phase gates (see below), followed by continuation records
 };
 
 // flags
@@ -84,6 +85,7 @@ enum FOpCode : uint8_t {
   OC_GRADM2 = 95,
   OC_X1S = 96,        // X on tile bit b with controls ctile, through shared memory (multi-controlled X)
   OC_CPHASE = 97,     // + A: 97..101, phase fan on register bit A
+  OC_PPOLY = 102,     // phases of a run of controlled-phase gates
   OC_NOP = 0xFF       // continuation record: dispatched as an op that does nothing
 };
 
@@ -98,8 +100,35 @@ enum FOpCode : uint8_t {
 // records 1.. hold the out-of-tile controls as (angle, global qubit mask)
 // double2 pairs, 19 per record.  The op's `lmask` field holds the number of
 // pairs and `ctile` the number of records.
+//
+// FO_PPOLY: a run of phase gates diag(1, p), |p| = 1, on any targets and with
+// any controls, where each gate's target and register-bit controls name at
+// most one register bit, merged into one op.  Term t multiplies the amplitude
+// in slot j of thread tid of the tile at ctx by p_t when (ctx & cm_t) ==
+// cm_t, (tid & tm_t) == tm_t and slot j has the term's register bit (if it
+// names one).  Terms are grouped by (register bit, tm); lane g of each warp
+// multiplies the phases of group g's terms that match the tile, in term
+// order, and every thread multiplies the group products whose tm it matches
+// into one factor per register bit (and one for groups without), which its
+// slots then take.  The op's m holds, as uint32, the number of groups of
+// each register bit (none first, then bit 0, 1, ...) and, from byte 32, one
+// descriptor {tm, number of terms, record, unused} per group (at most
+// KET_PPOLY_MAX_GROUPS); `lmask` is the number of groups, `b` the register
+// bits that some group names and `ctile` the number of records.  A group's
+// terms {double re, im; uint64 cm; uint64 unused} (32 bytes) fill records
+// from its own (`record` counts from the op: 1 is the first after it), 9 per
+// record after the record's 16-byte no-op header.
 enum : int {
-  KET_CPHASE_TERMS_PER_RECORD = 19
+  KET_CPHASE_TERMS_PER_RECORD = 19,
+  KET_PPOLY_TERMS_PER_RECORD = 9,
+  KET_PPOLY_MAX_GROUPS = 14
+};
+struct PPolyTerm {
+  double re, im;
+  uint64_t cm, unused;
+};
+struct PPolyGroup {
+  uint32_t tm, n, rec, unused;
 };
 
 struct FOp {
@@ -127,6 +156,8 @@ struct FOp {
   double m[32];
 };
 static_assert(sizeof(FOp) == 64 + 256, "FOp layout");
+static_assert(16 + KET_PPOLY_TERMS_PER_RECORD * sizeof(PPolyTerm) <= sizeof(FOp), "FO_PPOLY record");
+static_assert(32 + KET_PPOLY_MAX_GROUPS * sizeof(PPolyGroup) <= sizeof(FOp::m), "FO_PPOLY groups");
 
 // Byte offset of tile index i in the XOR-swizzled exchange buffer.  The map is
 // linear over GF(2), so the offset of a sum of disjoint bits is the XOR of

@@ -355,14 +355,18 @@ __device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][NS], const FOp* op, ui
   // record 0 after the op: H[0..7]; records 1..: (angle, mask) pairs; each
   // record's data starts after its 16-byte no-op header
   const double2* H = reinterpret_cast<const double2*>(reinterpret_cast<const char*>(op + 1) + 16);
+  // the out-of-tile angles: lane l adds terms l, l + 32, ...; then a warp sum
+  // (the whole warp runs this: the op has no thread-bit controls)
   double th0 = 0.0, thp = 0.0;
-  for (uint32_t i = 0; i < nterms; i++) {
+  for (uint32_t i = tid & 31; i < nterms; i += 32) {
     const uint32_t r = i / KET_CPHASE_TERMS_PER_RECORD, w = i - r * KET_CPHASE_TERMS_PER_RECORD;
     const double2 t = __ldg(reinterpret_cast<const double2*>(reinterpret_cast<const char*>(op + 2 + r) + 16) + w);
     const uint64_t mk = (uint64_t)__double_as_longlong(t.y);
     if (ctx0 & mk) th0 += t.x;
     if (pairq & mk) thp += t.x;
   }
+  th0 = warp_sum(th0);
+  if (TT > 1) thp = warp_sum(thp);
   const double2* mp = reinterpret_cast<const double2*>(op->m);
   // thread factor: H[s] for every thread-id bit s that is set
   double fr = 1.0, fi = 0.0;
@@ -386,6 +390,79 @@ __device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][NS], const FOp* op, ui
       const double2 tk = __ldg(mp + k);
       const R pr = (R)(tk.x * gr - tk.y * gi), pi = (R)(tk.x * gi + tk.y * gr);
       cmul_in<R>(x[t][j], pr, pi);
+    }
+  }
+}
+
+// FO_PPOLY: the phases of a run of controlled-phase gates (the layout is
+// described in fused_abi.h), for the TT tiles of a thread (the second at
+// ctx0 | pairq).  Lane g multiplies the phases of group g's terms that match
+// the tile; each thread then multiplies, per register bit, the products of
+// the groups whose thread mask it matches, and its slots take them.  The
+// whole warp runs this (no thread-bit controls on the op).
+template <typename R, int TT, int NS>
+__device__ __forceinline__ void phase_poly(cpx<R> (&x)[TT][NS], const FOp* op, uint64_t ctx0, uint64_t pairq,
+                                           int tid) {
+  const char* m = reinterpret_cast<const char*>(op->m);
+  const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(m));
+  const uint2 c1 = __ldg(reinterpret_cast<const uint2*>(m + 16));
+  const uint32_t cnt[KET_NR_MAX + 1] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y};
+  const uint32_t ngrp = __ldg(reinterpret_cast<const uint32_t*>(op) + 4);  // FOp::lmask
+  const int lane = tid & 31;
+  uint4 d = make_uint4(0u, 0u, 0u, 0u);  // this lane's group: {tm, terms, record}
+  if ((uint32_t)lane < ngrp) d = __ldg(reinterpret_cast<const uint4*>(m + 32) + lane);
+  // the group products for each tile
+  cpx<double> K[TT];
+#pragma unroll
+  for (int t = 0; t < TT; t++) {
+    K[t].re = 1.0;
+    K[t].im = 0.0;
+  }
+  {
+    const char* p = reinterpret_cast<const char*>(op + d.z) + 16;
+    uint32_t w = 0;
+    for (uint32_t k = 0; k < d.y; k++) {
+      const double2 ph = __ldg(reinterpret_cast<const double2*>(p));
+      const uint64_t cm = __ldg(reinterpret_cast<const unsigned long long*>(p + 16));
+#pragma unroll
+      for (int t = 0; t < TT; t++) {
+        const uint64_t ctx = ctx0 | (t ? pairq : 0);
+        if ((ctx & cm) == cm) cmul_in<double>(K[t], ph.x, ph.y);
+      }
+      if (++w == KET_PPOLY_TERMS_PER_RECORD) {
+        w = 0;
+        p += sizeof(FOp) - (KET_PPOLY_TERMS_PER_RECORD - 1) * sizeof(PPolyTerm);
+      } else {
+        p += sizeof(PPolyTerm);
+      }
+    }
+  }
+  uint32_t g = 0;
+#pragma unroll
+  for (int seg = 0; seg <= KET_NR_MAX; seg++) {
+    if (seg > 0 && (1 << (seg - 1)) >= NS) break;  // register bits beyond the slots name no group
+    if (cnt[seg] == 0) continue;
+    cpx<double> F[TT];
+#pragma unroll
+    for (int t = 0; t < TT; t++) {
+      F[t].re = 1.0;
+      F[t].im = 0.0;
+    }
+    for (uint32_t k = 0; k < cnt[seg]; k++, g++) {
+      const uint32_t tm = __shfl_sync(0xffffffffu, d.x, (int)g);
+#pragma unroll
+      for (int t = 0; t < TT; t++) {
+        const double kr = __shfl_sync(0xffffffffu, K[t].re, (int)g);
+        const double ki = __shfl_sync(0xffffffffu, K[t].im, (int)g);
+        if (((uint32_t)tid & tm) == tm) cmul_in<double>(F[t], kr, ki);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < TT; t++) {
+      const R fr = (R)F[t].re, fi = (R)F[t].im;
+#pragma unroll
+      for (int j = 0; j < NS; j++)
+        if (seg == 0 || ((j >> (seg - 1)) & 1)) cmul_in<R>(x[t][j], fr, fi);
     }
   }
 }

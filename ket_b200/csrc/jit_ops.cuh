@@ -304,6 +304,8 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
     constexpr int A = OPC - OC_CPHASE;
     const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(g) + 1);
     phase_fan<R, A, 1, NS>(reinterpret_cast<cpx<R>(&)[1][NS]>(x), g, h2.x, t.ctx0, 0, t.tid);
+  } else if constexpr (OPC == OC_PPOLY) {
+    phase_poly<R, 1, NS>(reinterpret_cast<cpx<R>(&)[1][NS]>(x), g, t.ctx0, 0, t.tid);
   } else if constexpr (OPC == OC_DIAGT || OPC == OC_DIAGX) {
     bool one;
     if constexpr (OPC == OC_DIAGT) one = (t.tid >> LA) & 1;

@@ -355,6 +355,126 @@ void merge_phase_fans(std::vector<FOp>& prog) {
   prog.swap(out);
 }
 
+// A phase gate diag(1, p) with |p| = 1 whose target and register-bit controls
+// name at most one register bit (rb: that bit, or -1).
+bool poly_member(const FOp& o, int& rb) {
+  if (!(o.flags & FOF_D0ONE)) return false;
+  if (o.type != FO_DIAGR && o.type != FO_DIAGT && o.type != FO_DIAGX) return false;
+  const double r2 = o.m[2] * o.m[2] + o.m[3] * o.m[3];
+  if (!(std::fabs(r2 - 1.0) <= 4e-16)) return false;
+  const uint32_t regs = o.creg | (o.type == FO_DIAGR ? 1u << o.a : 0u);
+  if (popc(regs) > 1) return false;
+  rb = regs ? __builtin_ctz(regs) : -1;
+  return true;
+}
+
+// Runs of at least this many phase gates become FO_PPOLY ops.
+constexpr size_t kPolyMinRun = 6;
+
+// One FO_PPOLY op and its records from prog[i, j), all poly members, whose
+// (register bit, tm) groups number at most KET_PPOLY_MAX_GROUPS.
+void emit_poly(const std::vector<FOp>& prog, size_t i, size_t j, std::vector<FOp>& out) {
+  struct Grp {
+    int rb;
+    uint32_t tm;
+    std::vector<PPolyTerm> terms;
+  };
+  std::vector<Grp> grps;
+  uint8_t used = 0;
+  for (size_t g = i; g < j; g++) {
+    const FOp& o = prog[g];
+    int rb;
+    poly_member(o, rb);
+    PPolyTerm t;
+    t.re = o.m[2];
+    t.im = o.m[3];
+    t.cm = o.cctx | (o.type == FO_DIAGX ? o.dg0 : 0);
+    t.unused = 0;
+    const uint32_t tm = o.cthr | (o.type == FO_DIAGT ? 1u << o.a : 0u);
+    Grp* G = nullptr;
+    for (auto& x : grps)
+      if (x.rb == rb && x.tm == tm) G = &x;
+    if (!G) {
+      grps.push_back({rb, tm, {}});
+      G = &grps.back();
+    }
+    G->terms.push_back(t);
+    if (rb >= 0) used |= (uint8_t)(1u << rb);
+  }
+  // groups of no register bit first, then bit 0, 1, ... (stable: first use)
+  std::stable_sort(grps.begin(), grps.end(), [](const Grp& a, const Grp& b) { return a.rb < b.rb; });
+  FOp f;
+  memset(&f, 0, sizeof(f));
+  f.type = FO_PPOLY;
+  f.d0 = f.d1 = -2;
+  f.b = used;
+  f.lmask = (uint32_t)grps.size();
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(f.m);
+  PPolyGroup* desc = reinterpret_cast<PPolyGroup*>(reinterpret_cast<unsigned char*>(f.m) + 32);
+  std::vector<FOp> recs;
+  for (size_t g = 0; g < grps.size(); g++) {
+    cnt[grps[g].rb + 1]++;
+    desc[g].tm = grps[g].tm;
+    desc[g].n = (uint32_t)grps[g].terms.size();
+    desc[g].rec = (uint32_t)recs.size() + 1;
+    desc[g].unused = 0;
+    for (size_t k = 0; k < grps[g].terms.size(); k++) {
+      if (k % KET_PPOLY_TERMS_PER_RECORD == 0) {
+        FOp c;
+        memset(&c, 0, sizeof(c));
+        c.opc = OC_NOP;
+        c.type = FO_CONT;
+        c.d0 = c.d1 = -2;
+        recs.push_back(c);
+      }
+      PPolyTerm* d = reinterpret_cast<PPolyTerm*>(reinterpret_cast<unsigned char*>(&recs.back()) + 16);
+      d[k % KET_PPOLY_TERMS_PER_RECORD] = grps[g].terms[k];
+    }
+  }
+  f.ctile = (uint32_t)recs.size();
+  out.push_back(f);
+  out.insert(out.end(), recs.begin(), recs.end());
+}
+
+// Merge runs of phase gates into FO_PPOLY ops.  All of them are diagonal, so
+// only the order in which a thread multiplies their phases changes.
+void merge_phase_polys(std::vector<FOp>& prog) {
+  std::vector<FOp> out;
+  out.reserve(prog.size());
+  size_t i = 0;
+  int rb;
+  while (i < prog.size()) {
+    size_t j = i;
+    while (j < prog.size() && poly_member(prog[j], rb)) j++;
+    if (j - i < kPolyMinRun) {
+      const size_t e = j > i ? j : i + 1;
+      for (size_t k = i; k < e; k++) out.push_back(prog[k]);
+      i = e;
+      continue;
+    }
+    // split where a piece would need more groups than an op holds
+    size_t s = i;
+    std::vector<std::pair<int, uint32_t>> keys;
+    for (size_t k = i; k <= j; k++) {
+      if (k < j) {
+        poly_member(prog[k], rb);
+        const FOp& o = prog[k];
+        const std::pair<int, uint32_t> key{rb, o.cthr | (o.type == FO_DIAGT ? 1u << o.a : 0u)};
+        if (std::find(keys.begin(), keys.end(), key) != keys.end()) continue;
+        if (keys.size() < KET_PPOLY_MAX_GROUPS) {
+          keys.push_back(key);
+          continue;
+        }
+        keys.assign(1, key);
+      }
+      emit_poly(prog, s, k, out);
+      s = k;
+    }
+    i = j;
+  }
+  prog.swap(out);
+}
+
 }  // namespace
 
 void assign_opcode(FOp& o) {
@@ -387,6 +507,7 @@ void assign_opcode(FOp& o) {
     case FO_GRADD: o.opc = OC_GRADD; break;
     case FO_GRADM2: o.opc = OC_GRADM2; break;
     case FO_CPHASE: o.opc = (uint8_t)(OC_CPHASE + o.a); break;
+    case FO_PPOLY: o.opc = OC_PPOLY; break;
     case FO_CONT: o.opc = OC_NOP; break;
     default: o.opc = 0xff; break;
   }
@@ -418,7 +539,10 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
     prog.push_back(make_exch(cur, precision));
   }
   for (int i = 0; i < NB; i++) store_pos[i] = (uint8_t)cur.pos[i];
-  if (g_anc_tb < 0) merge_phase_fans(prog);
+  if (g_anc_tb < 0) {
+    merge_phase_polys(prog);
+    merge_phase_fans(prog);
+  }
   for (FOp& o : prog) assign_opcode(o);
 }
 

@@ -66,10 +66,14 @@ const double* record_data(const std::vector<FOp>& prog, size_t k) {
   return reinterpret_cast<const double*>(reinterpret_cast<const unsigned char*>(&prog[k]) + 16);
 }
 
+// Ops of each FOpType in the programs emulated since the last reset.
+int64_t g_type_count[32];
+
 void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
   std::vector<FOp> prog;
   uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
   plan_program(plan, p, KET_C128, prunef, NR, prog, lp, sp);
+  for (const FOp& o : prog) g_type_count[o.type & 31]++;
   const int L = p.L;
   auto gq = [&](int tb) { return tb < L ? tb : p.hbits[tb - L]; };
   uint64_t S = (uint64_t(1) << L) - 1;
@@ -114,6 +118,33 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
             if (!((j >> op.a) & 1)) continue;
             const int k = ((j >> (op.a + 1)) << op.a) | (j & ((1 << op.a) - 1));
             x[t * NS + j] *= cx(op.m[2 * k], op.m[2 * k + 1]) * F;
+          }
+        }
+        oi += op.ctile;
+        continue;
+      }
+      if (op.type == FO_PPOLY) {
+        // group products over the matching terms, then per thread and register bit
+        const uint32_t* cnt = reinterpret_cast<const uint32_t*>(op.m);
+        const PPolyGroup* desc =
+            reinterpret_cast<const PPolyGroup*>(reinterpret_cast<const unsigned char*>(op.m) + 32);
+        std::vector<cx> K(op.lmask, cx(1.0, 0.0));
+        for (uint32_t g = 0; g < op.lmask; g++)
+          for (uint32_t k = 0; k < desc[g].n; k++) {
+            const size_t rec = desc[g].rec + k / KET_PPOLY_TERMS_PER_RECORD;
+            const PPolyTerm& tm =
+                reinterpret_cast<const PPolyTerm*>(record_data(prog, oi + rec))[k % KET_PPOLY_TERMS_PER_RECORD];
+            if ((ctx & tm.cm) == tm.cm) K[g] *= cx(tm.re, tm.im);
+          }
+        for (int t = 0; t < NTH; t++) {
+          uint32_t g = 0;
+          for (int seg = 0; seg <= KET_NR_MAX; seg++) {
+            if (!cnt[seg]) continue;
+            cx f(1.0, 0.0);
+            for (uint32_t k = 0; k < cnt[seg]; k++, g++)
+              if (((uint32_t)t & desc[g].tm) == desc[g].tm) f *= K[g];
+            for (int j = 0; j < NS; j++)
+              if (seg == 0 || ((j >> (seg - 1)) & 1)) x[t * NS + j] *= f;
           }
         }
         oi += op.ctile;
@@ -238,6 +269,7 @@ int emu_apply_nreg(int n, const ket_op* ops, size_t nops, const double* mats, si
   plan_passes(n, KET_C128, fusion, prune != 0, plan);
   cx* amp = reinterpret_cast<cx*>(re_im);
   passes[0] = passes[1] = 0;
+  memset(g_type_count, 0, sizeof g_type_count);
   for (const Pass& p : plan.passes) {
     if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) { passes[1]++; return -1; }
     run_pass(plan, p, n, prune != 0, amp);
@@ -245,6 +277,9 @@ int emu_apply_nreg(int n, const ket_op* ops, size_t nops, const double* mats, si
   }
   return 0;
 }
+
+// Ops of FOpType `type` in the programs of the last emu_apply call.
+int64_t emu_type_count(int type) { return g_type_count[type & 31]; }
 
 int emu_apply(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int prune, int fusion,
               double* re_im, int64_t* passes) {

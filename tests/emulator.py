@@ -29,8 +29,15 @@ def lib():
     L.emu_apply_nreg.restype = C.c_int
     L.emu_apply_nreg.argtypes = [C.c_int, C.POINTER(ket_op), C.c_size_t, C.POINTER(C.c_double), C.c_size_t, C.c_int,
                                  C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
+    L.emu_type_count.restype = C.c_int64
+    L.emu_type_count.argtypes = [C.c_int]
     _lib = L
     return L
+
+
+def type_count(fop_type):
+    """Ops of the given FOpType in the programs of the last emu_apply call."""
+    return lib().emu_type_count(fop_type)
 
 
 def emu_apply(n, ops, init_state, prune=True, fusion=-1, nreg=5):

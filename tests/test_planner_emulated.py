@@ -40,3 +40,26 @@ def test_emulated_brickwork_qft(n, nreg):
     oc, _ = O.brickwork(n, 8, 42, with_qft=True)
     assert rc == 0
     assert np.max(np.abs(got - oc.simulate(mode=O.DENSE).dense())) < 1e-12
+
+
+FO_CPHASE, FO_PPOLY = 11, 16
+
+
+@pytest.mark.parametrize("n", [14, 16])
+@pytest.mark.parametrize("nreg", [5, 4])
+def test_emulated_brickwork_qft_pruned_phase_runs(n, nreg):
+    """With pruning on, the QFT's runs of controlled phases become merged
+    phase ops (FO_PPOLY and FO_CPHASE); the result still equals the
+    reference algorithm with its per-gate pruning."""
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import flatten_ops
+    from emulator import type_count
+    from oracle import oracle as O
+    c, _ = W.brickwork_qft(n, 8, 42)
+    st0 = np.zeros(1 << n, complex)
+    st0[0] = 1
+    rc, got, passes = emu_apply(n, flatten_ops(c.ops), st0, prune=True, nreg=nreg)
+    assert rc == 0
+    assert type_count(FO_PPOLY) > 0
+    oc, _ = O.brickwork(n, 8, 42, with_qft=True)
+    assert np.max(np.abs(got - oc.simulate(mode=O.DENSE_PRUNE).dense())) < 1e-12
