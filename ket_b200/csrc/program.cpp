@@ -290,7 +290,11 @@ void merge_phase_fans(std::vector<FOp>& prog) {
   while (i < prog.size()) {
     size_t j = i;
     while (j < prog.size() && fan_member(prog[j]) && prog[j].a == prog[i].a) j++;
-    if (!fan_member(prog[i]) || j - i < 2) {
+    // phases whose control is a register bit run as cheap compiled ops of
+    // their own (4 of 16 slots each); a fan of only those costs more
+    bool other = false;
+    for (size_t k = i; k < j; k++) other = other || !prog[k].creg;
+    if (!fan_member(prog[i]) || j - i < 2 || (!other && j - i < 6)) {
       out.push_back(prog[i]);
       i++;
       continue;
@@ -436,30 +440,43 @@ void emit_poly(const std::vector<FOp>& prog, size_t i, size_t j, std::vector<FOp
   out.insert(out.end(), recs.begin(), recs.end());
 }
 
-// Merge runs of phase gates into FO_PPOLY ops.  All of them are diagonal, so
-// only the order in which a thread multiplies their phases changes.
+bool diagonal_op(const FOp& o) { return o.type == FO_DIAGR || o.type == FO_DIAGT || o.type == FO_DIAGX; }
+
+// Merge the phase gates of each run of diagonal ops into FO_PPOLY ops placed
+// first in the run, the run's other diagonal ops following in their order.
+// All of them are diagonal, so only the order in which a thread multiplies
+// their factors changes.
 void merge_phase_polys(std::vector<FOp>& prog) {
   std::vector<FOp> out;
   out.reserve(prog.size());
   size_t i = 0;
   int rb;
   while (i < prog.size()) {
-    size_t j = i;
-    while (j < prog.size() && poly_member(prog[j], rb)) j++;
-    if (j - i < kPolyMinRun) {
-      const size_t e = j > i ? j : i + 1;
-      for (size_t k = i; k < e; k++) out.push_back(prog[k]);
-      i = e;
+    if (!diagonal_op(prog[i])) {
+      out.push_back(prog[i]);
+      i++;
       continue;
     }
+    size_t j = i;
+    std::vector<size_t> mem, rest;
+    while (j < prog.size() && diagonal_op(prog[j])) {
+      (poly_member(prog[j], rb) ? mem : rest).push_back(j);
+      j++;
+    }
+    if (mem.size() < kPolyMinRun) {
+      for (size_t k = i; k < j; k++) out.push_back(prog[k]);
+      i = j;
+      continue;
+    }
+    std::vector<FOp> ms;
+    for (size_t k : mem) ms.push_back(prog[k]);
     // split where a piece would need more groups than an op holds
-    size_t s = i;
+    size_t s0 = 0;
     std::vector<std::pair<int, uint32_t>> keys;
-    for (size_t k = i; k <= j; k++) {
-      if (k < j) {
-        poly_member(prog[k], rb);
-        const FOp& o = prog[k];
-        const std::pair<int, uint32_t> key{rb, o.cthr | (o.type == FO_DIAGT ? 1u << o.a : 0u)};
+    for (size_t k = 0; k <= ms.size(); k++) {
+      if (k < ms.size()) {
+        poly_member(ms[k], rb);
+        const std::pair<int, uint32_t> key{rb, ms[k].cthr | (ms[k].type == FO_DIAGT ? 1u << ms[k].a : 0u)};
         if (std::find(keys.begin(), keys.end(), key) != keys.end()) continue;
         if (keys.size() < KET_PPOLY_MAX_GROUPS) {
           keys.push_back(key);
@@ -467,9 +484,10 @@ void merge_phase_polys(std::vector<FOp>& prog) {
         }
         keys.assign(1, key);
       }
-      emit_poly(prog, s, k, out);
-      s = k;
+      emit_poly(ms, s0, k, out);
+      s0 = k;
     }
+    for (size_t k : rest) out.push_back(prog[k]);
     i = j;
   }
   prog.swap(out);
