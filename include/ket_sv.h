@@ -220,7 +220,8 @@ KET_API int ket_plan_stats(int nqubits, int precision, const ket_op* ops, size_t
 
 /* Same, for the register-tiled passes: counts[t] = number of program ops of type t
  * (0 layout exchange, 1/2 2x2 on a register/lane bit, 3/4 X on a register/lane
- * bit, 5 register swap, 6 4x4, 7-10 diagonal forms, 11 merged phase fans), counts[12] / counts[13] =
+ * bit, 5 register swap, 6 4x4, 7-10 diagonal forms, 11 merged phase fans and
+ * phase polynomials), counts[12] / counts[13] =
  * 2x2 ops with a general / a real or Rx-like matrix, counts[14] = tiled passes,
  * counts[15] = other passes.  Programs use the register bits a run with these
  * options would (opts->reg_bits, else the automatic choice for nqubits).  No

@@ -377,7 +377,8 @@ int ket_plan_program_stats(int n, int precision, const ket_op* ops, size_t nops,
     uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
     plan_program(plan, p, precision, o.prune != 0, tiled_nreg(n, o.reg_bits), prog, lp, sp);
     for (const FOp& f : prog) {
-      if (f.type != FO_CONT) counts[f.type]++;
+      if (f.type == FO_PPOLY) counts[FO_CPHASE]++;  // merged phase ops share one count
+      else if (f.type <= FO_CPHASE) counts[f.type]++;  // probes (12-14) never occur here
       if (f.type == FO_MAT1R || f.type == FO_MAT1L) counts[(f.flags & (FOF_REAL | FOF_RXFORM)) ? 13 : 12]++;
     }
     counts[14]++;

@@ -198,6 +198,24 @@ def test_planner_pass_counts_on_the_bench_workload():
         assert out[1] == 0 and out[2] <= k
 
 
+def test_program_statistics_stay_in_their_array():
+    """ket_plan_program_stats on the 30-qubit bench circuit writes its 16 counts
+    and nothing past them, whatever op types the programs hold (the QFT's
+    phase polynomials included)."""
+    c, _ = W.brickwork_qft(30, 40, 42)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    mv = np.ascontiguousarray(m).view(np.float64)
+    for reg_bits in (4, 5):
+        o = _lib.exec_opts(prune=True, specialize=1, reg_bits=reg_bits)
+        buf = (C.c_int64 * 24)(*([-7] * 24))
+        _lib.check(_lib.lib().ket_plan_program_stats(30, 0, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)),
+                                                     m.size, C.byref(o), buf))
+        assert list(buf)[16:] == [-7] * 8
+        assert buf[14] == 106 and buf[15] == 0
+        assert buf[11] > 0  # phase fans and phase polynomials of the QFT
+        assert buf[12] + buf[13] == buf[1] + buf[2]  # every 2x2 op has one matrix form
+
+
 def test_planner_statistics():
     c, _ = W.brickwork_circuit(16, 20, 42)
     fused = plan(c)
