@@ -10,6 +10,7 @@
 // of each warp touch contiguous 128-byte lines.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "launch.h"
@@ -493,6 +494,96 @@ void merge_phase_polys(std::vector<FOp>& prog) {
   prog.swap(out);
 }
 
+// Deferred register swaps (FOF_SW, fused_abi.h), for the compiled kernels:
+// an X on a register bit under thread or out-of-tile controls becomes a
+// per-thread flag, and the ops after it read the flag where they can (a 2x2
+// or general diagonal on that bit exchanges its matrix entries; exchanges,
+// shared-memory ops and the store address the logical slots).  Where an op
+// needs the register slots in logical order -- register controls on a
+// swapped bit, a phase on one, merged phase ops, and a lane op whose partner
+// lanes could disagree (a swap decided by a control on that lane bit) --
+// FO_REAL carries the pending swaps out first.
+void defer_swaps(std::vector<FOp>& prog) {
+  const int nr = NRg();
+  uint32_t pend = 0;               // register bits with pending swaps
+  uint32_t src[KET_NR_MAX] = {};   // per register bit: thread-id bits of the controls that decided them (bit 8: outside the tile)
+  std::vector<FOp> out;
+  out.reserve(prog.size() + 8);
+  auto clear = [&]() {
+    pend = 0;
+    for (int k = 0; k < nr; k++) src[k] = 0;
+  };
+  auto realize = [&](uint32_t m) {
+    m &= pend;
+    if (!m) return;
+    FOp r;
+    memset(&r, 0, sizeof(r));
+    r.type = FO_REAL;
+    r.creg = (uint8_t)m;
+    r.d0 = r.d1 = -2;
+    r.lmask = 0xffffffffu;
+    out.push_back(r);
+    pend &= ~m;
+    for (int k = 0; k < nr; k++)
+      if ((m >> k) & 1) src[k] = 0;
+  };
+  for (const FOp& in : prog) {
+    FOp o = in;
+    switch (o.type) {
+      case FO_CONT:  // the records of the op before: kept right after it
+        break;
+      case FO_EXCH: case FO_SWAPS: case FO_MAT2S: case FO_DIAG:
+        clear();  // written out through the logical slots
+        break;
+      case FO_X1R: {
+        if (!o.creg) {
+          if (o.cthr || o.cctx) {
+            o.flags |= FOF_SW;
+            pend |= 1u << o.a;
+            src[o.a] |= o.cthr | (o.cctx ? 0x100u : 0u);
+          }  // uncontrolled: a renaming, which commutes with the pending swaps
+        } else if (!(o.creg & (o.creg - 1)) && !o.cthr && !o.cctx) {
+          const int c = __builtin_ctz(o.creg);
+          if ((pend >> c) & 1) {
+            o.flags |= FOF_SW;
+            pend |= 1u << o.a;
+            src[o.a] |= src[c];
+          }
+        } else {
+          clear();  // the shared-memory form (several controls)
+        }
+        break;
+      }
+      case FO_MAT1R:
+        realize(o.creg);
+        if ((pend >> o.a) & 1) o.flags |= FOF_SW;
+        break;
+      case FO_DIAGR:
+        realize(o.creg);
+        if ((pend >> o.a) & 1) {
+          if (o.flags & FOF_D0ONE) realize(1u << o.a);
+          else o.flags |= FOF_SW;
+        }
+        break;
+      case FO_MAT1L: case FO_X1L: {
+        uint32_t m = o.creg;
+        for (int k = 0; k < nr; k++)
+          if ((src[k] >> o.a) & 1) m |= 1u << k;
+        realize(m);
+        break;
+      }
+      case FO_DIAGT: case FO_DIAGX:
+        realize(o.creg);
+        break;
+      default:  // merged phase ops and anything else
+        realize(pend);
+        break;
+    }
+    out.push_back(o);
+  }
+  prog.swap(out);  // the store takes what is still pending
+}
+
 }  // namespace
 
 void assign_opcode(FOp& o) {
@@ -526,16 +617,175 @@ void assign_opcode(FOp& o) {
     case FO_GRADM2: o.opc = OC_GRADM2; break;
     case FO_CPHASE: o.opc = (uint8_t)(OC_CPHASE + o.a); break;
     case FO_PPOLY: o.opc = OC_PPOLY; break;
+    case FO_REAL: o.opc = OC_REAL; break;
     case FO_CONT: o.opc = OC_NOP; break;
     default: o.opc = 0xff; break;
   }
 }
+
+namespace {
+
+// Estimated cost, in milliseconds per op on a 2^30-amplitude complex128 state,
+// of the program's ops by kind and placement.  Fitted to the event-timed
+// passes of the 30-qubit brickwork step (compiled kernels, 4 register bits):
+// a 2x2 on a register bit about 0.6 (general matrices more, real and Rx-like
+// less), the same on a lane bit about 0.25 more (its shuffles), an X on a lane
+// bit 0.4, an X on a register bit under a thread or out-of-tile control 0.22
+// (conditional register moves; uncontrolled or register-controlled, a
+// renaming), a diagonal 0.16, a layout exchange 0.45.
+constexpr double kCostExch = 0.45;
+
+double mat_form_cost(const Gate& g) {
+  bool real = true;
+  for (int k = 0; k < 4; k++) real = real && g.m[k].im == 0.0;
+  const bool rx = g.m[0].im == 0.0 && g.m[3].im == 0.0 && g.m[1].re == 0.0 && g.m[2].re == 0.0;
+  return real || rx ? 0.5 : 0.75;
+}
+
+double gate_cost(const Gate& g, const Pass& p, const Lay& l) {
+  switch (g.type) {
+    case G_MAT1: return mat_form_cost(g) + (is_lane(l, tpos(p, g.t0)) ? 0.25 : 0.0);
+    case G_X1: {
+      if (is_lane(l, tpos(p, g.t0))) return 0.4;
+      int nreg = 0;
+      bool other = false;
+      for (int q = 0; q < 64; q++) {
+        if (!((g.cmask >> q) & 1)) continue;
+        const int t = tpos(p, q);
+        if (t >= 0 && is_reg(l, t)) nreg++;
+        else other = true;
+      }
+      if (nreg == 0) return other ? 0.22 : 0.0;
+      if (nreg == 1 && !other) return 0.0;
+      return 2 * kCostExch;  // several controls with one on a register bit: a shared-memory op
+    }
+    case G_DIAG1: return 0.16;
+    default: return 2 * kCostExch;  // shared-memory ops: the same in every layout
+  }
+}
+
+bool same_lay(const Lay& a, const Lay& b) { return memcmp(a.pos, b.pos, sizeof a.pos) == 0; }
+
+// Layouts of a pass by dynamic programming over where to exchange.  Candidate
+// layouts at gate i are the look-ahead layouts from i (one keeping the
+// store's lanes, one not); the load layout is any lane-keeping candidate.
+// The cheapest sequence of runs and exchanges under gate_cost, with the
+// restore to a lane-keeping layout at the end, wins.  lay[i] is the layout
+// gate i runs in.  False when no sequence fits (the caller falls back to the
+// greedy rule).
+bool plan_layouts(const Plan& plan, const Pass& p, int precision, std::vector<Lay>& lay) {
+  const size_t G = p.gates.size();
+  std::vector<std::vector<Lay>> cand(G + 1);
+  for (size_t i = 0; i <= G; i++) {
+    for (int a0 = 1; a0 >= 0; a0--) {
+      const Lay l = choose(plan, p, i, a0 != 0, precision);
+      bool dup = false;
+      for (const Lay& c : cand[i]) dup = dup || same_lay(c, l);
+      if (!dup) cand[i].push_back(l);
+    }
+  }
+  struct St {
+    Lay l;
+    double cost;
+    int from;   // index of the state it came from (in the previous position's list), -1 at the start
+    bool exch;  // entered by an exchange at this position
+  };
+  std::vector<std::vector<St>> at(G + 1);  // states in effect before gate i (after any exchange at i)
+  // starting layouts: every lane-keeping candidate
+  for (size_t i = 0; i <= G; i++)
+    for (const Lay& c : cand[i]) {
+      if (!a0_compatible(c)) continue;
+      bool dup = false;
+      for (const St& s : at[0]) dup = dup || same_lay(s.l, c);
+      if (!dup) at[0].push_back({c, 0.0, -1, false});
+    }
+  std::vector<std::vector<St>> run(G + 1);  // states arriving at i by running gate i-1 (or the start)
+  run[0] = at[0];
+  at[0].clear();
+  auto relax = [](std::vector<St>& v, const St& s) {
+    for (St& o : v)
+      if (same_lay(o.l, s.l)) {
+        if (s.cost < o.cost) o = s;
+        return;
+      }
+    v.push_back(s);
+  };
+  for (size_t i = 0; i <= G; i++) {
+    // stay, or exchange to a candidate
+    for (size_t k = 0; k < run[i].size(); k++) {
+      St s = run[i][k];
+      s.from = (int)k;
+      s.exch = false;
+      relax(at[i], s);
+    }
+    for (size_t k = 0; k < run[i].size(); k++)
+      for (const Lay& c : cand[i]) {
+        if (same_lay(c, run[i][k].l)) continue;
+        if (i < G && !fits(plan.gates[p.gates[i]], p, c)) continue;
+        if (i == G && !a0_compatible(c)) continue;
+        relax(at[i], {c, run[i][k].cost + kCostExch, (int)k, true});
+      }
+    if (i == G) break;
+    const Gate& g = plan.gates[p.gates[i]];
+    for (size_t k = 0; k < at[i].size(); k++) {
+      const St& s = at[i][k];
+      if (!fits(g, p, s.l)) continue;
+      relax(run[i + 1], {s.l, s.cost + gate_cost(g, p, s.l), (int)k, false});
+    }
+    if (run[i + 1].empty()) return false;
+  }
+  // the end: the store needs the lanes kept (a restore exchange otherwise)
+  int best = -1;
+  double bc = 0;
+  for (size_t k = 0; k < at[G].size(); k++) {
+    const St& s = at[G][k];
+    if (!a0_compatible(s.l)) continue;
+    if (best < 0 || s.cost < bc) { best = (int)k; bc = s.cost; }
+  }
+  if (best < 0) return false;
+  // walk back: at[i][k] came from run[i][from]; run[i][k] came from at[i-1][from]
+  lay.assign(G + 1, Lay());
+  int k = best;
+  for (size_t i = G + 1; i-- > 0;) {
+    const St& s = at[i][k];
+    lay[i] = s.l;
+    const int r = s.from;  // index in run[i]
+    if (i == 0) break;
+    k = run[i][r].from;    // index in at[i-1]
+  }
+  return true;
+}
+
+}  // namespace
 
 void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, int nreg, std::vector<FOp>& prog,
                   uint8_t load_pos[KET_T2_BITS], uint8_t store_pos[KET_T2_BITS]) {
   prog.clear();
   g_nreg = nreg;
   g_anc_tb = plan.anc >= 0 ? tpos(p, plan.anc) : -1;
+  std::vector<Lay> lay;
+  if (g_anc_tb < 0 && !getenv("KET_GREEDY_LAYOUT") && plan_layouts(plan, p, precision, lay)) {
+    // lay[i]: the layout gate i runs in; lay[G]: the store layout
+    Lay cur = lay[0];
+    for (int i = 0; i < NB; i++) load_pos[i] = (uint8_t)cur.pos[i];
+    for (size_t i = 0; i < p.gates.size(); i++) {
+      if (!same_lay(lay[i], cur)) {
+        cur = lay[i];
+        prog.push_back(make_exch(cur, precision));
+      }
+      prog.push_back(make_op(plan.gates[p.gates[i]], p, cur, prune));
+    }
+    if (!same_lay(lay[p.gates.size()], cur)) {
+      cur = lay[p.gates.size()];
+      prog.push_back(make_exch(cur, precision));
+    }
+    for (int i = 0; i < NB; i++) store_pos[i] = (uint8_t)cur.pos[i];
+    merge_phase_polys(prog);
+    merge_phase_fans(prog);
+    if (getenv("KET_DEFER")) defer_swaps(prog);
+    for (FOp& o : prog) assign_opcode(o);
+    return;
+  }
   Lay cur = choose(plan, p, 0, true, precision);
   for (int i = 0; i < NB; i++) load_pos[i] = (uint8_t)cur.pos[i];
   for (size_t i = 0; i < p.gates.size(); i++) {

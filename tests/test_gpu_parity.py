@@ -226,17 +226,25 @@ def test_invalid_ops_leave_state_untouched():
 @pytest.mark.parametrize("n", [21, 22, 24, 26])
 def test_fused_equals_unfused_many_tiles(n):
     """States with many tiles per CTA (the persistent loop's later iterations):
-    the fused passes give the unfused per-gate result, run twice (a race would
-    show up as a difference between runs)."""
+    the fused passes give the unfused per-gate result, run twice on each form
+    of the pass (a race would show up as a difference between runs).  Each
+    form is pinned: under the default policy a pass of a 26+ qubit state runs
+    on the interpreter until its compiled kernel is ready, and the two forms
+    agree to rounding only where merged phase ops are present."""
     from ket_b200 import workloads as W
     from ket_b200.circuit import DeviceState, flatten_ops, ops_to_abi
     c, _ = W.brickwork_qft(n, 10, 42)
     arr, m, k = ops_to_abi(flatten_ops(c.ops))
-    res = []
-    for fusion in (-1, -1, 0):
-        st = DeviceState(n)
-        st.apply_abi(arr, m, k, fusion=fusion, prune=False)
-        res.append(st.amplitudes_dense())
-        del st
-    assert np.max(np.abs(res[0] - res[2])) < 1e-13
-    assert np.array_equal(res[0], res[1])
+    st = DeviceState(n)
+    st.apply_abi(arr, m, k, fusion=0, prune=False)
+    unfused = st.amplitudes_dense()
+    del st
+    for specialize in (-1, 1):
+        res = []
+        for _ in range(2):
+            st = DeviceState(n)
+            st.apply_abi(arr, m, k, fusion=-1, prune=False, specialize=specialize)
+            res.append(st.amplitudes_dense())
+            del st
+        assert np.max(np.abs(res[0] - unfused)) < 1e-13, specialize
+        assert np.array_equal(res[0], res[1]), specialize
