@@ -102,7 +102,8 @@ typedef struct ket_exec_opts {
                           that the programs large states run can be checked on small ones.  The
                           interpreter always uses 5.  No counterpart in the reference. */
   int32_t stage;       /* compiled kernels' tile loads: 1 = staged in shared memory by TMA copies
-                          (one CTA per SM, a copy warp keeps the next tiles in flight), -1 = loads
+                          (one CTA per SM: two tile groups, each tile's copy issued while the
+                          tile before it computes), -1 = loads
                           into registers (two CTAs per SM), 0 = automatic.  Results are identical
                           either way.  No counterpart in the reference. */
   int32_t reserved[3];
@@ -164,8 +165,8 @@ KET_API int ket_debug_batch_hook(int drop_item, uint32_t spin_limit);
  * spare -- the default).  No counterpart in the reference. */
 KET_API int ket_debug_adjoint_budget(int64_t device_bytes);
 /* Test hook for the bounded waits of the staged pass kernels
- * (ket_exec_opts.stage = 1): tile >= 0 makes each such kernel's copy warp skip
- * the copies of that tile, so the tile threads' wait for it runs out (about
+ * (ket_exec_opts.stage = 1): tile >= 0 makes each such kernel skip the copies
+ * of that tile, so the tile group's wait for it runs out (about
  * two seconds) and the call returns KET_ERR_TIMEOUT with the context still
  * usable; -1 disables.  No counterpart in the reference. */
 KET_API int ket_debug_stage_drop(int64_t tile);

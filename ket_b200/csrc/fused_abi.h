@@ -52,7 +52,10 @@ enum FOpType : uint8_t {
   FO_GRADD = 13,  // adjoint probe, D = diag(m0, m1) on target a (register / thread / outside, see flags)
   FO_GRADM2 = 14, // adjoint probe, D 4x4 on tile bits a (MSB), b through shared memory; ancilla tile bit anc
   FO_CONT = 15,   // continuation record of the op before it (data only, never dispatched)
-  FO_PPOLY = 16   // phases of a run of controlled-phase gates (see below), followed by continuation records
+  FO_PPOLY = 16,  // phases of a run of controlled-phase gates (see below), followed by continuation records
+  FO_REAL = 17,   // compiled kernels: carry out the deferred register swaps of the register bits in creg (see FOF_SW)
+  FO_RELAY = 18   // an uncontrolled swap of two tile bits as a relabelling: the layout pos (as FO_EXCH's) takes
+                  // effect with no data moved
 };
 
 // flags
@@ -60,6 +63,18 @@ enum FOpType : uint8_t {
 #define FOF_REAL 2u     // MAT1: every matrix entry is real
 #define FOF_D0ONE 4u    // DIAG*: m0 == 1 exactly (only bit-1 amplitudes change)
 #define FOF_RXFORM 8u   // MAT1: m00, m11 real and m01, m10 imaginary (Rx-like)
+// FOF_SW: deferred register swaps (compiled kernels only; the interpreter and
+// the emulator carry every swap out at once and ignore it).  An X on register
+// bit a under thread or out-of-tile controls only records, per thread, that
+// the slot pairs along a are exchanged (sw ^= 1 << a) instead of moving them;
+// physical slot j then holds logical slot j ^ sw.  FOF_SW on such an X marks
+// it deferred; on an X controlled by one register bit C it adds that the
+// thread's sw bit C moves to a as well; on a 2x2 or a diagonal on register
+// bit a it makes the op exchange its matrix rows and columns (its d0 and d1)
+// where the thread's sw bit a is set.  Exchanges, shared-memory ops and the
+// store address the logical slots, which clears sw; FO_REAL carries out the
+// pending swaps where an op needs the logical order in registers.
+#define FOF_SW 16u
 #define FOF_TGT_THR 32u // FO_GRADD: target is a thread-id bit (a)
 #define FOF_TGT_CTX 64u // FO_GRADD: target is outside the tile (mask dg0)
 
@@ -86,6 +101,8 @@ enum FOpCode : uint8_t {
   OC_X1S = 96,        // X on tile bit b with controls ctile, through shared memory (multi-controlled X)
   OC_CPHASE = 97,     // + A: 97..101, phase fan on register bit A
   OC_PPOLY = 102,     // phases of a run of controlled-phase gates
+  OC_REAL = 103,      // FO_REAL: carry out the deferred swaps of the register bits in creg (compiled kernels)
+  OC_RELAY = 104,     // FO_RELAY: the new layout's exchange offsets, no data moved
   OC_NOP = 0xFF       // continuation record: dispatched as an op that does nothing
 };
 
@@ -186,7 +203,7 @@ struct Pass2Args {
   uint64_t lgb[KET_T2_BITS];       // byte offset in the state of each role's tile bit, load layout
   uint64_t sgb[KET_T2_BITS];       // same, store layout
   uint32_t lbx[KET_T2_BITS];       // exchange-buffer offset of each role's tile bit, load layout
-  int64_t drop_tile;               // staged form, test hook: the copy lane skips this tile (-1 = none)
+  int64_t drop_tile;               // staged form, test hook: this tile's copies are skipped (-1 = none)
 };
 
 }  // namespace ket

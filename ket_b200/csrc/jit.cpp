@@ -185,8 +185,9 @@ int static_lane(const FOp& f) {
   return (f.opc >= OC_MAT1L && f.opc < OC_MAT1L + 3) || f.opc == OC_X1L || f.opc == OC_DIAGT ? f.a : 0;
 }
 
-// Stages of the staged form: 3 tiles of 64 KB (complex128) or 6 of 32 KB.
-int stage_count(int precision) { return precision == KET_C64 ? 6 : 3; }
+// Stages of the staged form: one per tile group and one in flight (64 KB
+// each at complex128, 32 KB at complex64).
+int stage_count(int) { return 3; }
 
 // A program with adjoint probes: its kernel keeps per-CTA probe sums.
 bool has_probes(const FOp* prog, int nops) {
@@ -204,7 +205,7 @@ std::string make_source(const FOp* prog, int nops, int precision, int NR, bool s
   s += "#include \"jit_ops.cuh\"\n";
   s += "__constant__ ket::jit::COp c_ops[" + std::to_string(nops > 0 ? nops : 1) + "];\n";
   if (staged) {
-    s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(NT + 32) +
+    s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(2 * NT) +
          ", 1) ket_pass(const ket::Pass2Args a, const __grid_constant__ ket::jit::TMap tm) {\n";
   } else {
     s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(NT) +
@@ -216,15 +217,15 @@ std::string make_source(const FOp* prog, int nops, int precision, int NR, bool s
   if (staged)
     s += std::string("  jit::run_tiles_staged<") + R + ", " + std::to_string(NR) + ", " +
          std::to_string(stage_count(precision)) + ">(a, &tm, [&](cpx<" + R + "> (&x)[" + std::to_string(1 << NR) +
-         "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
+         "], SLay<" + std::to_string(NR) + ">& sl, jit::Tile& t) {\n";
   else
     s += std::string("  jit::run_tiles<") + R + ", " + std::to_string(NR) +
          (has_probes(prog, nops) ? ", true" : ", false") + ">(a, [&](cpx<" + R + "> (&x)[" + std::to_string(1 << NR) +
-         "], SLay<" + std::to_string(NR) + ">& sl, const jit::Tile& t) {\n";
+         "], SLay<" + std::to_string(NR) + ">& sl, jit::Tile& t) {\n";
   for (int k = 0; k < nops; k++) {
     const FOp& f = prog[k];
     if (f.type == FO_CONT || f.opc == OC_NOP) continue;
-    const unsigned fl = f.flags & (FOF_PRUNE | FOF_D0ONE);
+    const unsigned fl = f.flags & (FOF_PRUNE | FOF_D0ONE | FOF_SW);
     s += std::string("    jit::step<") + R + ", " + std::to_string(NR) + ", " + std::to_string((int)f.opc) + ", " +
          std::to_string(fl) + ", " + std::to_string((int)f.creg) + ", " + std::to_string((unsigned)f.cthr) + "u, " +
          (f.cctx ? "true" : "false") + ", " + std::to_string(static_lane(f)) + ">(x, sl, c_ops[" + std::to_string(k) +
@@ -244,7 +245,7 @@ std::string shape_key(const FOp* prog, int nops, int precision, int nreg, bool s
       k += '.';
       continue;
     }
-    const unsigned fl = f.flags & (FOF_PRUNE | FOF_D0ONE);
+    const unsigned fl = f.flags & (FOF_PRUNE | FOF_D0ONE | FOF_SW);
     char buf[32];
     snprintf(buf, sizeof buf, "%x,%x,%x,%x,%d,%d;", (unsigned)f.opc, fl, (unsigned)f.creg, (unsigned)f.cthr,
              f.cctx ? 1 : 0, static_lane(f));
@@ -551,13 +552,13 @@ cudaError_t jit_launch(const JitFn& f, const Pass2Args& in, int precision, cudaS
   const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
   CUresult r;
   if (f.staged) {
-    // one CTA per SM: the tile's threads plus the copy warp
+    // one CTA per SM: two tile groups
     jit::TMap tm;
     if (!encode_tile_map(a, precision, tm)) return cudaErrorInvalidValue;
     a.drop_tile = g_stage_drop;
     const unsigned blocks = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)num_sms());
     void* params[2] = {&a, &tm};
-    r = driver().launch((CUfunction)f.fn, blocks, 1, 1, (32 << (7 - a.nreg)) + 32, 1, 1, smem, (CUstream)s, params,
+    r = driver().launch((CUfunction)f.fn, blocks, 1, 1, 2 * (32 << (7 - a.nreg)), 1, 1, smem, (CUstream)s, params,
                         nullptr);
   } else {
     // two CTAs per SM at either register-bit count (__launch_bounds__(NT, 2));

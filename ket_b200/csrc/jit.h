@@ -42,7 +42,7 @@ int tiled_nreg(int nqubits, int reg_bits = 0);
 #define KET_JIT_MAX_PROBES 512
 
 struct JitFn {
-  bool staged = false;              // the staged form (one CTA per SM, TMA copy warp)
+  bool staged = false;              // the staged form (one CTA per SM, two tile groups, TMA copies)
   bool grad = false;                // an adjoint probe pass
   void* fn = nullptr;               // CUfunction, null = run the interpreter
   unsigned long long cops = 0;      // device address of the kernel's constant op array

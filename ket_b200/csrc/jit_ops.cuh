@@ -23,17 +23,6 @@
 namespace ket {
 namespace jit {
 
-// The barrier among the threads that hold a tile.  In the staged form
-// (KET_STAGED_THREADS defined: the tile's threads plus one copy warp) only the
-// tile's threads take part, on named barrier 1; otherwise the whole CTA.
-__device__ __forceinline__ void tile_sync() {
-#ifdef KET_STAGED_THREADS
-  asm volatile("bar.sync 1, %0;" ::"n"(KET_STAGED_THREADS) : "memory");
-#else
-  __syncthreads();
-#endif
-}
-
 template <int NS>
 __host__ __device__ constexpr uint32_t slotmask(int creg) {
   uint32_t v = 0;
@@ -91,11 +80,55 @@ struct Tile {
   int tid, lane, warp;
   uint64_t ctx0;  // global index bits of the tile outside its 12 bits
   double* sgrad;  // adjoint probe passes: the CTA's partial sums [slot][warp] in shared memory
+  uint32_t sw;    // deferred register swaps (FOF_SW): physical slot j holds logical slot j ^ sw
+  uint32_t bar;   // staged form: the named barrier of the tile's thread group
 };
+
+// The barrier among the threads that hold a tile.  In the staged form
+// (KET_STAGED_THREADS defined: a CTA of two tile groups of that many threads)
+// only the tile's group takes part, on its named barrier; otherwise the whole
+// CTA.
+__device__ __forceinline__ void tile_sync(const Tile& t) {
+#ifdef KET_STAGED_THREADS
+  asm volatile("bar.sync %0, %1;" ::"r"(t.bar), "n"(KET_STAGED_THREADS) : "memory");
+#else
+  (void)t;
+  __syncthreads();
+#endif
+}
+
+// The layout sl as seen from the logical slots: slot j's amplitude, held in
+// physical slot j ^ sw, goes to the exchange-buffer address of logical slot j.
+template <int NR>
+__device__ __forceinline__ SLay<NR> logical_slay(const SLay<NR>& sl, uint32_t sw) {
+  SLay<NR> w = sl;
+#pragma unroll
+  for (int k = 0; k < NR; k++)
+    if ((sw >> k) & 1) w.b ^= sl.s[k];
+  return w;
+}
+
+// Carry out the deferred swaps of register bits M (a compile-time mask).
+template <typename R, int NR, int M>
+__device__ __forceinline__ void realize_swaps(cpx<R> (&x)[1 << NR], Tile& t) {
+#pragma unroll
+  for (int k = 0; k < NR; k++) {
+    if (!((M >> k) & 1)) continue;
+    const bool s = (t.sw >> k) & 1;
+#pragma unroll
+    for (int j = 0; j < (1 << NR); j++) {
+      if (j & (1 << k)) continue;
+      const cpx<R> a = x[j], b = x[j | (1 << k)];
+      x[j] = sel<R>(s, b, a);
+      x[j | (1 << k)] = sel<R>(s, a, b);
+    }
+  }
+  t.sw &= ~(uint32_t)M;
+}
 
 // Rare ops on the shared-memory copy of the tile, as in k_fused2.
 template <typename R, int NR, int OPC, int FL>
-__device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl, const FOp* op, const Tile& t) {
+__device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl, const FOp* op, Tile& t) {
   constexpr int NT = 32 << (7 - NR);
   constexpr double thr = 1e-14, qthr = 1e-7;
   const uint4 h = __ldg(reinterpret_cast<const uint4*>(op));
@@ -104,9 +137,10 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
   const int oa = (h.x >> 8) & 0xff, ob = (int)(h2.w & 0xffu);
   const double* M = op->m;
   const uint32_t smb = t.smb;
-  tile_sync();
-  write_tile<R, NR>(smb, sl, x);
-  tile_sync();
+  tile_sync(t);
+  write_tile<R, NR>(smb, logical_slay<NR>(sl, t.sw), x);
+  t.sw = 0;
+  tile_sync(t);
   if constexpr (OPC == OC_GRADM2) {
     // Re<lambda| D |psi> with D 4x4 on tile bits a (MSB), b; the ancilla tile
     // bit selects psi (0) / lambda (1).  Read-only: the registers keep the tile.
@@ -193,7 +227,7 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
       }
     }
   }
-  tile_sync();
+  tile_sync(t);
   read_tile<R, NR>(smb, sl, x);
 }
 
@@ -203,15 +237,24 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
 // c: the op's constant copy; g: the op in the global copy of the program.
 template <typename R, int NR, int OPC, int FL, int CREG, uint32_t CTHR, bool CCTX, int LA>
 __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const COp& c, const FOp* g,
-                                     const Tile& t) {
+                                     Tile& t) {
   constexpr int NS = 1 << NR;
   constexpr double thr = 1e-14, qthr = 1e-7;
   if constexpr (OPC == OC_EXCH) {
-    tile_sync();
-    write_tile<R, NR>(t.smb, sl, x);
-    tile_sync();
+    tile_sync(t);
+    write_tile<R, NR>(t.smb, logical_slay<NR>(sl, t.sw), x);
+    t.sw = 0;
+    tile_sync(t);
     sl = exch_slay_c<NR>(c, t.lane, t.warp);
     read_tile<R, NR>(t.smb, sl, x);
+    return;
+  }
+  if constexpr (OPC == OC_REAL) {
+    realize_swaps<R, NR, CREG>(x, t);
+    return;
+  }
+  if constexpr (OPC == OC_RELAY) {  // a relabelling swap: the data stays, the layout changes
+    sl = exch_slay_c<NR>(c, t.lane, t.warp);
     return;
   }
   if constexpr (CCTX) {
@@ -254,8 +297,17 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   constexpr uint32_t SM = slotmask<NS>(CREG);
   if constexpr (OPC >= OC_MAT1R && OPC < OC_MAT1R + 15) {
     constexpr int A = (OPC - OC_MAT1R) / 3, F = (OPC - OC_MAT1R) % 3;
-    const R m[8] = {(R)c.m[0], (R)c.m[1], (R)c.m[2], (R)c.m[3], (R)c.m[4], (R)c.m[5], (R)c.m[6], (R)c.m[7]};
-    mat1_reg<R, A, F, NS>(x, m, SM);
+    if constexpr ((FL & FOF_SW) != 0) {
+      // slot pairs along A exchanged in this thread: rows and columns of the matrix too
+      const bool s = (t.sw >> A) & 1;
+      const R m[8] = {(R)(s ? c.m[6] : c.m[0]), (R)(s ? c.m[7] : c.m[1]), (R)(s ? c.m[4] : c.m[2]),
+                      (R)(s ? c.m[5] : c.m[3]), (R)(s ? c.m[2] : c.m[4]), (R)(s ? c.m[3] : c.m[5]),
+                      (R)(s ? c.m[0] : c.m[6]), (R)(s ? c.m[1] : c.m[7])};
+      mat1_reg<R, A, F, NS>(x, m, SM);
+    } else {
+      const R m[8] = {(R)c.m[0], (R)c.m[1], (R)c.m[2], (R)c.m[3], (R)c.m[4], (R)c.m[5], (R)c.m[6], (R)c.m[7]};
+      mat1_reg<R, A, F, NS>(x, m, SM);
+    }
   } else if constexpr (OPC >= OC_MAT1L && OPC < OC_MAT1L + 3) {
     const uint32_t members = c.lmask;
     const bool bitv = (t.lane >> LA) & 1;
@@ -280,6 +332,10 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
     }
   } else if constexpr (OPC >= OC_X1R && OPC < OC_X1R + 5) {
     constexpr int A = OPC - OC_X1R;
+    if constexpr ((FL & FOF_SW) != 0) {
+      t.sw ^= 1u << A;  // deferred: this thread passed the op's controls
+      return;
+    }
 #pragma unroll
     for (int j = 0; j < NS; j++)
       if (!(j & (1 << A)) && ((SM >> j) & 1)) swp<R>(x[j], x[j | (1 << A)]);
@@ -288,6 +344,9 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
 #pragma unroll
     for (int j = 0; j < NS; j++)
       if (!(j & (1 << A)) && (j & (1 << C))) swp<R>(x[j], x[j | (1 << A)]);
+    // a deferred swap on the control bit: the pairs whose logical control
+    // bit is 1 are the other half, which flipping every pair along A adds
+    if constexpr ((FL & FOF_SW) != 0) t.sw ^= ((t.sw >> C) & 1u) << A;
   } else if constexpr (OPC == OC_X1L) {
     const uint32_t members = c.lmask;
 #pragma unroll
@@ -296,7 +355,13 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   } else if constexpr ((OPC >= OC_DIAGR && OPC < OC_DIAGR + 5) || (OPC >= OC_DIAGR1 && OPC < OC_DIAGR1 + 5)) {
     constexpr bool ONE = OPC >= OC_DIAGR1;
     constexpr int A = OPC - (ONE ? OC_DIAGR1 : OC_DIAGR);
-    diag_reg<R, A, ONE, NS>(x, (R)c.m[0], (R)c.m[1], (R)c.m[2], (R)c.m[3], SM);
+    if constexpr ((FL & FOF_SW) != 0 && !ONE) {
+      const bool s = (t.sw >> A) & 1;
+      diag_reg<R, A, ONE, NS>(x, (R)(s ? c.m[2] : c.m[0]), (R)(s ? c.m[3] : c.m[1]), (R)(s ? c.m[0] : c.m[2]),
+                              (R)(s ? c.m[1] : c.m[3]), SM);
+    } else {
+      diag_reg<R, A, ONE, NS>(x, (R)c.m[0], (R)c.m[1], (R)c.m[2], (R)c.m[3], SM);
+    }
   } else if constexpr (OPC >= OC_DIAGR1C && OPC < OC_DIAGR1C + 25) {
     constexpr int A = (OPC - OC_DIAGR1C) / 5, C = (OPC - OC_DIAGR1C) % 5;
     diag1c_reg<R, A, C, NS>(x, (R)c.m[2], (R)c.m[3]);
@@ -315,11 +380,37 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   } else {
     // handled above (the exchange and the shared-memory ops return early)
     static_assert(OPC == OC_NOP || OPC == OC_EXCH || OPC == OC_SWAPS || OPC == OC_MAT2S || OPC == OC_DIAG ||
-                      OPC == OC_X1S || (OPC >= OC_GRADM && OPC <= OC_GRADM2),
+                      OPC == OC_X1S || OPC == OC_REAL || OPC == OC_RELAY || (OPC >= OC_GRADM && OPC <= OC_GRADM2),
                   "op code without a compiled form");
     return;
   }
   if constexpr ((FL & FOF_PRUNE) != 0) prune_slots<R, NS>(x, thr, qthr);
+}
+
+// ---------------------------------------------------------------- store
+// Store the tile: physical slot j holds logical slot j ^ t.sw, which goes to
+// the address of the logical slot.  With a register bit k swapped, bit k of
+// the address offset is taken where the physical slot's bit k is clear: the
+// base gains that bit's offset and the slot's own term turns negative
+// (unsigned arithmetic, exact modulo 2^64).
+template <typename R, int NR>
+__device__ __forceinline__ void store_tile(char* p, const uint64_t* rb, uint32_t sw, const cpx<R> (&x)[1 << NR]) {
+  typedef typename Vec2<R>::T V;
+  uint64_t sk[NR];
+#pragma unroll
+  for (int k = 0; k < NR; k++) {
+    const bool s = (sw >> k) & 1;
+    if (s) p += rb[k];
+    sk[k] = s ? (uint64_t)0 - rb[k] : rb[k];
+  }
+#pragma unroll
+  for (int j = 0; j < (1 << NR); j++) {
+    uint64_t o = 0;
+#pragma unroll
+    for (int k = 0; k < NR; k++)
+      if (j & (1 << k)) o += sk[k];
+    st_amp<R>(reinterpret_cast<V*>(p + o), x[j]);
+  }
 }
 
 // The tile loop around a program: load each tile in the load layout, run the
@@ -372,18 +463,9 @@ __device__ __forceinline__ void run_tiles(const Pass2Args& a, Body body) {
       }
     }
     SLay<NR> sl = make_slay<NR>(a.lbx, t.lane, t.warp);
+    t.sw = 0;
     body(x, sl, t);
-    {
-      char* p = amp + t.ctx0 * sizeof(V) + gs;
-#pragma unroll
-      for (int j = 0; j < NS; j++) {
-        uint64_t o = 0;
-#pragma unroll
-        for (int k = 0; k < NR; k++)
-          if (j & (1 << k)) o += a.sgb[5 + NW + k];
-        st_amp<R>(reinterpret_cast<V*>(p + o), x[j]);
-      }
-    }
+    store_tile<R, NR>(amp + t.ctx0 * sizeof(V) + gs, a.sgb + 5 + NW, t.sw, x);
   }
   if constexpr (GRAD) {
     __syncthreads();
@@ -393,24 +475,31 @@ __device__ __forceinline__ void run_tiles(const Pass2Args& a, Body body) {
 
 // ---------------------------------------------------------------- staged tile loop
 // The same pass with every tile staged in shared memory by the tensor-memory
-// accelerator.  One CTA per SM: NT tile threads plus one copy warp whose lane
-// 0 keeps NSTAGE tiles in flight.  A tile lands in shared memory in its
-// natural order -- byte offset = tile index x amplitude size, tile bits 0-4
-// the 5 contiguous low qubits, bits 5-11 the pass's high qubits -- as 128
-// boxes of a 2-D tensor map over the state, {the 2^5 amplitudes of a row (as
-// 2 x 32 reals), rows}: box j is the row at the tile's context plus the high
-// qubits set in j.
+// accelerator.  One CTA per SM runs two tile groups of NT threads (16 warps
+// at 4 register bits, as the register-load form's two CTAs) over NSTAGE
+// stages: the CTA's k-th tile lands in stage k % NSTAGE and group k % 2 runs
+// it, so while both groups compute, the next tile is already on its way.  A
+// tile lands in its natural order -- byte offset = tile index x amplitude
+// size, tile bits 0-4 the 5 contiguous low qubits, bits 5-11 the pass's high
+// qubits -- as 128 boxes of a 2-D tensor map over the state, {the 2^5
+// amplitudes of a row (as 2 x 32 reals), rows}: box j is the row at the
+// tile's context plus the high qubits set in j.
 //
-// Per tile and stage s: the copy lane waits for `empty[s]` (the tile threads
-// released the stage), arms `full[s]` with the tile's byte count and issues
-// the boxes; the tile threads wait for `full[s]`, read the tile into
-// registers in the load layout, run the ops -- exchanges and shared-memory
-// ops use the stage itself as their buffer -- release the stage (after a
-// proxy fence, since the next copy into it comes from the async proxy) and
-// store their registers straight to the state.  Every wait is bounded in
-// time: past KET_STAGE_WAIT_NS the status word gets KET_ERR_TIMEOUT, the tile
-// threads (all together, by a barrier vote) stop, and the copy lane waits
-// for its copies in flight before the CTA exits.
+// Per tile k in stage s: the group waits until the copy of tile k has been
+// issued (a per-stage count in shared memory: the mbarrier's phase parity
+// alone cannot tell tile k from tile k - NSTAGE when the group runs ahead of
+// the other one) and for `full[s]`, reads the tile into
+// registers in the load layout, runs the ops -- exchanges and shared-memory
+// ops use the stage itself as their buffer, on the group's own named barrier
+// -- then every thread fences its shared-memory writes against the async
+// proxy, the group meets at its barrier, and the group's first warp arms
+// `full[s]` with the byte count of tile k + NSTAGE and issues its boxes (4 per
+// lane) before the group stores its registers straight to the state.  The
+// stage's next user is the other group, which waits for `full[s]` again.
+// Every wait is bounded in time: past KET_STAGE_WAIT_NS the status word gets
+// KET_ERR_TIMEOUT, the group (all together, by a barrier vote) stops, and
+// before the CTA exits thread 0 waits for the last copy issued into every
+// stage.
 struct __align__(64) TMap {
   unsigned long long w[16];
 };
@@ -426,9 +515,6 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 }
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t ok;
@@ -453,6 +539,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (global_ns() - t0 > KET_STAGE_WAIT_NS) return false;
   return true;
 }
+// Wait until *p >= want (a count another warp of the CTA raises); false once
+// KET_STAGE_WAIT_NS has passed without it.
+__device__ __forceinline__ bool wait_count(const uint32_t* p, uint32_t want) {
+  const volatile uint32_t* v = p;
+  if (*v >= want) return true;
+  const uint64_t t0 = global_ns();
+  while (*v < want)
+    if (global_ns() - t0 > KET_STAGE_WAIT_NS) return false;
+  return true;
+}
 __device__ __forceinline__ void tma_load2(uint32_t dst, const TMap* m, int row, uint32_t bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
@@ -460,25 +556,30 @@ __device__ __forceinline__ void tma_load2(uint32_t dst, const TMap* m, int row, 
       "l"((unsigned long long)m), "r"(0), "r"(row), "r"(bar)
       : "memory");
 }
-// AND of v over the NT tile threads (named barrier 1).
+// AND of v over the NT threads of the group on named barrier `bar`.
 template <int NT>
-__device__ __forceinline__ bool all_tile_threads(bool v) {
+__device__ __forceinline__ bool all_group_threads(bool v, uint32_t bar) {
   uint32_t r;
-  asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}"
+  asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred p, %2, %3, q;\n selp.u32 %0, 1, 0, p;\n}"
                : "=r"(r)
-               : "r"((uint32_t)v), "n"(NT)
+               : "r"((uint32_t)v), "r"(bar), "n"(NT)
                : "memory");
   return r != 0;
 }
 
 template <typename R, int NR, int NSTAGE, typename Body>
 __device__ __forceinline__ void run_tiles_staged(const Pass2Args& a, const TMap* tm, Body body) {
-  constexpr int NW = 7 - NR, NS = 1 << NR, NT = 32 << NW;
+  constexpr int NW = 7 - NR, NS = 1 << NR, NT = 32 << NW;  // NT: threads of one tile group
+  constexpr int NG = 2;                                      // tile groups per CTA
+  static_assert(NSTAGE > NG, "a stage in flight beside each group's");
   typedef typename Vec2<R>::T V;
   constexpr uint32_t TB = (uint32_t)sizeof(V) << KET_T2_BITS;  // bytes per tile
+  constexpr int nbox = 1 << (KET_T2_BITS - 5);                 // one box per row of 2^5 amplitudes
+  constexpr uint32_t boxb = TB / (uint32_t)nbox;
   extern __shared__ __align__(1024) unsigned char smraw[];
   const uint32_t sm0 = (uint32_t)__cvta_generic_to_shared(smraw);
-  const uint32_t full0 = sm0 + NSTAGE * TB, empty0 = full0 + 8 * NSTAGE;
+  const uint32_t full0 = sm0 + NSTAGE * TB;
+  uint32_t* const issued = reinterpret_cast<uint32_t*>(smraw + NSTAGE * TB + 8 * NSTAGE);  // fills per stage
   const int tid = threadIdx.x;
   if (sm0 & 1023u) {  // the copies need aligned stages: refuse rather than misalign
     if (tid == 0) atomicExch(a.status, kStageMisaligned);
@@ -487,48 +588,41 @@ __device__ __forceinline__ void run_tiles_staged(const Pass2Args& a, const TMap*
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; s++) {
       mbar_init(full0 + 8 * s, 1);
-      mbar_init(empty0 + 8 * s, NT / 32);
+      *(volatile uint32_t*)(issued + s) = 0;
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
   const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
-  if (tid >= NT) {
-    // ---- copy lane
-    if (tid != NT) return;
-    constexpr int nbox = 1 << (KET_T2_BITS - 5);  // one box per row of 2^5 amplitudes
-    constexpr uint32_t boxb = TB / (uint32_t)nbox;
-    uint32_t k = 0;
-    bool ok = true;
-    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
-      const uint32_t s = k % NSTAGE;
-      if (k >= NSTAGE && !mbar_wait(empty0 + 8 * s, ((k / NSTAGE) - 1) & 1)) {
-        ok = false;
-        break;
-      }
-      if ((int64_t)tile == a.drop_tile) continue;  // test hook: the tile threads' wait for it runs out
-      const uint64_t ctx0 = ctx_of(a, tile);
-      mbar_expect_tx(full0 + 8 * s, TB);
-      for (int j = 0; j < nbox; j++) {
-        uint64_t idx = ctx0;
-#pragma unroll
-        for (int e = 0; e < KET_T2_BITS - 5; e++)
-          if ((j >> e) & 1) idx |= uint64_t(1) << a.hbits[e];
-        tma_load2(sm0 + s * TB + (uint32_t)j * boxb, tm, (int)(idx >> 5), full0 + 8 * s);
-      }
-    }
-    if (!ok) atomicExch(a.status, kStageTimeout);
-    // every copy in flight lands before the CTA may exit
-    for (uint32_t kk = k > NSTAGE ? k - NSTAGE : 0; kk < k; kk++)
-      if (!mbar_wait(full0 + 8 * (kk % NSTAGE), (kk / NSTAGE) & 1)) atomicExch(a.status, kStageTimeout);
-    return;
-  }
-  // ---- tile threads
+  const uint32_t nk = ntiles > blockIdx.x ? (uint32_t)((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0u;
+  const int grp = tid / NT;
   Tile t;
-  t.tid = tid;
-  t.lane = tid & 31;
-  t.warp = tid >> 5;
+  t.tid = tid - grp * NT;
+  t.lane = t.tid & 31;
+  t.warp = t.tid >> 5;
+  t.bar = 1 + grp;
+  // the CTA's k-th tile into stage k % NSTAGE, by one whole warp (4 boxes a lane)
+  auto fill = [&](uint32_t k) {
+    const uint32_t s = k % NSTAGE;
+    const uint64_t tile = blockIdx.x + (uint64_t)k * gridDim.x;
+    if ((int64_t)tile == a.drop_tile) return;  // test hook: the group's wait for it runs out
+    const uint64_t ctx0 = ctx_of(a, tile);
+    if (t.lane == 0) {
+      *(volatile uint32_t*)(issued + s) = k / NSTAGE + 1;
+      mbar_expect_tx(full0 + 8 * s, TB);
+    }
+    __syncwarp();
+    for (int j = t.lane; j < nbox; j += 32) {
+      uint64_t idx = ctx0;
+#pragma unroll
+      for (int e = 0; e < KET_T2_BITS - 5; e++)
+        if ((j >> e) & 1) idx |= uint64_t(1) << a.hbits[e];
+      tma_load2(sm0 + s * TB + (uint32_t)j * boxb, tm, (int)(idx >> 5), full0 + 8 * s);
+    }
+  };
+  if (grp == 0 && t.warp == 0)
+    for (uint32_t k = 0; k < nk && k < (uint32_t)NSTAGE; k++) fill(k);
   char* const amp = reinterpret_cast<char*>(a.amp);
   uint64_t gs = 0;
 #pragma unroll
@@ -543,31 +637,32 @@ __device__ __forceinline__ void run_tiles_staged(const Pass2Args& a, const TMap*
   for (int r = 0; r < KET_T2_BITS; r++) nbx[r] = (uint32_t)sizeof(V) << a.load_pos[r];
   const SLay<NR> nat = make_slay<NR>(nbx, t.lane, t.warp);
   cpx<R> x[NS];
-  uint32_t k = 0;
-  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
+  for (uint32_t k = grp; k < nk; k += NG) {
     const uint32_t s = k % NSTAGE;
-    if (!all_tile_threads<NT>(mbar_wait(full0 + 8 * s, (k / NSTAGE) & 1))) {
-      if (tid == 0) atomicExch(a.status, kStageTimeout);
+    const bool landed = wait_count(issued + s, k / NSTAGE + 1) && mbar_wait(full0 + 8 * s, (k / NSTAGE) & 1);
+    if (!all_group_threads<NT>(landed, t.bar)) {
+      if (t.tid == 0) atomicExch(a.status, kStageTimeout);
       break;
     }
+    const uint64_t tile = blockIdx.x + (uint64_t)k * gridDim.x;
     t.ctx0 = ctx_of(a, tile);
     t.smb = sm0 + s * TB;
     read_tile<R, NR>(t.smb, nat, x);
     SLay<NR> sl = make_slay<NR>(a.lbx, t.lane, t.warp);
+    t.sw = 0;
     body(x, sl, t);
+    // the stage is free once every thread of the group is past its last
+    // shared-memory access; its next copy comes from the async proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncwarp();
-    if (t.lane == 0) mbar_arrive(empty0 + 8 * s);
-    char* p = amp + t.ctx0 * sizeof(V) + gs;
-#pragma unroll
-    for (int j = 0; j < NS; j++) {
-      uint64_t o = 0;
-#pragma unroll
-      for (int q = 0; q < NR; q++)
-        if (j & (1 << q)) o += a.sgb[5 + NW + q];
-      st_amp<R>(reinterpret_cast<V*>(p + o), x[j]);
-    }
+    tile_sync(t);
+    if (t.warp == 0 && k + NSTAGE < nk) fill(k + NSTAGE);
+    store_tile<R, NR>(amp + t.ctx0 * sizeof(V) + gs, a.sgb + 5 + NW, t.sw, x);
   }
+  // no copy may still be landing when the CTA exits
+  __syncthreads();
+  if (tid == 0)
+    for (int s = 0; s < NSTAGE; s++)
+      if (issued[s] && !mbar_wait(full0 + 8 * s, (issued[s] - 1) & 1)) atomicExch(a.status, kStageTimeout);
 }
 
 }  // namespace jit

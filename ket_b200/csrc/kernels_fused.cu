@@ -108,6 +108,10 @@ __global__ void __launch_bounds__(32 << (7 - NR), NR == 5 ? 2 : 1) k_fused2(Pass
         for (int t = 0; t < TT; t++) read_tile<R, NR>(smb + t * TB, sl, x[t]);
         continue;
       }
+      if (opc == OC_RELAY) {  // a relabelling swap: the data stays, the layout changes
+        sl = exch_slay<NR>(op, lane, warp);
+        continue;
+      }
       const uint64_t cctx = ((uint64_t)h.w << 32) | h.z;
       if ((ctx0 & cctx) != cctx) continue;  // uniform over the CTA (and the same for all TT tiles)
       const double* M = op->m;

@@ -56,6 +56,12 @@ int tpos(const Pass& p, int q) {
 bool needs_two_regs(const Gate&) { return false; }
 
 thread_local int g_anc_tb = -1;  // tile bit of the adjoint ancilla in the pass being lowered
+thread_local bool g_relabel = false;  // uncontrolled swaps of two tile bits become relabellings (FO_RELAY)
+
+// An uncontrolled swap of two qubits of the tile: a relabelling of the layout.
+bool relabel_gate(const Gate& g, const Pass& p) {
+  return g_relabel && g.type == G_SWAP && g.cmask == 0 && tpos(p, g.t0) >= 0 && tpos(p, g.t1) >= 0;
+}
 
 bool fits(const Gate& g, const Pass& p, const Lay& l) {
   switch (g.type) {
@@ -79,6 +85,7 @@ Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision)
   for (size_t i = from; i < p.gates.size(); i++) {
     const Gate& g = plan.gates[p.gates[i]];
     if (g.type == G_DIAG1 || g.type == G_DIAG2 || g.type == G_GRADD || g.type == G_GRADM2) continue;
+    if (relabel_gate(g, p)) continue;  // needs no role
     int ts[2] = {tpos(p, g.t0), g.type == G_SWAP || g.type == G_MAT2 ? tpos(p, g.t1) : -1};
     for (int t : ts) {
       if (t < 0) continue;
@@ -137,6 +144,17 @@ Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision)
   for (int i = 0; i < NRg(); i++) l.pos[REG0() + i] = regs[i];
   fill_roles(l);
   return l;
+}
+
+// l with tile bits a and b exchanged: where the data stays after swapping them.
+Lay relabeled(const Lay& l, int a, int b) {
+  Lay r = l;
+  for (int i = 0; i < NB; i++) {
+    if (r.pos[i] == a) r.pos[i] = b;
+    else if (r.pos[i] == b) r.pos[i] = a;
+  }
+  fill_roles(r);
+  return r;
 }
 
 FOp make_exch(const Lay& l, int precision) {
@@ -531,6 +549,7 @@ void defer_swaps(std::vector<FOp>& prog) {
     FOp o = in;
     switch (o.type) {
       case FO_CONT:  // the records of the op before: kept right after it
+      case FO_RELAY:  // no data moves
         break;
       case FO_EXCH: case FO_SWAPS: case FO_MAT2S: case FO_DIAG:
         clear();  // written out through the logical slots
@@ -618,6 +637,7 @@ void assign_opcode(FOp& o) {
     case FO_CPHASE: o.opc = (uint8_t)(OC_CPHASE + o.a); break;
     case FO_PPOLY: o.opc = OC_PPOLY; break;
     case FO_REAL: o.opc = OC_REAL; break;
+    case FO_RELAY: o.opc = OC_RELAY; break;
     case FO_CONT: o.opc = OC_NOP; break;
     default: o.opc = 0xff; break;
   }
@@ -727,8 +747,13 @@ bool plan_layouts(const Plan& plan, const Pass& p, int precision, std::vector<La
       }
     if (i == G) break;
     const Gate& g = plan.gates[p.gates[i]];
+    const bool rel = relabel_gate(g, p);
     for (size_t k = 0; k < at[i].size(); k++) {
       const St& s = at[i][k];
+      if (rel) {
+        relax(run[i + 1], {relabeled(s.l, tpos(p, g.t0), tpos(p, g.t1)), s.cost, (int)k, false});
+        continue;
+      }
       if (!fits(g, p, s.l)) continue;
       relax(run[i + 1], {s.l, s.cost + gate_cost(g, p, s.l), (int)k, false});
     }
@@ -764,7 +789,9 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
   g_nreg = nreg;
   g_anc_tb = plan.anc >= 0 ? tpos(p, plan.anc) : -1;
   std::vector<Lay> lay;
-  if (g_anc_tb < 0 && !getenv("KET_GREEDY_LAYOUT") && plan_layouts(plan, p, precision, lay)) {
+  const bool dp = g_anc_tb < 0 && !getenv("KET_GREEDY_LAYOUT");
+  g_relabel = dp && getenv("KET_RELABEL");
+  if (dp && plan_layouts(plan, p, precision, lay)) {
     // lay[i]: the layout gate i runs in; lay[G]: the store layout
     Lay cur = lay[0];
     for (int i = 0; i < NB; i++) load_pos[i] = (uint8_t)cur.pos[i];
@@ -773,7 +800,15 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
         cur = lay[i];
         prog.push_back(make_exch(cur, precision));
       }
-      prog.push_back(make_op(plan.gates[p.gates[i]], p, cur, prune));
+      const Gate& g = plan.gates[p.gates[i]];
+      if (relabel_gate(g, p)) {
+        cur = relabeled(cur, tpos(p, g.t0), tpos(p, g.t1));
+        FOp r = make_exch(cur, precision);
+        r.type = FO_RELAY;
+        prog.push_back(r);
+        continue;
+      }
+      prog.push_back(make_op(g, p, cur, prune));
     }
     if (!same_lay(lay[p.gates.size()], cur)) {
       cur = lay[p.gates.size()];
@@ -782,10 +817,12 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
     for (int i = 0; i < NB; i++) store_pos[i] = (uint8_t)cur.pos[i];
     merge_phase_polys(prog);
     merge_phase_fans(prog);
-    if (getenv("KET_DEFER")) defer_swaps(prog);
+    if (!getenv("KET_NO_DEFER")) defer_swaps(prog);
     for (FOp& o : prog) assign_opcode(o);
+    g_relabel = false;
     return;
   }
+  g_relabel = false;
   Lay cur = choose(plan, p, 0, true, precision);
   for (int i = 0; i < NB; i++) load_pos[i] = (uint8_t)cur.pos[i];
   for (size_t i = 0; i < p.gates.size(); i++) {

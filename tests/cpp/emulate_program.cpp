@@ -68,12 +68,20 @@ const double* record_data(const std::vector<FOp>& prog, size_t k) {
 
 // Ops of each FOpType in the programs emulated since the last reset.
 int64_t g_type_count[32];
+// 1: emulate the compiled kernels' deferred register swaps (FOF_SW, FO_REAL:
+// physical slot j of thread t holds logical slot j ^ sw[t]); 0: the
+// interpreter's, which carries every swap out at once and ignores both.
+int g_deferred = 1;
+int64_t g_sw_count = 0;  // ops with FOF_SW in the programs emulated since the last reset
 
 void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
   std::vector<FOp> prog;
   uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
   plan_program(plan, p, KET_C128, prunef, NR, prog, lp, sp);
-  for (const FOp& o : prog) g_type_count[o.type & 31]++;
+  for (const FOp& o : prog) {
+    g_type_count[o.type & 31]++;
+    if (o.type != FO_CONT && (o.flags & FOF_SW)) g_sw_count++;
+  }
   const int L = p.L;
   auto gq = [&](int tb) { return tb < L ? tb : p.hbits[tb - L]; };
   uint64_t S = (uint64_t(1) << L) - 1;
@@ -96,8 +104,31 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
     Lay Lc = make_lay(lp);
     for (int t = 0; t < NTH; t++)
       for (int j = 0; j < NS; j++) x[t * NS + j] = amp[gaddr(ctx, Lc.tbase[t] | rofs(Lc, j))];
+    std::vector<uint32_t> sw(NTH, 0);
+    // carry out the pending swaps of register bits m (physical slot order = logical)
+    auto realize = [&](uint32_t m) {
+      for (int t = 0; t < NTH; t++) {
+        const uint32_t s = sw[t] & m;
+        if (!s) continue;
+        std::vector<cx> v(x.begin() + t * NS, x.begin() + (t + 1) * NS);
+        for (int j = 0; j < NS; j++) x[t * NS + (j ^ s)] = v[j];
+        sw[t] &= ~m;
+      }
+    };
     for (size_t oi = 0; oi < prog.size(); oi++) {
       const FOp& op = prog[oi];
+      if (op.type == FO_REAL) {
+        realize(op.creg);
+        continue;
+      }
+      if (op.type == FO_RELAY) {  // the data stays; the layout names its bits anew
+        Lc = make_lay(op.pos);
+        continue;
+      }
+      // the kernel's exchanges and shared-memory ops write the logical slots
+      const bool smem_x1 = op.type == FO_X1R && op.creg && ((op.creg & (op.creg - 1)) || op.cthr || op.cctx);
+      if (op.type == FO_EXCH || op.type == FO_SWAPS || op.type == FO_MAT2S || op.type == FO_DIAG || smem_x1)
+        realize(0xffffffffu);
       if (op.type == FO_CPHASE) {
         // phase fan on register bit a: T[k] * prod H[thread bits] * exp(i sum ctx angles)
         const double* H = record_data(prog, oi + 1);
@@ -160,13 +191,24 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
       }
       if ((ctx & op.cctx) != op.cctx) continue;
       const bool pr = op.flags & FOF_PRUNE;
-      const cx m0(op.m[0], op.m[1]), m1(op.m[2], op.m[3]), m2(op.m[4], op.m[5]), m3(op.m[6], op.m[7]);
+      const bool dfr = g_deferred && (op.flags & FOF_SW);
+      if (dfr && op.type == FO_X1R && !op.creg) {
+        for (int t = 0; t < NTH; t++)
+          if ((uint32_t)(t & op.cthr) == op.cthr) sw[t] ^= 1u << op.a;
+        continue;
+      }
       std::vector<cx> nx = x;
       for (int t = 0; t < NTH; t++) {
         const uint32_t sm_ = ((uint32_t)(t & op.cthr) == op.cthr) ? slotmask(op.creg) : 0;
         cx* xt = &x[t * NS];
         cx* nt = &nx[t * NS];
         const int lane = t & 31;
+        // a 2x2 or diagonal on a register bit whose slot pairs this thread has exchanged
+        const bool xs = dfr && (op.type == FO_MAT1R || op.type == FO_DIAGR) && ((sw[t] >> op.a) & 1);
+        const cx m0(op.m[xs ? 6 : 0], op.m[xs ? 7 : 1]), m1(op.m[xs ? 4 : 2], op.m[xs ? 5 : 3]),
+            m2(op.m[xs ? 2 : 4], op.m[xs ? 3 : 5]), m3(op.m[xs ? 0 : 6], op.m[xs ? 1 : 7]);
+        // the diagonal's two entries
+        const cx d0(op.m[xs ? 2 : 0], op.m[xs ? 3 : 1]), d1(op.m[xs ? 0 : 2], op.m[xs ? 1 : 3]);
         switch (op.type) {
           case FO_MAT1R: case FO_X1R:
             for (int j = 0; j < NS; j++) {
@@ -190,12 +232,12 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
           }
           case FO_DIAGR:
             for (int j = 0; j < NS; j++)
-              if ((sm_ >> j) & 1) nt[j] = ((j >> op.a) & 1 ? m1 : m0) * xt[j];
+              if ((sm_ >> j) & 1) nt[j] = ((j >> op.a) & 1 ? d1 : d0) * xt[j];
             break;
           case FO_DIAGT: case FO_DIAGX: {
             bool one = op.type == FO_DIAGT ? ((t >> op.a) & 1) : ((ctx & op.dg0) != 0);
             for (int j = 0; j < NS; j++)
-              if ((sm_ >> j) & 1) nt[j] = (one ? m1 : m0) * xt[j];
+              if ((sm_ >> j) & 1) nt[j] = (one ? d1 : d0) * xt[j];
             break;
           }
           case FO_DIAG: {
@@ -241,7 +283,14 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
       if (pr)
         for (auto& v : nx) prune(v);
       x = nx;
+      if (dfr && op.type == FO_X1R && op.creg) {
+        // X1RC on a deferred control bit C: flipping every pair along a adds the other half
+        const int c = __builtin_ctz(op.creg);
+        for (int t = 0; t < NTH; t++)
+          if ((uint32_t)(t & op.cthr) == op.cthr) sw[t] ^= ((sw[t] >> c) & 1u) << op.a;
+      }
     }
+    realize(0xffffffffu);  // the store writes the logical slots
     Lay Ls = make_lay(sp);
     for (int t = 0; t < NTH; t++)
       for (int j = 0; j < NS; j++) amp[gaddr(ctx, Ls.tbase[t] | rofs(Ls, j))] = x[t * NS + j];
@@ -270,6 +319,7 @@ int emu_apply_nreg(int n, const ket_op* ops, size_t nops, const double* mats, si
   cx* amp = reinterpret_cast<cx*>(re_im);
   passes[0] = passes[1] = 0;
   memset(g_type_count, 0, sizeof g_type_count);
+  g_sw_count = 0;
   for (const Pass& p : plan.passes) {
     if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) { passes[1]++; return -1; }
     run_pass(plan, p, n, prune != 0, amp);
@@ -280,6 +330,10 @@ int emu_apply_nreg(int n, const ket_op* ops, size_t nops, const double* mats, si
 
 // Ops of FOpType `type` in the programs of the last emu_apply call.
 int64_t emu_type_count(int type) { return g_type_count[type & 31]; }
+
+// 1 (the default): deferred register swaps as the compiled kernels run them; 0: as the interpreter.
+void emu_set_deferred(int on) { g_deferred = on; }
+int64_t emu_sw_count() { return g_sw_count; }
 
 int emu_apply(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int prune, int fusion,
               double* re_im, int64_t* passes) {

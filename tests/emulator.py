@@ -31,8 +31,17 @@ def lib():
                                  C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
     L.emu_type_count.restype = C.c_int64
     L.emu_type_count.argtypes = [C.c_int]
+    L.emu_set_deferred.restype = None
+    L.emu_set_deferred.argtypes = [C.c_int]
+    L.emu_sw_count.restype = C.c_int64
+    L.emu_sw_count.argtypes = []
     _lib = L
     return L
+
+
+def sw_count():
+    """Ops with deferred register swaps (FOF_SW) in the programs of the last emu_apply call."""
+    return lib().emu_sw_count()
 
 
 def type_count(fop_type):
@@ -40,9 +49,12 @@ def type_count(fop_type):
     return lib().emu_type_count(fop_type)
 
 
-def emu_apply(n, ops, init_state, prune=True, fusion=-1, nreg=5):
-    """nreg: register bits of the emulated layouts (5: ordinary passes, 4: adjoint passes)."""
+def emu_apply(n, ops, init_state, prune=True, fusion=-1, nreg=5, deferred=True):
+    """nreg: register bits of the emulated layouts (5: ordinary passes, 4: adjoint passes).
+    deferred: run the programs' deferred register swaps as the compiled kernels
+    do (True) or carry every swap out at once as the interpreter does (False)."""
     from ket_b200.circuit import ops_to_abi
+    lib().emu_set_deferred(1 if deferred else 0)
     arr, m, k = ops_to_abi(ops)
     st = np.ascontiguousarray(init_state, dtype=np.complex128).copy()
     passes = (C.c_int64 * 2)()

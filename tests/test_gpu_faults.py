@@ -62,11 +62,12 @@ def test_batch_wait_times_out_and_recovers():
 
 
 def test_staged_pass_wait_times_out_and_recovers():
-    """The staged pass kernels' tile threads wait for each tile's copies with a
-    bounded wait.  The test hook makes the copy warp skip one tile, so that wait
-    runs out (about two seconds), every tile thread stops together, the copy
-    warp drains its copies in flight, and the call reports KET_ERR_TIMEOUT; the
-    next call on the same context runs normally and matches the other form."""
+    """The staged pass kernels' tile groups wait for each tile's copies with a
+    bounded wait.  The test hook makes the issuing warp skip one tile, so that
+    wait runs out (about two seconds), the group's threads stop together, the
+    CTA waits for the copies it has in flight, and the call reports
+    KET_ERR_TIMEOUT; the next call on the same context runs normally and
+    matches the other form."""
     import ket_b200 as K
     from ket_b200 import _lib
     from ket_b200 import workloads as W

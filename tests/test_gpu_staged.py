@@ -1,7 +1,7 @@
 """The staged form of the compiled pass kernels (ket_exec_opts.stage = 1):
 every tile is brought into shared memory by tensor-memory-accelerator copies
-that a copy warp keeps in flight, one CTA per SM, instead of per-thread loads
-into registers.  The program, the layouts and the arithmetic are the same, so
+issued ahead of use, one CTA per SM with two tile groups sharing three
+stages, instead of per-thread loads into registers.  The program, the layouts and the arithmetic are the same, so
 the two forms must give equal states bit for bit -- over every op kind, with
 and without the reference's pruning, in both precisions, down to a state of
 one tile -- and the staged form must match the oracle to 1e-12."""
