@@ -54,8 +54,10 @@ enum FOpType : uint8_t {
   FO_CONT = 15,   // continuation record of the op before it (data only, never dispatched)
   FO_PPOLY = 16,  // phases of a run of controlled-phase gates (see below), followed by continuation records
   FO_REAL = 17,   // compiled kernels: carry out the deferred register swaps of the register bits in creg (see FOF_SW)
-  FO_RELAY = 18   // an uncontrolled swap of two tile bits as a relabelling: the layout pos (as FO_EXCH's) takes
+  FO_RELAY = 18,  // an uncontrolled swap of two tile bits as a relabelling: the layout pos (as FO_EXCH's) takes
                   // effect with no data moved
+  FO_SYNC = 19    // a barrier of the tile's threads: every load of the tile is done before any store (a program
+                  // whose relabellings move amplitudes between threads but that holds no exchange)
 };
 
 // flags
@@ -103,6 +105,7 @@ enum FOpCode : uint8_t {
   OC_PPOLY = 102,     // phases of a run of controlled-phase gates
   OC_REAL = 103,      // FO_REAL: carry out the deferred swaps of the register bits in creg (compiled kernels)
   OC_RELAY = 104,     // FO_RELAY: the new layout's exchange offsets, no data moved
+  OC_SYNC = 105,      // FO_SYNC: the tile's threads meet
   OC_NOP = 0xFF       // continuation record: dispatched as an op that does nothing
 };
 

@@ -257,6 +257,10 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
     sl = exch_slay_c<NR>(c, t.lane, t.warp);
     return;
   }
+  if constexpr (OPC == OC_SYNC) {  // every load of the tile done before any store
+    tile_sync(t);
+    return;
+  }
   if constexpr (CCTX) {
     if ((t.ctx0 & c.cctx) != c.cctx) return;  // uniform over the CTA
   }
@@ -380,7 +384,7 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   } else {
     // handled above (the exchange and the shared-memory ops return early)
     static_assert(OPC == OC_NOP || OPC == OC_EXCH || OPC == OC_SWAPS || OPC == OC_MAT2S || OPC == OC_DIAG ||
-                      OPC == OC_X1S || OPC == OC_REAL || OPC == OC_RELAY || (OPC >= OC_GRADM && OPC <= OC_GRADM2),
+                      OPC == OC_X1S || OPC == OC_REAL || OPC == OC_RELAY || OPC == OC_SYNC || (OPC >= OC_GRADM && OPC <= OC_GRADM2),
                   "op code without a compiled form");
     return;
   }

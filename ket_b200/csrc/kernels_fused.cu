@@ -112,6 +112,10 @@ __global__ void __launch_bounds__(32 << (7 - NR), NR == 5 ? 2 : 1) k_fused2(Pass
         sl = exch_slay<NR>(op, lane, warp);
         continue;
       }
+      if (opc == OC_SYNC) {  // every load of the tile done before any store
+        __syncthreads();
+        continue;
+      }
       const uint64_t cctx = ((uint64_t)h.w << 32) | h.z;
       if ((ctx0 & cctx) != cctx) continue;  // uniform over the CTA (and the same for all TT tiles)
       const double* M = op->m;

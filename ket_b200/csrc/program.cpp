@@ -550,6 +550,7 @@ void defer_swaps(std::vector<FOp>& prog) {
     switch (o.type) {
       case FO_CONT:  // the records of the op before: kept right after it
       case FO_RELAY:  // no data moves
+      case FO_SYNC:
         break;
       case FO_EXCH: case FO_SWAPS: case FO_MAT2S: case FO_DIAG:
         clear();  // written out through the logical slots
@@ -638,6 +639,7 @@ void assign_opcode(FOp& o) {
     case FO_PPOLY: o.opc = OC_PPOLY; break;
     case FO_REAL: o.opc = OC_REAL; break;
     case FO_RELAY: o.opc = OC_RELAY; break;
+    case FO_SYNC: o.opc = OC_SYNC; break;
     case FO_CONT: o.opc = OC_NOP; break;
     default: o.opc = 0xff; break;
   }
@@ -790,7 +792,7 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
   g_anc_tb = plan.anc >= 0 ? tpos(p, plan.anc) : -1;
   std::vector<Lay> lay;
   const bool dp = g_anc_tb < 0 && !getenv("KET_GREEDY_LAYOUT");
-  g_relabel = dp && getenv("KET_RELABEL");
+  g_relabel = dp && !getenv("KET_NO_RELABEL");
   if (dp && plan_layouts(plan, p, precision, lay)) {
     // lay[i]: the layout gate i runs in; lay[G]: the store layout
     Lay cur = lay[0];
@@ -815,6 +817,20 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
       prog.push_back(make_exch(cur, precision));
     }
     for (int i = 0; i < NB; i++) store_pos[i] = (uint8_t)cur.pos[i];
+    // Relabellings can make a thread store amplitudes that another thread
+    // loaded.  An exchange puts a barrier between every load and every store;
+    // without one, a barrier of its own does.
+    bool barrier = false, moved = false;
+    for (const FOp& o : prog) barrier = barrier || o.type == FO_EXCH;
+    for (int r = 0; r < 5 + NWg(); r++) moved = moved || load_pos[r] != store_pos[r];
+    if (moved && !barrier) {
+      FOp b;
+      memset(&b, 0, sizeof(b));
+      b.type = FO_SYNC;
+      b.d0 = b.d1 = -2;
+      b.lmask = 0xffffffffu;
+      prog.push_back(b);
+    }
     merge_phase_polys(prog);
     merge_phase_fans(prog);
     if (!getenv("KET_NO_DEFER")) defer_swaps(prog);

@@ -125,6 +125,7 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
         Lc = make_lay(op.pos);
         continue;
       }
+      if (op.type == FO_SYNC) continue;  // a barrier: nothing to emulate
       // the kernel's exchanges and shared-memory ops write the logical slots
       const bool smem_x1 = op.type == FO_X1R && op.creg && ((op.creg & (op.creg - 1)) || op.cthr || op.cctx);
       if (op.type == FO_EXCH || op.type == FO_SWAPS || op.type == FO_MAT2S || op.type == FO_DIAG || smem_x1)

@@ -97,3 +97,60 @@ def test_emulated_deferred_register_swaps(n, nreg, prune):
         outs.append(got)
     assert np.array_equal(outs[0], outs[1])  # swaps are exact: both orders give the same bits
 
+
+
+FO_SWAPS, FO_RELAY = 5, 18
+
+
+@pytest.mark.parametrize("n", [13, 16])
+@pytest.mark.parametrize("nreg", [5, 4])
+@pytest.mark.parametrize("prune", [True, False])
+def test_emulated_swaps_as_relabellings(n, nreg, prune):
+    """The QFT's closing swaps, uncontrolled and with both qubits in the tile,
+    run as relabellings of the layout (FO_RELAY: no data moves, no
+    shared-memory round trip); controlled swaps stay shared-memory ops.  The
+    state is the reference algorithm's."""
+    import ket_b200 as K
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import flatten_ops
+    from emulator import type_count
+    from oracle import oracle as O
+    c, _ = W.brickwork_qft(n, 6, 3)
+    c = c.cswap(0, 1, n - 1).swap(2, n - 2)
+    st0 = np.zeros(1 << n, complex)
+    st0[5] = 1
+    rc, got, passes = emu_apply(n, flatten_ops(c.ops), st0, prune=prune, nreg=nreg)
+    assert rc == 0
+    assert type_count(FO_RELAY) >= n // 2
+    assert type_count(FO_SWAPS) >= 1  # the controlled one
+    oc, _ = O.brickwork(n, 6, 3, with_qft=True)
+    oc.add("cswap", [0, 1, n - 1])
+    oc.add("swap", [2, n - 2])
+    want = oc.simulate(init=5, mode=O.DENSE_PRUNE if prune else O.DENSE).dense()
+    assert np.max(np.abs(got - want)) < 1e-12
+
+
+FO_EXCH, FO_SYNC = 0, 19
+
+
+@pytest.mark.parametrize("nreg", [5, 4])
+def test_relabelling_programs_keep_loads_before_stores(nreg):
+    """A pass of swaps only: the relabellings change which qubits the warp and
+    register roles hold, so the store writes amplitudes that other threads
+    loaded; the program then holds a barrier (FO_SYNC, or an exchange) between
+    the loads and the store."""
+    import ket_b200 as K
+    from ket_b200.circuit import flatten_ops
+    from emulator import type_count
+    n = 16
+    c = K.Circuit(n).swap(6, 13).swap(9, 15).swap(7, 12)
+    rng = np.random.default_rng(1)
+    a0 = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    rc, got, passes = emu_apply(n, flatten_ops(c.ops), a0, prune=False, nreg=nreg)
+    assert rc == 0 and passes[0] == 1
+    assert type_count(FO_RELAY) == 3
+    assert type_count(FO_SYNC) + type_count(FO_EXCH) >= 1
+    want = a0.reshape([2] * n)
+    for p, q in ((6, 13), (9, 15), (7, 12)):
+        want = np.swapaxes(want, n - 1 - p, n - 1 - q)
+    assert np.array_equal(got, want.reshape(-1))
