@@ -74,6 +74,45 @@ __device__ __forceinline__ SLay<NR> exch_slay_c(const COp& c, int lane, int warp
   return make_slay<NR>(bx, lane, warp);
 }
 
+// ---------------------------------------------------------------- mbarriers
+#define KET_STAGE_WAIT_NS 2000000000ull
+// Status words the staged loop writes: KET_ERR_TIMEOUT and KET_ERR_CUDA of
+// ket_sv.h (the run-time compiler sees only these headers; jit.cpp checks that
+// the values agree).
+constexpr int kStageTimeout = 5, kStageMisaligned = 4;
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for the phase of `parity` to complete; false once KET_STAGE_WAIT_NS has
+// passed without it.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try(bar, parity))
+    if (global_ns() - t0 > KET_STAGE_WAIT_NS) return false;
+  return true;
+}
 // Per-tile context of the ops.
 struct Tile {
   uint32_t smb;   // exchange buffer (shared-memory address)
@@ -82,6 +121,9 @@ struct Tile {
   double* sgrad;  // adjoint probe passes: the CTA's partial sums [slot][warp] in shared memory
   uint32_t sw;    // deferred register swaps (FOF_SW): physical slot j holds logical slot j ^ sw
   uint32_t bar;   // staged form: the named barrier of the tile's thread group
+  uint32_t xbar;  // register form: mbarrier on which the warps announce their reads of the exchange buffer
+  uint32_t xcnt;  // register form: exchange-buffer uses so far (every warp takes the same ones)
+  int* status;    // the call's status word (a bounded wait that ran out)
 };
 
 // The barrier among the threads that hold a tile.  In the staged form
@@ -94,6 +136,30 @@ __device__ __forceinline__ void tile_sync(const Tile& t) {
 #else
   (void)t;
   __syncthreads();
+#endif
+}
+
+// Reuse of the exchange buffer.  An exchange writes the tile into the buffer,
+// meets the other warps, and reads its new slots back; the next use of the
+// buffer must not write before every warp has done those reads.  In the
+// register form each warp announces its reads on an mbarrier right after
+// them, and the next use waits for that phase -- normally long complete --
+// instead of holding a barrier of the whole CTA.  The staged form keeps its
+// group barrier.
+__device__ __forceinline__ void xbuf_acquire(Tile& t) {
+#ifdef KET_STAGED_THREADS
+  tile_sync(t);
+#else
+  if (t.xcnt && !mbar_wait(t.xbar, (t.xcnt - 1) & 1)) atomicExch(t.status, kStageTimeout);
+#endif
+}
+__device__ __forceinline__ void xbuf_release(Tile& t) {
+#ifndef KET_STAGED_THREADS
+  __syncwarp();
+  if (t.lane == 0) mbar_arrive(t.xbar);
+  t.xcnt++;
+#else
+  (void)t;
 #endif
 }
 
@@ -137,7 +203,7 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
   const int oa = (h.x >> 8) & 0xff, ob = (int)(h2.w & 0xffu);
   const double* M = op->m;
   const uint32_t smb = t.smb;
-  tile_sync(t);
+  xbuf_acquire(t);
   write_tile<R, NR>(smb, logical_slay<NR>(sl, t.sw), x);
   t.sw = 0;
   tile_sync(t);
@@ -170,6 +236,7 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
       }
     }
     grad_accum(t.sgrad, slot, t.warp, t.lane, acc);
+    xbuf_release(t);
     return;
   } else if constexpr (OPC == OC_X1S) {
     for (uint32_t g = t.tid; g < (1u << (KET_T2_BITS - 1)); g += NT) {
@@ -229,6 +296,7 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
   }
   tile_sync(t);
   read_tile<R, NR>(smb, sl, x);
+  xbuf_release(t);
 }
 
 // One op of the program.  OPC: op code; FL: flags; CREG: register controls;
@@ -241,12 +309,13 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   constexpr int NS = 1 << NR;
   constexpr double thr = 1e-14, qthr = 1e-7;
   if constexpr (OPC == OC_EXCH) {
-    tile_sync(t);
+    xbuf_acquire(t);
     write_tile<R, NR>(t.smb, logical_slay<NR>(sl, t.sw), x);
     t.sw = 0;
     tile_sync(t);
     sl = exch_slay_c<NR>(c, t.lane, t.warp);
     read_tile<R, NR>(t.smb, sl, x);
+    xbuf_release(t);
     return;
   }
   if constexpr (OPC == OC_REAL) {
@@ -433,10 +502,17 @@ __device__ __forceinline__ void run_tiles(const Pass2Args& a, Body body) {
   t.lane = t.tid & 31;
   t.warp = t.tid >> 5;
   t.sgrad = reinterpret_cast<double*>(smraw + ((size_t)sizeof(V) << KET_T2_BITS));
-  if constexpr (GRAD) {
-    for (int i = t.tid; i < a.nslots * 8; i += NT) t.sgrad[i] = 0.0;
-    __syncthreads();
+  __shared__ __align__(8) unsigned long long xbar_word;
+  t.xbar = (uint32_t)__cvta_generic_to_shared(&xbar_word);
+  t.xcnt = 0;
+  t.status = a.status;
+  if (t.tid == 0) {
+    mbar_init(t.xbar, NT / 32);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if constexpr (GRAD)
+    for (int i = t.tid; i < a.nslots * 8; i += NT) t.sgrad[i] = 0.0;
+  __syncthreads();
   char* const amp = reinterpret_cast<char*>(a.amp);
   const uint64_t ntiles = uint64_t(1) << (a.n - KET_T2_BITS);
   uint64_t gl = 0, gs = 0;
@@ -508,41 +584,6 @@ struct __align__(64) TMap {
   unsigned long long w[16];
 };
 
-#define KET_STAGE_WAIT_NS 2000000000ull
-// Status words the staged loop writes: KET_ERR_TIMEOUT and KET_ERR_CUDA of
-// ket_sv.h (the run-time compiler sees only these headers; jit.cpp checks that
-// the values agree).
-constexpr int kStageTimeout = 5, kStageMisaligned = 4;
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-// Wait for the phase of `parity` to complete; false once KET_STAGE_WAIT_NS has
-// passed without it.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  if (mbar_try(bar, parity)) return true;
-  const uint64_t t0 = global_ns();
-  while (!mbar_try(bar, parity))
-    if (global_ns() - t0 > KET_STAGE_WAIT_NS) return false;
-  return true;
-}
 // Wait until *p >= want (a count another warp of the CTA raises); false once
 // KET_STAGE_WAIT_NS has passed without it.
 __device__ __forceinline__ bool wait_count(const uint32_t* p, uint32_t want) {

@@ -655,7 +655,13 @@ namespace {
 // bit 0.4, an X on a register bit under a thread or out-of-tile control 0.22
 // (conditional register moves; uncontrolled or register-controlled, a
 // renaming), a diagonal 0.16, a layout exchange 0.45.
-constexpr double kCostExch = 0.45;
+double exch_cost() {
+  static const double c = [] {
+    const char* e = getenv("KET_COST_EXCH");  // experiments only
+    return e ? atof(e) : 0.45;
+  }();
+  return c;
+}
 
 double mat_form_cost(const Gate& g) {
   bool real = true;
@@ -679,10 +685,10 @@ double gate_cost(const Gate& g, const Pass& p, const Lay& l) {
       }
       if (nreg == 0) return other ? 0.22 : 0.0;
       if (nreg == 1 && !other) return 0.0;
-      return 2 * kCostExch;  // several controls with one on a register bit: a shared-memory op
+      return 2 * exch_cost();  // several controls with one on a register bit: a shared-memory op
     }
     case G_DIAG1: return 0.16;
-    default: return 2 * kCostExch;  // shared-memory ops: the same in every layout
+    default: return 2 * exch_cost();  // shared-memory ops: the same in every layout
   }
 }
 
@@ -745,7 +751,7 @@ bool plan_layouts(const Plan& plan, const Pass& p, int precision, std::vector<La
         if (same_lay(c, run[i][k].l)) continue;
         if (i < G && !fits(plan.gates[p.gates[i]], p, c)) continue;
         if (i == G && !a0_compatible(c)) continue;
-        relax(at[i], {c, run[i][k].cost + kCostExch, (int)k, true});
+        relax(at[i], {c, run[i][k].cost + exch_cost(), (int)k, true});
       }
     if (i == G) break;
     const Gate& g = plan.gates[p.gates[i]];
