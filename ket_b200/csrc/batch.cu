@@ -170,6 +170,16 @@ __device__ void rx_bits(double2* s, int m, uint32_t bits, double cb, double sb) 
   }
 }
 
+// 16-byte asynchronous copy global -> shared (through L2 only: the data was
+// written by other CTAs of the same launch).
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n cp.async.wait_group 0;" ::: "memory");
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, batch_min_blocks<NT>()) k_batch_qaoa(QArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -177,7 +187,8 @@ __global__ void __launch_bounds__(NT, batch_min_blocks<NT>()) k_batch_qaoa(QArgs
   double2* tab = s + (1u << a.tile);                             // phase table (<= 65 entries)
   uint64_t* em = reinterpret_cast<uint64_t*>(tab + KQ_MAX_EDGES + 1);
   double* red = reinterpret_cast<double*>(em + KQ_MAX_EDGES);     // 32 doubles
-  uint8_t* cutb = reinterpret_cast<uint8_t*>(red + 32);           // whole instances: cut(x) per amplitude
+  uint8_t* cutb = reinterpret_cast<uint8_t*>(red + 32);           // cut(x) per amplitude (whole instance / tile)
+  static_assert((16 * (KQ_MAX_EDGES + 1) + 8 * KQ_MAX_EDGES + 8 * 32) % 16 == 0, "cut bytes 16-byte aligned");
   __shared__ int item_sh;
   const int T = a.tile;
   for (;;) {
@@ -269,17 +280,15 @@ __global__ void __launch_bounds__(NT, batch_min_blocks<NT>()) k_batch_qaoa(QArgs
       const double amp0 = 1.0 / sqrt((double)(uint64_t(1) << n));
       for (uint32_t i = threadIdx.x; i < TN; i += NT) s[sw(i)] = make_double2(amp0, 0.0);
     } else {
-      // four loads in flight per thread before any lands in shared memory
-      // (written by other CTAs: bypass L1)
-      for (uint32_t i0 = threadIdx.x; i0 < TN; i0 += 4 * NT) {
-        double2 v[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (i0 + j * NT < TN) v[j] = __ldcg(g + gidx(i0 + j * NT));
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (i0 + j * NT < TN) s[sw(i0 + j * NT)] = v[j];
+      // the whole tile in flight at once, straight into shared memory, and
+      // for pass A of later layers its cut values (kept by layer 0; pass-A
+      // tiles are contiguous)
+      for (uint32_t i = threadIdx.x; i < TN; i += NT) cp_async16(s + sw(i), g + gidx(i));
+      if (passA && layer > 0) {
+        const uint8_t* cw = a.cutw + I.cut + ((uint64_t)w.tile << T);
+        for (uint32_t i = 16 * threadIdx.x; i < TN; i += 16 * NT) cp_async16(cutb + i, cw + i);
       }
+      cp_async_wait_all();
     }
     double sb, cb;
     sincos(a.beta[w.inst * I.p + layer], &sb, &cb);
@@ -288,7 +297,7 @@ __global__ void __launch_bounds__(NT, batch_min_blocks<NT>()) k_batch_qaoa(QArgs
       fill_phase<NT>(tab, a.gamma[w.inst * I.p + layer], I.ne);
       __syncthreads();
       // pass A tiles are contiguous: layer 0 computes cut(x) and keeps it,
-      // later layers read it back (written by other CTAs: bypass L1)
+      // later layers copied it into shared memory with the tile
       uint8_t* cw = a.cutw + I.cut;
       for (uint32_t i = threadIdx.x; i < TN; i += NT) {
         const uint64_t x = gidx(i);
@@ -297,7 +306,7 @@ __global__ void __launch_bounds__(NT, batch_min_blocks<NT>()) k_batch_qaoa(QArgs
           cx = cut_of(x, em, I.ne);
           cw[x] = (uint8_t)cx;
         } else {
-          cx = __ldcg(cw + x);
+          cx = cutb[i];
         }
         const double2 ph = tab[cx];
         const double2 v = s[sw(i)];
