@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(32 << (7 - NR), NR == 5 ? 2 : 1) k_fused2(Pass
         continue;  // pruning already done
       }
       const bool thr_ok = ((uint32_t)tid & cthr) == cthr;
-      if (GRAD && opc >= OC_GRADM) {  // adjoint passes hold no phase fans (the host merges none there)
+      if (GRAD && opc >= OC_GRADM && opc <= OC_GRADD) {  // adjoint passes hold no phase fans (the host merges none there)
         // <lambda|D|psi> over this thread's amplitudes: register bit 3 of the
         // slot index selects psi (0) or lambda (1) -- the planner pins the
         // ancilla there.  Every lane takes part in the warp sum.  (TT == 1)

@@ -797,8 +797,11 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
   g_nreg = nreg;
   g_anc_tb = plan.anc >= 0 ? tpos(p, plan.anc) : -1;
   std::vector<Lay> lay;
-  const bool dp = g_anc_tb < 0 && !getenv("KET_GREEDY_LAYOUT");
-  g_relabel = dp && !getenv("KET_NO_RELABEL");
+  // adjoint passes too (their probes fit only where the ancilla and a 2x2
+  // probe's target sit in registers, which the candidates respect); their
+  // swaps stay data moves
+  const bool dp = !getenv("KET_GREEDY_LAYOUT") && (g_anc_tb < 0 || !getenv("KET_ADJOINT_GREEDY"));
+  g_relabel = dp && g_anc_tb < 0 && !getenv("KET_NO_RELABEL");
   if (dp && plan_layouts(plan, p, precision, lay)) {
     // lay[i]: the layout gate i runs in; lay[G]: the store layout
     Lay cur = lay[0];
@@ -837,8 +840,10 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
       b.lmask = 0xffffffffu;
       prog.push_back(b);
     }
-    merge_phase_polys(prog);
-    merge_phase_fans(prog);
+    if (g_anc_tb < 0) {  // the probe passes run no merged phase ops
+      merge_phase_polys(prog);
+      merge_phase_fans(prog);
+    }
     if (!getenv("KET_NO_DEFER")) defer_swaps(prog);
     for (FOp& o : prog) assign_opcode(o);
     g_relabel = false;
