@@ -238,8 +238,8 @@ static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpa
     int rc = ctx_scratch(c, fb + 256, &dev);
     if (rc) return rc;
     c->h2d_bytes += fb;
-    cudaError_t e = cudaMemcpyAsync(dev, prog.data(), fb, cudaMemcpyHostToDevice, c->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(probe ops)");
+    rc = ctx_upload(c, dev, prog.data(), fb);
+    if (rc) return rc;
     a.amp = s->amp;
     a.ops = reinterpret_cast<const FOp*>(dev);
     a.nops = (int)prog.size();
@@ -271,7 +271,7 @@ static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpa
     const int nctas = jf.fn ? (int)jit_grid(s->n) : std::min<int>(fused2_grid(4), 1 << (s->n - KET_T2_BITS));
     if ((size_t)nctas * nprobe * 8 > gpart_cap) return fail(KET_ERR_UNSUPPORTED, "too many gradient probes in a pass");
     prof_begin(c);
-    e = jf.fn ? jit_launch(jf, a, s->precision, c->stream) : launch_fused2(a, s->precision, c->stream);
+    cudaError_t e = jf.fn ? jit_launch(jf, a, s->precision, c->stream) : launch_fused2(a, s->precision, c->stream);
     prof_end(c, PK_ADJOINT);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint pass launch");
     e = launch_grad_reduce(gpart, nctas, nprobe, slot_out + slot_lo, c->stream);
@@ -499,7 +499,8 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
     // ---- forward, segment by segment, saving checkpoints
     cudaMemsetAsync(buf, 0, 2 * half, ctx->stream);
     static const double one[2] = {1.0, 0.0};
-    cudaMemcpyAsync((char*)buf + 16 * init, one, 16, cudaMemcpyHostToDevice, ctx->stream);
+    rc = ctx_upload(ctx, (char*)buf + 16 * init, one, 16);
+    if (rc) { cleanup(); return rc; }
     for (int sg = 0; sg < nseg; sg++) {
       size_t lo = (size_t)sg * C, hi = std::min(nops, lo + C);
       if (sg >= 1 && sg <= nck && save(sg) != cudaSuccess) { cleanup(); return cuda_fail(cudaGetLastError(), "checkpoint save"); }

@@ -83,6 +83,32 @@ double wait_deadline_s() {
   return e ? atof(e) : 1800.0;
 }
 
+int ctx_upload(ket_ctx* c, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return KET_OK;
+  constexpr size_t kSlots = 16;
+  if (c->stage_ring.empty()) c->stage_ring.resize(kSlots);
+  ket_ctx::StageSlot& sl = c->stage_ring[c->stage_next];
+  c->stage_next = (c->stage_next + 1) % kSlots;
+  cudaError_t e;
+  if (sl.used && (e = cudaEventSynchronize(sl.ev)) != cudaSuccess) return cuda_fail(e, "staging slot");
+  if (sl.cap < bytes) {
+    if (sl.p) cudaFreeHost(sl.p);
+    sl.p = nullptr;
+    sl.cap = 0;
+    const size_t cap = std::max<size_t>(bytes, 64 << 10);
+    if ((e = cudaHostAlloc(&sl.p, cap, cudaHostAllocDefault)) != cudaSuccess) return cuda_fail(e, "cudaHostAlloc(staging)");
+    sl.cap = cap;
+  }
+  if (!sl.ev && (e = cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming)) != cudaSuccess)
+    return cuda_fail(e, "cudaEventCreate");
+  memcpy(sl.p, src, bytes);
+  if ((e = cudaMemcpyAsync(dst, sl.p, bytes, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+    return cuda_fail(e, "cudaMemcpyAsync(upload)");
+  if ((e = cudaEventRecord(sl.ev, c->stream)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+  sl.used = true;
+  return KET_OK;
+}
+
 int ctx_wait(ket_ctx* ctx) {
   cudaError_t e = cudaEventRecord(ctx->done, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
@@ -181,6 +207,10 @@ int ket_ctx_destroy(ket_ctx* c) {
   if (c->vqe_graph_exec) cudaGraphExecDestroy(c->vqe_graph_exec);
   if (c->vqe_work) cudaFree(c->vqe_work);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  for (auto& sl : c->stage_ring) {
+    if (sl.p) cudaFreeHost(sl.p);
+    if (sl.ev) cudaEventDestroy(sl.ev);
+  }
   cudaEventDestroy(c->done);
   cudaStreamDestroy(c->stream);
   delete c;
@@ -562,8 +592,8 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait) 
       memcpy(dst + 64, g.mk.data(), 16 * g.mk.size());
     }
     c->h2d_bytes += total;
-    cudaError_t e = cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, c->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(ops)");
+    int urc = ctx_upload(c, dev, host.data(), total);
+    if (urc) return urc;
   }
   const FOp* dfops = reinterpret_cast<const FOp*>(dev);
   const DevOp* dops = reinterpret_cast<const DevOp*>((const char*)dev + f_bytes);

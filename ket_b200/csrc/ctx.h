@@ -35,6 +35,17 @@ struct ket_ctx {
   size_t prof_next = 0;           // next free event pair
   int batch_threads = 256;        // ket_batch_qaoa: threads per CTA (set by ket_batch_config)
   int batch_tile = 12;            // ket_batch_qaoa: tile width in qubits
+  // Pinned staging for uploads of op programs (ctx_upload): a copy from
+  // pageable memory may wait for the stream, which would keep the host from
+  // planning ahead of the GPU.  A slot is reused once its copy has run.
+  struct StageSlot {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+    bool used = false;
+  };
+  std::vector<StageSlot> stage_ring;
+  size_t stage_next = 0;
 };
 
 struct ket_state {
@@ -53,6 +64,10 @@ int cuda_fail(cudaError_t e, const char* where);
 int dev_alloc(void** p, size_t bytes);
 int ctx_scratch(ket_ctx* ctx, size_t bytes, void** out);
 int ctx_wait(ket_ctx* ctx);
+// Copy bytes from host memory to device memory dst, in stream order, through
+// the context's pinned staging ring: the call returns without waiting for
+// the stream (unless every slot's copy is still queued).
+int ctx_upload(ket_ctx* ctx, void* dst, const void* src, size_t bytes);
 // Run a plan's passes on the state's stream.  wait = false returns once the
 // launches are queued (the caller waits and reads the status word later);
 // every buffer the passes read is stream-ordered, so queued plans may follow
