@@ -208,30 +208,37 @@ static int run_plan_grad(ket_state* s, Plan& plan, double* slot_out, double* gpa
   ket_exec_opts_default(&o);
   o.prune = 0;
   o.specialize = specialize;
-  // Passes without probes use the ordinary runner, one at a time.
-  for (size_t i = 0; i < np; i++) {
-    const Pass& p = plan.passes[i];
-    int nprobe = 0, slot_lo = 1 << 30;
-    for (int gi : p.gates)
+  auto probes_of = [&](size_t i, int& slot_lo) {
+    int nprobe = 0;
+    slot_lo = 1 << 30;
+    for (int gi : plan.passes[i].gates)
       if (is_grad(plan.gates[gi])) { nprobe++; slot_lo = std::min(slot_lo, plan.gates[gi].slot); }
-    Plan one;
-    one.gates = plan.gates;
-    one.anc = plan.anc;
-    one.passes.push_back(p);
+    return nprobe;
+  };
+  for (size_t i = 0; i < np;) {
+    const Pass& p = plan.passes[i];
+    int slot_lo;
+    const int nprobe = probes_of(i, slot_lo);
     if (nprobe == 0) {
-      int rc = run_plan(s, one, o, false);
+      // a run of passes without probes: the ordinary runner, in one call
+      size_t j = i + 1;
+      int lo2;
+      while (j < np && probes_of(j, lo2) == 0) j++;
+      int rc = run_plan(s, plan, o, false, i, j);
       if (rc) return rc;
+      i = j;
       continue;
     }
+    i++;
     if (!(p.fused && p.m == KET_T2_BITS && s->n >= KET_T2_BITS))
       return fail(KET_ERR_UNSUPPORTED, "adjoint probe outside a register-tiled pass");
-    // renumber the probes of this pass 0..nprobe-1 (they are consecutive slots)
-    for (int gi : p.gates)
-      if (is_grad(one.gates[gi])) one.gates[gi].slot -= slot_lo;
     std::vector<FOp> prog;
     Pass2Args a;
     memset(&a, 0, sizeof(a));
-    plan_program(one, p, s->precision, false, 4, prog, a.load_pos, a.store_pos);
+    plan_program(plan, p, s->precision, false, 4, prog, a.load_pos, a.store_pos);
+    // the probes of this pass write slots 0..nprobe-1 (they are consecutive)
+    for (FOp& f : prog)
+      if (f.type == FO_GRADM || f.type == FO_GRADD || f.type == FO_GRADM2) f.slot = (int16_t)(f.slot - slot_lo);
     a.nreg = 4;  // probes: 256 threads, ancilla on register bit 3
     void* dev;
     size_t fb = sizeof(FOp) * prog.size();
@@ -491,11 +498,23 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
   // KET_ADJ_TIMING=1: host seconds spent queueing the batch and waiting for it, to stderr
   static const bool timing = getenv("KET_ADJ_TIMING") != nullptr;
   const auto t_start = std::chrono::steady_clock::now();
+  // host seconds per section (with KET_ADJ_TIMING): binding, forward planning,
+  // forward launches, energy, reverse gates, reverse planning, probe passes
+  double sec[7] = {0, 0, 0, 0, 0, 0, 0};
+  auto t_last = t_start;
+  auto tick = [&](int k) {
+    if (!timing) return;
+    const auto now = std::chrono::steady_clock::now();
+    sec[k] += std::chrono::duration<double>(now - t_last).count();
+    t_last = now;
+  };
   for (int b = 0; b < batch; b++) {
     const double* theta = params + (size_t)b * nparams;
     Bound bd;
+    tick(6);
     rc = bind_params(ops, nops, mats, nmat, binds, nbinds, theta, nparams, bd);
     if (rc) { cleanup(); return rc; }
+    tick(0);
     // ---- forward, segment by segment, saving checkpoints
     cudaMemsetAsync(buf, 0, 2 * half, ctx->stream);
     static const double one[2] = {1.0, 0.0};
@@ -510,8 +529,10 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
       if (rc) { cleanup(); return fail(rc, err); }
       if (fp.gates.empty()) continue;
       plan_passes(n, KET_C128, -1, false, fp);
+      tick(1);
       rc = run_plan(&w.psi, fp, fo, false);
       if (rc) { cleanup(); return rc; }
+      tick(2);
     }
     // ---- lambda = H psi, energy
     prof_begin(ctx);
@@ -520,6 +541,7 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
     k_sum_fixed<<<1, 32, 0, ctx->stream>>>(w.epart, hblocks, d_energy + b);
     prof_end(ctx, PK_ADJOINT);
     ctx->launches += 1;
+    tick(3);
     // ---- reverse sweep
     double* slots_b = w.slot_out + (size_t)b * nslot;
     std::vector<int> sb;
@@ -587,10 +609,13 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
         }
       }
       if (bp.gates.empty()) continue;
+      tick(4);
       plan_passes(n + 1, KET_C128, -1, false, bp);
+      tick(5);
       // probes must stay in order within each pass: slots are consecutive per pass by construction
       rc = run_plan_grad(&w.full, bp, slots_b, w.gpart, w.gpart_cap, specialize);
       if (rc) { cleanup(); return rc; }
+      tick(6);
     }
     if (b == 0) slot_bind = sb;
   }
@@ -608,6 +633,8 @@ int ket_adjoint_gradient(ket_ctx* ctx, int n, uint64_t init, const ket_op* ops, 
     fprintf(stderr, "ket_adjoint_gradient: %d vectors, %d segments: queued in %.3f s, then waited %.3f s\n", batch,
             nseg, std::chrono::duration<double>(t_queued - t_start).count(),
             std::chrono::duration<double>(t_done - t_queued).count());
+    fprintf(stderr, "  host s: bind %.3f, forward plan %.3f, forward launch %.3f, energy %.3f, reverse gates %.3f,"
+            " reverse plan %.3f, probe passes %.3f\n", sec[0], sec[1], sec[2], sec[3], sec[4], sec[5], sec[6]);
   }
   if (rc) { cleanup(); return rc; }
   for (int b = 0; b < batch; b++) {

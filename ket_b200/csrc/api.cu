@@ -494,12 +494,15 @@ int ket_apply_ops(ket_state* s, const ket_op* ops, size_t nops, const double* ma
 
 namespace ket {
 
-int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait) {
+int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait, size_t first, size_t last) {
   ket_ctx* c = s->ctx;
   cudaSetDevice(c->device);
   const bool prune = o.prune != 0;
   // Device image: v2 programs (FOp), v1 programs (DevOp), then MATK descriptors.
-  const size_t np = plan.passes.size();
+  // passes [first, last) of the plan
+  last = std::min(last, plan.passes.size());
+  first = std::min(first, last);
+  const size_t np = last - first;
   std::vector<FOp> fops;
   std::vector<DevOp> devops;
   std::vector<size_t> off(np, 0), matk_off(np, 0);
@@ -516,10 +519,10 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait) 
     Pass2Args& a = p2[i];
     memset(&a, 0, sizeof(a));
     a.nreg = nreg;
-    plan_program(plan, plan.passes[i], s->precision, prune, nreg, progs[i], a.load_pos, a.store_pos);
+    plan_program(plan, plan.passes[first + i], s->precision, prune, nreg, progs[i], a.load_pos, a.store_pos);
   };
   for (size_t i = 0; i < np; i++) {
-    const Pass& p = plan.passes[i];
+    const Pass& p = plan.passes[first + i];
     if (p.fused && p.m == KET_T2_BITS && s->n >= KET_T2_BITS) {
       use2[i] = true;
       lower_pass(i, o.specialize < 0 ? KET_FUSED_NREG : jit_nr);
@@ -530,7 +533,7 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait) 
     for (size_t i = 0; i < np; i++)
       if (use2[i])
         jp[i] = JitPass{progs[i].data(), (int)progs[i].size(), s->n, jit_nr, p2[i].load_pos,
-                        use_staged(s->n, o.stage) && plan.passes[i].L == 5};
+                        use_staged(s->n, o.stage) && plan.passes[first + i].L == 5};
     std::string err;
     int rc = jit_prepare(jp, s->precision, o.specialize, c->stream, jf, err);
     if (rc) return fail(rc, err);
@@ -538,7 +541,7 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait) 
       if (use2[i] && !jf[i].fn && jit_nr != KET_FUSED_NREG) lower_pass(i, KET_FUSED_NREG);
   }
   for (size_t i = 0; i < np; i++) {
-    const Pass& p = plan.passes[i];
+    const Pass& p = plan.passes[first + i];
     if (use2[i]) {
       const std::vector<FOp>& prog = progs[i];
       Pass2Args& a = p2[i];
@@ -582,7 +585,7 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait) 
     if (!fops.empty()) memcpy(host.data(), fops.data(), sizeof(FOp) * fops.size());
     if (!devops.empty()) memcpy(host.data() + f_bytes, devops.data(), sizeof(DevOp) * devops.size());
     for (size_t i = 0; i < np; i++) {
-      const Pass& p = plan.passes[i];
+      const Pass& p = plan.passes[first + i];
       if (p.fused) continue;
       const Gate& g = plan.gates[p.gates[0]];
       if (g.type != G_MATK) continue;
@@ -598,7 +601,7 @@ int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait) 
   const FOp* dfops = reinterpret_cast<const FOp*>(dev);
   const DevOp* dops = reinterpret_cast<const DevOp*>((const char*)dev + f_bytes);
   for (size_t i = 0; i < np; i++) {
-    const Pass& p = plan.passes[i];
+    const Pass& p = plan.passes[first + i];
     cudaError_t e;
     int kind = use2[i] ? PK_FUSED2 : (p.fused ? PK_FUSED1 : PK_GATE);
     prof_begin(c);

@@ -71,8 +71,9 @@ int ctx_upload(ket_ctx* ctx, void* dst, const void* src, size_t bytes);
 // Run a plan's passes on the state's stream.  wait = false returns once the
 // launches are queued (the caller waits and reads the status word later);
 // every buffer the passes read is stream-ordered, so queued plans may follow
-// one another.
-int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait = true);
+// one another.  first, last: run only passes [first, last) of the plan.
+int run_plan(ket_state* s, const Plan& plan, const ket_exec_opts& o, bool wait = true, size_t first = 0,
+             size_t last = SIZE_MAX);
 int check_status(ket_ctx* c);
 // ket_sample with the sequential CDF up to seq_qubits qubits (see read.h).
 int sample_indices(const ket_state* s, const double* r, size_t shots, double thr, uint64_t* out);
