@@ -245,3 +245,21 @@ def test_no_gpu_reports_cuda_error():
     h = C.c_void_p()
     rc = _lib.lib().ket_ctx_create(0, C.byref(h))
     assert rc == _lib.KET_ERR_CUDA
+
+
+def test_program_generator_on_the_bench_workload():
+    """The cost-model layouts on the 30-qubit bench circuit (4 register bits,
+    pruning on): 2x2 gates on lane bits, which cost a shuffle per amplitude,
+    nearly all become register gates (145 under the greedy rule), and no swap
+    is left as a shared-memory op (the QFT's closing swaps are relabellings)."""
+    c, _ = W.brickwork_qft(30, 40, 42)
+    arr, m, k = ops_to_abi(flatten_ops(c.ops))
+    mv = np.ascontiguousarray(m).view(np.float64)
+    o = _lib.exec_opts(prune=True, specialize=1, reg_bits=4)
+    cnt = (C.c_int64 * 16)()
+    _lib.check(_lib.lib().ket_plan_program_stats(30, 0, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size,
+                                                 C.byref(o), cnt))
+    assert cnt[14] == 106
+    assert cnt[2] <= 32, list(cnt)   # 2x2 on lane bits
+    assert cnt[5] == 0, list(cnt)    # swaps through shared memory
+    assert 150 <= cnt[0] <= 260, list(cnt)  # layout exchanges
