@@ -33,6 +33,7 @@ __device__ __forceinline__ uint32_t swz(uint32_t i) {
 template <int NR>
 struct SLay {
   uint32_t b, s[NR];
+  uint32_t l[5];  // the lane bits' offsets (deferred lane moves address the logical lanes with them)
 };
 
 template <int NR>
@@ -59,6 +60,8 @@ __device__ __forceinline__ SLay<NR> make_slay(const uint32_t* bx, int lane, int 
   l.b = b;
 #pragma unroll
   for (int k = 0; k < NR; k++) l.s[k] = bx[5 + NW + k];
+#pragma unroll
+  for (int r = 0; r < 5; r++) l.l[r] = bx[r];
   return l;
 }
 
@@ -349,9 +352,11 @@ __device__ __forceinline__ void grad_accum(double* sgrad, int slot, int warp, in
 // ---------------------------------------------------------------- phase fans
 // FO_CPHASE on register bit A for the TT tiles of a thread; tile t's context is
 // ctx0 | (t ? pairq : 0).
+// tid: the thread (which lanes add which terms); ltid: the logical thread id
+// whose bits the thread factor reads (tid but for deferred lane X gates).
 template <typename R, int A, int TT, int NS>
 __device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][NS], const FOp* op, uint32_t nterms, uint64_t ctx0,
-                                          uint64_t pairq, int tid) {
+                                          uint64_t pairq, int tid, int ltid) {
   // record 0 after the op: H[0..7]; records 1..: (angle, mask) pairs; each
   // record's data starts after its 16-byte no-op header
   const double2* H = reinterpret_cast<const double2*>(reinterpret_cast<const char*>(op + 1) + 16);
@@ -373,7 +378,7 @@ __device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][NS], const FOp* op, ui
 #pragma unroll
   for (int sb = 0; sb < 8; sb++) {
     const double2 h = __ldg(H + sb);
-    const bool on = (tid >> sb) & 1;
+    const bool on = (ltid >> sb) & 1;
     const double hr = on ? h.x : 1.0, hi = on ? h.y : 0.0;
     const double r = fr * hr - fi * hi;
     fi = fr * hi + fi * hr;
@@ -396,13 +401,14 @@ __device__ __forceinline__ void phase_fan(cpx<R> (&x)[TT][NS], const FOp* op, ui
 
 // FO_PPOLY: the phases of a run of controlled-phase gates (the layout is
 // described in fused_abi.h), for the TT tiles of a thread (the second at
-// ctx0 | pairq).  Lane g multiplies the phases of group g's terms that match
-// the tile; each thread then multiplies, per register bit, the products of
-// the groups whose thread mask it matches, and its slots take them.  The
+// ctx0 | pairq).  Lane g (of tid) multiplies the phases of group g's terms
+// that match the tile; each thread then multiplies, per register bit, the
+// products of the groups whose thread mask its logical id ltid matches (tid
+// but for deferred lane X gates), and its slots take them.  The
 // whole warp runs this (no thread-bit controls on the op).
 template <typename R, int TT, int NS>
 __device__ __forceinline__ void phase_poly(cpx<R> (&x)[TT][NS], const FOp* op, uint64_t ctx0, uint64_t pairq,
-                                           int tid) {
+                                           int tid, int ltid) {
   const char* m = reinterpret_cast<const char*>(op->m);
   const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(m));
   const uint2 c1 = __ldg(reinterpret_cast<const uint2*>(m + 16));
@@ -454,7 +460,7 @@ __device__ __forceinline__ void phase_poly(cpx<R> (&x)[TT][NS], const FOp* op, u
       for (int t = 0; t < TT; t++) {
         const double kr = __shfl_sync(0xffffffffu, K[t].re, (int)g);
         const double ki = __shfl_sync(0xffffffffu, K[t].im, (int)g);
-        if (((uint32_t)tid & tm) == tm) cmul_in<double>(F[t], kr, ki);
+        if (((uint32_t)ltid & tm) == tm) cmul_in<double>(F[t], kr, ki);
       }
     }
 #pragma unroll

@@ -117,6 +117,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 struct Tile {
   uint32_t smb;   // exchange buffer (shared-memory address)
   int tid, lane, warp;
+  int ltid;       // logical thread id: tid with the lane bits moved by deferred lane X gates (FOF_SW on FO_X1L)
   uint64_t ctx0;  // global index bits of the tile outside its 12 bits
   double* sgrad;  // adjoint probe passes: the CTA's partial sums [slot][warp] in shared memory
   uint32_t sw;    // deferred register swaps (FOF_SW): physical slot j holds logical slot j ^ sw
@@ -163,14 +164,19 @@ __device__ __forceinline__ void xbuf_release(Tile& t) {
 #endif
 }
 
-// The layout sl as seen from the logical slots: slot j's amplitude, held in
-// physical slot j ^ sw, goes to the exchange-buffer address of logical slot j.
+// The layout sl as seen from the logical slots and lanes: slot j's amplitude,
+// held in physical slot j ^ sw of this thread, goes to the exchange-buffer
+// address of logical slot j of the logical thread ltid.
 template <int NR>
-__device__ __forceinline__ SLay<NR> logical_slay(const SLay<NR>& sl, uint32_t sw) {
+__device__ __forceinline__ SLay<NR> logical_slay(const SLay<NR>& sl, const Tile& t) {
   SLay<NR> w = sl;
 #pragma unroll
   for (int k = 0; k < NR; k++)
-    if ((sw >> k) & 1) w.b ^= sl.s[k];
+    if ((t.sw >> k) & 1) w.b ^= sl.s[k];
+  const uint32_t dl = (uint32_t)(t.tid ^ t.ltid) & 31u;  // lane bits moved by deferred lane X gates
+#pragma unroll
+  for (int r = 0; r < 5; r++)
+    if ((dl >> r) & 1) w.b ^= sl.l[r];
   return w;
 }
 
@@ -204,8 +210,9 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
   const double* M = op->m;
   const uint32_t smb = t.smb;
   xbuf_acquire(t);
-  write_tile<R, NR>(smb, logical_slay<NR>(sl, t.sw), x);
+  write_tile<R, NR>(smb, logical_slay<NR>(sl, t), x);
   t.sw = 0;
+  t.ltid = t.tid;
   tile_sync(t);
   if constexpr (OPC == OC_GRADM2) {
     // Re<lambda| D |psi> with D 4x4 on tile bits a (MSB), b; the ancilla tile
@@ -310,8 +317,9 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   constexpr double thr = 1e-14, qthr = 1e-7;
   if constexpr (OPC == OC_EXCH) {
     xbuf_acquire(t);
-    write_tile<R, NR>(t.smb, logical_slay<NR>(sl, t.sw), x);
+    write_tile<R, NR>(t.smb, logical_slay<NR>(sl, t), x);
     t.sw = 0;
+    t.ltid = t.tid;
     tile_sync(t);
     sl = exch_slay_c<NR>(c, t.lane, t.warp);
     read_tile<R, NR>(t.smb, sl, x);
@@ -342,13 +350,13 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
     // 3 selects psi / lambda); every lane takes part in the warp sum, so
     // threads whose thread-bit controls fail add zero
     bool thr_ok = true;
-    if constexpr (CTHR != 0) thr_ok = ((uint32_t)t.tid & CTHR) == CTHR;
+    if constexpr (CTHR != 0) thr_ok = ((uint32_t)t.ltid & CTHR) == CTHR;
     const uint32_t smask = thr_ok ? (slotmask<NS>(CREG) & full_mask<NS>()) : 0u;
     double acc;
     if constexpr (OPC == OC_GRADD) {
       const R d0r = (R)c.m[0], d0i = (R)c.m[1], d1r = (R)c.m[2], d1i = (R)c.m[3];
       if (c.flags & (FOF_TGT_THR | FOF_TGT_CTX)) {
-        const bool one = (c.flags & FOF_TGT_CTX) ? (t.ctx0 & c.dg0) != 0 : (bool)((t.tid >> c.a) & 1);
+        const bool one = (c.flags & FOF_TGT_CTX) ? (t.ctx0 & c.dg0) != 0 : (bool)((t.ltid >> c.a) & 1);
         acc = grad_d<R, -1>(x, one ? d1r : d0r, one ? d1i : d0i, one ? d1r : d0r, one ? d1i : d0i, smask);
       } else if (c.a == 0) {
         acc = grad_d<R, 0>(x, d0r, d0i, d1r, d1i, smask);
@@ -365,7 +373,7 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
     return;
   }
   if constexpr (CTHR != 0) {
-    if (((uint32_t)t.tid & CTHR) != CTHR) return;
+    if (((uint32_t)t.ltid & CTHR) != CTHR) return;
   }
   constexpr uint32_t SM = slotmask<NS>(CREG);
   if constexpr (OPC >= OC_MAT1R && OPC < OC_MAT1R + 15) {
@@ -421,6 +429,10 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
     // bit is 1 are the other half, which flipping every pair along A adds
     if constexpr ((FL & FOF_SW) != 0) t.sw ^= ((t.sw >> C) & 1u) << A;
   } else if constexpr (OPC == OC_X1L) {
+    if constexpr ((FL & FOF_SW) != 0) {
+      t.ltid ^= 1 << LA;  // deferred: this thread passed the op's controls; its amplitudes stay
+      return;
+    }
     const uint32_t members = c.lmask;
 #pragma unroll
     for (int j = 0; j < NS; j++)
@@ -441,12 +453,12 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
   } else if constexpr (OPC >= OC_CPHASE && OPC < OC_CPHASE + 5) {
     constexpr int A = OPC - OC_CPHASE;
     const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(g) + 1);
-    phase_fan<R, A, 1, NS>(reinterpret_cast<cpx<R>(&)[1][NS]>(x), g, h2.x, t.ctx0, 0, t.tid);
+    phase_fan<R, A, 1, NS>(reinterpret_cast<cpx<R>(&)[1][NS]>(x), g, h2.x, t.ctx0, 0, t.tid, t.ltid);
   } else if constexpr (OPC == OC_PPOLY) {
-    phase_poly<R, 1, NS>(reinterpret_cast<cpx<R>(&)[1][NS]>(x), g, t.ctx0, 0, t.tid);
+    phase_poly<R, 1, NS>(reinterpret_cast<cpx<R>(&)[1][NS]>(x), g, t.ctx0, 0, t.tid, t.ltid);
   } else if constexpr (OPC == OC_DIAGT || OPC == OC_DIAGX) {
     bool one;
-    if constexpr (OPC == OC_DIAGT) one = (t.tid >> LA) & 1;
+    if constexpr (OPC == OC_DIAGT) one = (t.ltid >> LA) & 1;
     else one = (t.ctx0 & c.dg0) != 0;
     if ((FL & FOF_D0ONE) && !one) return;
     phase_all<R, NS>(x, (R)(one ? c.m[2] : c.m[0]), (R)(one ? c.m[3] : c.m[1]), SM);
@@ -461,6 +473,15 @@ __device__ __forceinline__ void step(cpx<R> (&x)[1 << NR], SLay<NR>& sl, const C
 }
 
 // ---------------------------------------------------------------- store
+// The store base of the thread's logical lane: gs (the physical lane's and
+// warp's offsets) corrected for the lane bits deferred lane X gates moved.
+__device__ __forceinline__ uint64_t logical_base(uint64_t gs, const uint64_t* sgb, const Tile& t) {
+  const uint32_t dl = (uint32_t)(t.tid ^ t.ltid) & 31u;
+#pragma unroll
+  for (int r = 0; r < 5; r++)
+    if ((dl >> r) & 1) gs += ((t.ltid >> r) & 1) ? sgb[r] : (uint64_t)0 - sgb[r];
+  return gs;
+}
 // Store the tile: physical slot j holds logical slot j ^ t.sw, which goes to
 // the address of the logical slot.  With a register bit k swapped, bit k of
 // the address offset is taken where the physical slot's bit k is clear: the
@@ -544,8 +565,9 @@ __device__ __forceinline__ void run_tiles(const Pass2Args& a, Body body) {
     }
     SLay<NR> sl = make_slay<NR>(a.lbx, t.lane, t.warp);
     t.sw = 0;
+    t.ltid = t.tid;
     body(x, sl, t);
-    store_tile<R, NR>(amp + t.ctx0 * sizeof(V) + gs, a.sgb + 5 + NW, t.sw, x);
+    store_tile<R, NR>(amp + t.ctx0 * sizeof(V) + logical_base(gs, a.sgb, t), a.sgb + 5 + NW, t.sw, x);
   }
   if constexpr (GRAD) {
     __syncthreads();
@@ -695,13 +717,14 @@ __device__ __forceinline__ void run_tiles_staged(const Pass2Args& a, const TMap*
     read_tile<R, NR>(t.smb, nat, x);
     SLay<NR> sl = make_slay<NR>(a.lbx, t.lane, t.warp);
     t.sw = 0;
+    t.ltid = t.tid;
     body(x, sl, t);
     // the stage is free once every thread of the group is past its last
     // shared-memory access; its next copy comes from the async proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tile_sync(t);
     if (t.warp == 0 && k + NSTAGE < nk) fill(k + NSTAGE);
-    store_tile<R, NR>(amp + t.ctx0 * sizeof(V) + gs, a.sgb + 5 + NW, t.sw, x);
+    store_tile<R, NR>(amp + t.ctx0 * sizeof(V) + logical_base(gs, a.sgb, t), a.sgb + 5 + NW, t.sw, x);
   }
   // no copy may still be landing when the CTA exits
   __syncthreads();

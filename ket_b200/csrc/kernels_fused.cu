@@ -372,13 +372,13 @@ __global__ void __launch_bounds__(32 << (7 - NR), NR == 5 ? 2 : 1) k_fused2(Pass
   case OC_CPHASE + A:                                                                         \
     if constexpr (A < NR) {                                                                   \
       const uint4 h2 = __ldg(reinterpret_cast<const uint4*>(op) + 1);                        \
-      phase_fan<R, A, TT, NS>(x, op, h2.x, ctx0, pairq, tid);                                 \
+      phase_fan<R, A, TT, NS>(x, op, h2.x, ctx0, pairq, tid, tid);                            \
     }                                                                                         \
     break; /* the continuation records that follow run as no-ops */
         KET_CPHASE(0) KET_CPHASE(1) KET_CPHASE(2) KET_CPHASE(3) KET_CPHASE(4)
 #undef KET_CPHASE
         case OC_PPOLY:
-          phase_poly<R, TT, NS>(x, op, ctx0, pairq, tid);
+          phase_poly<R, TT, NS>(x, op, ctx0, pairq, tid, tid);
           break;  // the continuation records that follow run as no-ops
         case OC_DIAGT: case OC_DIAGX: {
           bool one;

@@ -604,6 +604,40 @@ void defer_swaps(std::vector<FOp>& prog) {
   prog.swap(out);  // the store takes what is still pending
 }
 
+// Deferred X gates on lane bits (FOF_SW on FO_X1L, compiled kernels): an X
+// on lane bit a whose controls sit on thread bits or outside the tile moves
+// amplitudes between lanes.  Instead each thread keeps its logical thread id
+// (the lanes' amplitudes stay where they are; the X flips bit a of the
+// logical id of the threads whose controls hold), every control and phase
+// reads the logical id, and the next exchange, shared-memory op or store
+// addresses the logical lanes.  A lane op needs its partners in place, so an
+// X is deferred only when no lane op follows it before the layout is next
+// written out.  The interpreter ignores the flag and moves the amplitudes.
+void defer_lane_x(std::vector<FOp>& prog) {
+  auto writes_layout = [](const FOp& o) {
+    if (o.type == FO_EXCH || o.type == FO_SWAPS || o.type == FO_MAT2S || o.type == FO_DIAG) return true;
+    return o.type == FO_X1R && o.creg && ((o.creg & (o.creg - 1)) || o.cthr || o.cctx);  // the shared-memory X
+  };
+  auto lane_op = [](const FOp& o) {
+    return o.type == FO_MAT1L || (o.type == FO_X1L && o.creg) || o.type == FO_GRADM || o.type == FO_GRADD ||
+           o.type == FO_GRADM2;
+  };
+  bool later_lane_op = false;  // scanning backwards: a lane op follows in the current segment
+  for (size_t i = prog.size(); i-- > 0;) {
+    FOp& o = prog[i];
+    if (o.type == FO_CONT) continue;
+    if (writes_layout(o)) {
+      later_lane_op = false;
+      continue;
+    }
+    if (o.type == FO_X1L && !o.creg && !later_lane_op) {
+      o.flags |= FOF_SW;
+      continue;
+    }
+    if (lane_op(o)) later_lane_op = true;
+  }
+}
+
 }  // namespace
 
 void assign_opcode(FOp& o) {
@@ -845,6 +879,7 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
       merge_phase_fans(prog);
     }
     if (!getenv("KET_NO_DEFER")) defer_swaps(prog);
+    if (!getenv("KET_NO_LANE_DEFER")) defer_lane_x(prog);
     for (FOp& o : prog) assign_opcode(o);
     g_relabel = false;
     return;

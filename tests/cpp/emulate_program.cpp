@@ -73,6 +73,8 @@ int64_t g_type_count[32];
 // interpreter's, which carries every swap out at once and ignores both.
 int g_deferred = 1;
 int64_t g_sw_count = 0;  // ops with FOF_SW in the programs emulated since the last reset
+int g_lane_error = 0;    // a lane op met lanes moved by deferred lane X gates
+int64_t g_lane_defer_count = 0;  // deferred lane X gates in the programs emulated since the last reset
 
 void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
   std::vector<FOp> prog;
@@ -81,6 +83,7 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
   for (const FOp& o : prog) {
     g_type_count[o.type & 31]++;
     if (o.type != FO_CONT && (o.flags & FOF_SW)) g_sw_count++;
+    if (o.type == FO_X1L && (o.flags & FOF_SW)) g_lane_defer_count++;
   }
   const int L = p.L;
   auto gq = [&](int tb) { return tb < L ? tb : p.hbits[tb - L]; };
@@ -105,6 +108,22 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
     for (int t = 0; t < NTH; t++)
       for (int j = 0; j < NS; j++) x[t * NS + j] = amp[gaddr(ctx, Lc.tbase[t] | rofs(Lc, j))];
     std::vector<uint32_t> sw(NTH, 0);
+    // logical thread ids: deferred lane X gates (FOF_SW on FO_X1L) move the
+    // lane bits of a thread's logical id, not its amplitudes
+    std::vector<int> lt(NTH);
+    for (int t = 0; t < NTH; t++) lt[t] = t;
+    // move every thread's amplitudes to its logical thread (as the kernel's
+    // logical-lane addressing of exchanges and stores does)
+    auto lanes_home = [&]() {
+      std::vector<cx> v = x;
+      for (int t = 0; t < NTH; t++) {
+        for (int j = 0; j < NS; j++) x[lt[t] * NS + j] = v[t * NS + j];
+      }
+      std::vector<uint32_t> s2(NTH);
+      for (int t = 0; t < NTH; t++) s2[lt[t]] = sw[t];
+      sw = s2;
+      for (int t = 0; t < NTH; t++) lt[t] = t;
+    };
     // carry out the pending swaps of register bits m (physical slot order = logical)
     auto realize = [&](uint32_t m) {
       for (int t = 0; t < NTH; t++) {
@@ -128,8 +147,16 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
       if (op.type == FO_SYNC) continue;  // a barrier: nothing to emulate
       // the kernel's exchanges and shared-memory ops write the logical slots
       const bool smem_x1 = op.type == FO_X1R && op.creg && ((op.creg & (op.creg - 1)) || op.cthr || op.cctx);
-      if (op.type == FO_EXCH || op.type == FO_SWAPS || op.type == FO_MAT2S || op.type == FO_DIAG || smem_x1)
+      if (op.type == FO_EXCH || op.type == FO_SWAPS || op.type == FO_MAT2S || op.type == FO_DIAG || smem_x1) {
         realize(0xffffffffu);
+        lanes_home();
+      }
+      // a lane op needs the partner lanes in place: the program generator
+      // defers no lane X before one
+      if (op.type == FO_MAT1L || (op.type == FO_X1L && !(g_deferred && (op.flags & FOF_SW)))) {
+        for (int t = 0; t < NTH; t++)
+          if (lt[t] != t) g_lane_error = 1;
+      }
       if (op.type == FO_CPHASE) {
         // phase fan on register bit a: T[k] * prod H[thread bits] * exp(i sum ctx angles)
         const double* H = record_data(prog, oi + 1);
@@ -145,7 +172,7 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
         for (int t = 0; t < NTH; t++) {
           cx F = E;
           for (int sb = 0; sb < 8; sb++)
-            if ((t >> sb) & 1) F *= cx(H[2 * sb], H[2 * sb + 1]);
+            if ((lt[t] >> sb) & 1) F *= cx(H[2 * sb], H[2 * sb + 1]);
           for (int j = 0; j < NS; j++) {
             if (!((j >> op.a) & 1)) continue;
             const int k = ((j >> (op.a + 1)) << op.a) | (j & ((1 << op.a) - 1));
@@ -174,7 +201,7 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
             if (!cnt[seg]) continue;
             cx f(1.0, 0.0);
             for (uint32_t k = 0; k < cnt[seg]; k++, g++)
-              if (((uint32_t)t & desc[g].tm) == desc[g].tm) f *= K[g];
+              if (((uint32_t)lt[t] & desc[g].tm) == desc[g].tm) f *= K[g];
             for (int j = 0; j < NS; j++)
               if (seg == 0 || ((j >> (seg - 1)) & 1)) x[t * NS + j] *= f;
           }
@@ -195,12 +222,17 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
       const bool dfr = g_deferred && (op.flags & FOF_SW);
       if (dfr && op.type == FO_X1R && !op.creg) {
         for (int t = 0; t < NTH; t++)
-          if ((uint32_t)(t & op.cthr) == op.cthr) sw[t] ^= 1u << op.a;
+          if ((uint32_t)(lt[t] & op.cthr) == op.cthr) sw[t] ^= 1u << op.a;
+        continue;
+      }
+      if (dfr && op.type == FO_X1L) {  // a deferred lane X: the logical ids move
+        for (int t = 0; t < NTH; t++)
+          if ((uint32_t)(lt[t] & op.cthr) == op.cthr) lt[t] ^= 1 << op.a;
         continue;
       }
       std::vector<cx> nx = x;
       for (int t = 0; t < NTH; t++) {
-        const uint32_t sm_ = ((uint32_t)(t & op.cthr) == op.cthr) ? slotmask(op.creg) : 0;
+        const uint32_t sm_ = ((uint32_t)(lt[t] & op.cthr) == op.cthr) ? slotmask(op.creg) : 0;
         cx* xt = &x[t * NS];
         cx* nt = &nx[t * NS];
         const int lane = t & 31;
@@ -236,7 +268,7 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
               if ((sm_ >> j) & 1) nt[j] = ((j >> op.a) & 1 ? d1 : d0) * xt[j];
             break;
           case FO_DIAGT: case FO_DIAGX: {
-            bool one = op.type == FO_DIAGT ? ((t >> op.a) & 1) : ((ctx & op.dg0) != 0);
+            bool one = op.type == FO_DIAGT ? ((lt[t] >> op.a) & 1) : ((ctx & op.dg0) != 0);
             for (int j = 0; j < NS; j++)
               if ((sm_ >> j) & 1) nt[j] = (one ? d1 : d0) * xt[j];
             break;
@@ -288,10 +320,11 @@ void run_pass(const Plan& plan, const Pass& p, int n, bool prunef, cx* amp) {
         // X1RC on a deferred control bit C: flipping every pair along a adds the other half
         const int c = __builtin_ctz(op.creg);
         for (int t = 0; t < NTH; t++)
-          if ((uint32_t)(t & op.cthr) == op.cthr) sw[t] ^= ((sw[t] >> c) & 1u) << op.a;
+          if ((uint32_t)(lt[t] & op.cthr) == op.cthr) sw[t] ^= ((sw[t] >> c) & 1u) << op.a;
       }
     }
-    realize(0xffffffffu);  // the store writes the logical slots
+    realize(0xffffffffu);  // the store writes the logical slots and lanes
+    lanes_home();
     Lay Ls = make_lay(sp);
     for (int t = 0; t < NTH; t++)
       for (int j = 0; j < NS; j++) amp[gaddr(ctx, Ls.tbase[t] | rofs(Ls, j))] = x[t * NS + j];
@@ -321,12 +354,14 @@ int emu_apply_nreg(int n, const ket_op* ops, size_t nops, const double* mats, si
   passes[0] = passes[1] = 0;
   memset(g_type_count, 0, sizeof g_type_count);
   g_sw_count = 0;
+  g_lane_error = 0;
+  g_lane_defer_count = 0;
   for (const Pass& p : plan.passes) {
     if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) { passes[1]++; return -1; }
     run_pass(plan, p, n, prune != 0, amp);
     passes[0]++;
   }
-  return 0;
+  return g_lane_error ? -2 : 0;
 }
 
 // Ops of FOpType `type` in the programs of the last emu_apply call.
@@ -335,6 +370,7 @@ int64_t emu_type_count(int type) { return g_type_count[type & 31]; }
 // 1 (the default): deferred register swaps as the compiled kernels run them; 0: as the interpreter.
 void emu_set_deferred(int on) { g_deferred = on; }
 int64_t emu_sw_count() { return g_sw_count; }
+int64_t emu_lane_defer_count() { return g_lane_defer_count; }
 
 int emu_apply(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int prune, int fusion,
               double* re_im, int64_t* passes) {

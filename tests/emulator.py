@@ -35,6 +35,8 @@ def lib():
     L.emu_set_deferred.argtypes = [C.c_int]
     L.emu_sw_count.restype = C.c_int64
     L.emu_sw_count.argtypes = []
+    L.emu_lane_defer_count.restype = C.c_int64
+    L.emu_lane_defer_count.argtypes = []
     _lib = L
     return L
 
@@ -42,6 +44,11 @@ def lib():
 def sw_count():
     """Ops with deferred register swaps (FOF_SW) in the programs of the last emu_apply call."""
     return lib().emu_sw_count()
+
+
+def lane_defer_count():
+    """Deferred X gates on lane bits in the programs of the last emu_apply call."""
+    return lib().emu_lane_defer_count()
 
 
 def type_count(fop_type):

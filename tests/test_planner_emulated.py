@@ -75,13 +75,15 @@ FO_REAL = 17
 @pytest.mark.parametrize("prune", [True, False])
 def test_emulated_deferred_register_swaps(n, nreg, prune):
     """CNOTs whose control sits on a thread bit or outside the tile and whose
-    target is a register bit are deferred (FOF_SW): the brickwork's programs
-    hold such ops, and the compiled kernels' semantics (per-thread swap flags,
-    matrix entries exchanged, FO_REAL, logical-slot exchanges and stores) give
-    the reference algorithm's state, as the interpreter's eager swaps do."""
+    target is a register bit are deferred (FOF_SW), and so are X gates on lane
+    bits with no lane op after them before the next exchange: the brickwork's
+    programs hold both, and the compiled kernels' semantics (per-thread swap
+    flags and logical thread ids, matrix entries exchanged, FO_REAL,
+    logical-slot and logical-lane exchanges and stores) give the reference
+    algorithm's state, as the interpreter's eager moves do."""
     from ket_b200 import workloads as W
     from ket_b200.circuit import flatten_ops
-    from emulator import sw_count
+    from emulator import lane_defer_count, sw_count
     from oracle import oracle as O
     c, _ = W.brickwork_qft(n, 12, 7)
     st0 = np.zeros(1 << n, complex)
@@ -92,7 +94,7 @@ def test_emulated_deferred_register_swaps(n, nreg, prune):
     for deferred in (True, False):
         rc, got, passes = emu_apply(n, flatten_ops(c.ops), st0, prune=prune, nreg=nreg, deferred=deferred)
         assert rc == 0
-        assert sw_count() > 0
+        assert sw_count() > 0 and lane_defer_count() > 0
         assert np.max(np.abs(got - want)) < 1e-12
         outs.append(got)
     assert np.array_equal(outs[0], outs[1])  # swaps are exact: both orders give the same bits
