@@ -211,6 +211,9 @@ __device__ __forceinline__ void smem_op(cpx<R> (&x)[1 << NR], const SLay<NR>& sl
   const uint32_t smb = t.smb;
   xbuf_acquire(t);
   write_tile<R, NR>(smb, logical_slay<NR>(sl, t), x);
+  // the tile comes back in logical order below; a probe (read-only, it keeps
+  // the registers) never has swaps or lane moves pending: the program
+  // generator carries them out or defers none before a probe
   t.sw = 0;
   t.ltid = t.tid;
   tile_sync(t);
