@@ -96,7 +96,16 @@ int ctx_upload(ket_ctx* c, void* dst, const void* src, size_t bytes) {
     sl.p = nullptr;
     sl.cap = 0;
     const size_t cap = std::max<size_t>(bytes, 64 << 10);
-    if ((e = cudaHostAlloc(&sl.p, cap, cudaHostAllocDefault)) != cudaSuccess) return cuda_fail(e, "cudaHostAlloc(staging)");
+    if (cudaHostAlloc(&sl.p, cap, cudaHostAllocDefault) != cudaSuccess) {
+      // no pinned memory to be had: copy from the caller's buffer (the copy
+      // may then wait for the stream, as any copy from pageable memory does)
+      cudaGetLastError();
+      sl.p = nullptr;
+      sl.used = false;
+      if ((e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyAsync(upload)");
+      return KET_OK;
+    }
     sl.cap = cap;
   }
   if (!sl.ev && (e = cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming)) != cudaSuccess)
