@@ -35,7 +35,7 @@ struct Gate {
   int t0 = -1, t1 = -1;
   uint64_t cmask = 0;
   bool prune = false;         // computed outputs are flushed when |a|^2 < 1e-14
-  cd m[16];                   // MAT1: m[0..3]; DIAG1: m[0], m[1]; DIAG2: m[0..3]; MAT2: m[0..15]
+  cd m[16] = {};              // MAT1: m[0..3]; DIAG1: m[0], m[1]; DIAG2: m[0..3]; MAT2: m[0..15]
   std::vector<int> tk;        // MATK targets
   std::vector<cd> mk;         // MATK matrix
   int src_op = -1;            // index of the ket_op it came from

@@ -343,6 +343,16 @@ void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& pl
   const uint64_t low = (L >= 64) ? ~uint64_t(0) : bit(L) - 1;
   std::vector<int> pending(G.size());
   for (size_t i = 0; i < G.size(); i++) pending[i] = (int)i;
+  // what the sweeps ask of each gate, once
+  struct Use {
+    uint64_t qs;   // qubits it touches
+    uint64_t mix;  // qubits it mixes
+    bool mixing;   // keeps its order among mixing gates
+    bool fus;      // can join a tile pass
+  };
+  std::vector<Use> use(G.size());
+  for (size_t i = 0; i < G.size(); i++)
+    use[i] = {gate_qubits(G[i]), gate_mix(G[i]), keep_mix_order && is_mixing(G[i]), fusable(G[i])};
 
   auto single_pass = [&](int gi) {
     Pass p;
@@ -369,11 +379,11 @@ void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& pl
     int taken = 0, tmix = 0;
     for (int gi : pending) {
       if ((B & allq) == allq) break;
-      const Gate& g = G[gi];
-      uint64_t qs = gate_qubits(g);
-      bool mixing = keep_mix_order && is_mixing(g);
-      bool blocked = (qs & B) || (mixing && mixblocked) || !fusable(g);
-      uint64_t miss = gate_mix(g) & ~S;
+      const Use& u = use[gi];
+      const uint64_t qs = u.qs;
+      const bool mixing = u.mixing;
+      bool blocked = (qs & B) || (mixing && mixblocked) || !u.fus;
+      uint64_t miss = u.mix & ~S;
       if (blocked || miss) {
         if (!blocked && miss && cand && cand->size() < 16) {
           bool dup = false;
@@ -417,10 +427,10 @@ void plan_passes(int n, int precision, int fusion, bool keep_mix_order, Plan& pl
     bool mixblocked = false;
     std::vector<int> rest;
     for (int gi : pending) {
-      const Gate& g = G[gi];
-      uint64_t qs = gate_qubits(g);
-      bool mixing = keep_mix_order && is_mixing(g);
-      if ((qs & B) || (mixing && mixblocked) || !fusable(g) || (gate_mix(g) & ~S)) {
+      const Use& u = use[gi];
+      const uint64_t qs = u.qs;
+      const bool mixing = u.mixing;
+      if ((qs & B) || (mixing && mixblocked) || !u.fus || (u.mix & ~S)) {
         B |= qs;
         if (mixing) mixblocked = true;
         rest.push_back(gi);

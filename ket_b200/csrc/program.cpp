@@ -77,60 +77,92 @@ bool fits(const Gate& g, const Pass& p, const Lay& l) {
   }
 }
 
-// Choose a layout for the gates from index `from` on.
-Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision) {
-  const int INF = 1 << 30;
-  int next[NB], nreg[NB];
-  for (int b = 0; b < NB; b++) { next[b] = INF; nreg[b] = 0; }
-  for (size_t i = from; i < p.gates.size(); i++) {
-    const Gate& g = plan.gates[p.gates[i]];
-    if (g.type == G_DIAG1 || g.type == G_DIAG2 || g.type == G_GRADD || g.type == G_GRADM2) continue;
-    if (relabel_gate(g, p)) continue;  // needs no role
-    int ts[2] = {tpos(p, g.t0), g.type == G_SWAP || g.type == G_MAT2 ? tpos(p, g.t1) : -1};
-    for (int t : ts) {
-      if (t < 0) continue;
-      if (next[t] == INF) { next[t] = (int)i; nreg[t] = needs_two_regs(g) ? 1 : 0; }
-    }
+// For each tile bit, the index of the first gate from `from` on whose
+// target it is (kNever when none) and whether that gate needs two registers.
+struct FirstUse {
+  int next[NB];
+  int nreg[NB];
+};
+const int kNever = 1 << 30;
+
+// Fold gate i into the first uses of the gates after it.
+void first_use_step(const Plan& plan, const Pass& p, size_t i, FirstUse& f) {
+  const Gate& g = plan.gates[p.gates[i]];
+  if (g.type == G_DIAG1 || g.type == G_DIAG2 || g.type == G_GRADD || g.type == G_GRADM2) return;
+  if (relabel_gate(g, p)) return;  // needs no role
+  const int ts[2] = {tpos(p, g.t0), g.type == G_SWAP || g.type == G_MAT2 ? tpos(p, g.t1) : -1};
+  for (int t : ts)
+    if (t >= 0) { f.next[t] = (int)i; f.nreg[t] = needs_two_regs(g) ? 1 : 0; }
+}
+
+// First uses for every start index 0..G, by one backward sweep.
+std::vector<FirstUse> first_uses(const Plan& plan, const Pass& p) {
+  const size_t G = p.gates.size();
+  std::vector<FirstUse> f(G + 1);
+  for (int b = 0; b < NB; b++) { f[G].next[b] = kNever; f[G].nreg[b] = 0; }
+  for (size_t i = G; i-- > 0;) {
+    f[i] = f[i + 1];
+    first_use_step(plan, p, i, f[i]);
   }
+  return f;
+}
+
+// Choose a layout for the gates from index `from` on, given their first uses.
+Lay choose_with(const Plan& plan, const Pass& p, size_t from, bool a0, int precision, const FirstUse& fu) {
+  const int* next = fu.next;
+  const int* nreg = fu.nreg;
+  struct Bits {  // a short list of tile bits
+    int v[NB];
+    int n = 0;
+    void add(int b) { v[n++] = b; }
+  };
   // the adjoint ancilla always sits in registers; a 2x2 probe's target too
-  std::vector<int> must;
-  if (g_anc_tb >= 0) must.push_back(g_anc_tb);
+  Bits must;
+  if (g_anc_tb >= 0) must.add(g_anc_tb);
   if (from < p.gates.size()) {
     const Gate& g = plan.gates[p.gates[from]];
-    if (g.type == G_GRADM) must.push_back(tpos(p, g.t0));
+    if (g.type == G_GRADM) must.add(tpos(p, g.t0));
   }
-  std::vector<int> order(NB);
-  for (int b = 0; b < NB; b++) order[b] = b;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    if (next[x] != next[y]) return next[x] < next[y];
-    return nreg[x] > nreg[y];
-  });
+  // tile bits by first use (soonest first; a use needing two registers first
+  // among equals; the lower bit first among the rest): a stable insertion sort
+  int order[NB];
+  for (int b = 0; b < NB; b++) {
+    int j = b;
+    for (; j > 0; j--) {
+      const int y = order[j - 1];
+      const bool before = next[b] != next[y] ? next[b] < next[y] : nreg[b] > nreg[y];
+      if (!before) break;
+      order[j] = y;
+    }
+    order[j] = b;
+  }
   Lay l;
-  std::vector<bool> used(NB, false);
-  std::vector<int> regs, lanes, warps;
-  auto take_reg = [&](int b) { regs.push_back(b); used[b] = true; };
+  bool used[NB] = {};
+  Bits regs, lanes, warps;
+  auto take_reg = [&](int b) { regs.add(b); used[b] = true; };
   if (a0) {
-    for (int b = 0; b < 5; b++) { lanes.push_back(b); used[b] = true; }
-    for (int b : must) if (!used[b] && (int)regs.size() < NRg()) take_reg(b);
-    for (int b : order) if (!used[b] && (int)regs.size() < NRg() && b >= 5) take_reg(b);
-    for (int b : order) if (!used[b]) { warps.push_back(b); used[b] = true; }
+    for (int b = 0; b < 5; b++) { lanes.add(b); used[b] = true; }
+    for (int k = 0; k < must.n; k++) if (!used[must.v[k]] && regs.n < NRg()) take_reg(must.v[k]);
+    for (int b : order) if (!used[b] && regs.n < NRg() && b >= 5) take_reg(b);
+    for (int b : order) if (!used[b]) { warps.add(b); used[b] = true; }
   } else {
-    for (int b : must) if (!used[b] && (int)regs.size() < NRg()) take_reg(b);
+    for (int k = 0; k < must.n; k++) if (!used[must.v[k]] && regs.n < NRg()) take_reg(must.v[k]);
     // prefer registers for bits whose first use needs two registers
-    for (int b : order) if (!used[b] && (int)regs.size() < NRg() && nreg[b]) take_reg(b);
-    for (int b : order) if (!used[b] && (int)regs.size() < NRg()) take_reg(b);
-    for (int b : order) if (!used[b] && (int)lanes.size() < 5) { lanes.push_back(b); used[b] = true; }
-    for (int b = 0; b < NB; b++) if (!used[b]) { warps.push_back(b); used[b] = true; }
+    for (int b : order) if (!used[b] && regs.n < NRg() && nreg[b]) take_reg(b);
+    for (int b : order) if (!used[b] && regs.n < NRg()) take_reg(b);
+    for (int b : order) if (!used[b] && lanes.n < 5) { lanes.add(b); used[b] = true; }
+    for (int b = 0; b < NB; b++) if (!used[b]) { warps.add(b); used[b] = true; }
     // Shared-memory bank spread: the swizzle folds tile bits mod 3 (c128) or
     // mod 4 (c64) into the low bits, so lanes 0..2 (0..3) should cover
-    // distinct residues.
+    // distinct residues: the first lane of each residue in turn, then the rest
+    // in their order.
     const int mod = precision == KET_C64 ? 4 : 3;
-    std::vector<int> ln = lanes, out;
-    for (int r = 0; r < mod && !ln.empty(); r++) {
-      for (size_t k = 0; k < ln.size(); k++)
-        if (ln[k] % mod == r) { out.push_back(ln[k]); ln.erase(ln.begin() + k); break; }
-    }
-    for (int b : ln) out.push_back(b);
+    Bits out;
+    bool moved[NB] = {};
+    for (int r = 0; r < mod; r++)
+      for (int k = 0; k < lanes.n; k++)
+        if (!moved[k] && lanes.v[k] % mod == r) { out.add(lanes.v[k]); moved[k] = true; break; }
+    for (int k = 0; k < lanes.n; k++) if (!moved[k]) out.add(lanes.v[k]);
     lanes = out;
   }
   // the adjoint ancilla always occupies the top register bit (the kernel's
@@ -138,12 +170,19 @@ Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision)
   const int top = NRg() - 1;
   if (g_anc_tb >= 0)
     for (int i = 0; i < top; i++)
-      if (regs[i] == g_anc_tb) std::swap(regs[i], regs[top]);
-  for (int i = 0; i < 5; i++) l.pos[i] = lanes[i];
-  for (int i = 0; i < NWg(); i++) l.pos[5 + i] = warps[i];
-  for (int i = 0; i < NRg(); i++) l.pos[REG0() + i] = regs[i];
+      if (regs.v[i] == g_anc_tb) std::swap(regs.v[i], regs.v[top]);
+  for (int i = 0; i < 5; i++) l.pos[i] = lanes.v[i];
+  for (int i = 0; i < NWg(); i++) l.pos[5 + i] = warps.v[i];
+  for (int i = 0; i < NRg(); i++) l.pos[REG0() + i] = regs.v[i];
   fill_roles(l);
   return l;
+}
+
+Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision) {
+  FirstUse f;
+  for (int b = 0; b < NB; b++) { f.next[b] = kNever; f.nreg[b] = 0; }
+  for (size_t i = p.gates.size(); i-- > from;) first_use_step(plan, p, i, f);
+  return choose_with(plan, p, from, a0, precision, f);
 }
 
 // l with tile bits a and b exchanged: where the data stays after swapping them.
@@ -737,10 +776,11 @@ bool same_lay(const Lay& a, const Lay& b) { return memcmp(a.pos, b.pos, sizeof a
 // greedy rule).
 bool plan_layouts(const Plan& plan, const Pass& p, int precision, std::vector<Lay>& lay) {
   const size_t G = p.gates.size();
+  const std::vector<FirstUse> fu = first_uses(plan, p);
   std::vector<std::vector<Lay>> cand(G + 1);
   for (size_t i = 0; i <= G; i++) {
     for (int a0 = 1; a0 >= 0; a0--) {
-      const Lay l = choose(plan, p, i, a0 != 0, precision);
+      const Lay l = choose_with(plan, p, i, a0 != 0, precision, fu[i]);
       bool dup = false;
       for (const Lay& c : cand[i]) dup = dup || same_lay(c, l);
       if (!dup) cand[i].push_back(l);
@@ -753,17 +793,8 @@ bool plan_layouts(const Plan& plan, const Pass& p, int precision, std::vector<La
     bool exch;  // entered by an exchange at this position
   };
   std::vector<std::vector<St>> at(G + 1);  // states in effect before gate i (after any exchange at i)
-  // starting layouts: every lane-keeping candidate
-  for (size_t i = 0; i <= G; i++)
-    for (const Lay& c : cand[i]) {
-      if (!a0_compatible(c)) continue;
-      bool dup = false;
-      for (const St& s : at[0]) dup = dup || same_lay(s.l, c);
-      if (!dup) at[0].push_back({c, 0.0, -1, false});
-    }
   std::vector<std::vector<St>> run(G + 1);  // states arriving at i by running gate i-1 (or the start)
-  run[0] = at[0];
-  at[0].clear();
+  // a list keeps one state per layout, the cheapest (the first of equals)
   auto relax = [](std::vector<St>& v, const St& s) {
     for (St& o : v)
       if (same_lay(o.l, s.l)) {
@@ -772,32 +803,49 @@ bool plan_layouts(const Plan& plan, const Pass& p, int precision, std::vector<La
       }
     v.push_back(s);
   };
+  // starting layouts: every lane-keeping candidate
+  for (size_t i = 0; i <= G; i++)
+    for (const Lay& c : cand[i])
+      if (a0_compatible(c)) relax(run[0], {c, 0.0, -1, false});
+  // Every list holds distinct layouts: the start list and the exchange
+  // targets by relax, the stays because the run list they copy does, and the
+  // run list because running a gate keeps a layout and a relabelling maps
+  // distinct layouts to distinct ones.
   for (size_t i = 0; i <= G; i++) {
-    // stay, or exchange to a candidate
+    // stay
+    at[i].reserve(run[i].size() + cand[i].size());
     for (size_t k = 0; k < run[i].size(); k++) {
       St s = run[i][k];
       s.from = (int)k;
       s.exch = false;
-      relax(at[i], s);
+      at[i].push_back(s);
     }
-    for (size_t k = 0; k < run[i].size(); k++)
-      for (const Lay& c : cand[i]) {
+    // or exchange to a candidate from the cheapest state of another layout
+    // (the first of equals)
+    for (const Lay& c : cand[i]) {
+      if (i < G && !fits(plan.gates[p.gates[i]], p, c)) continue;
+      if (i == G && !a0_compatible(c)) continue;
+      int from = -1;
+      double fc = 0;
+      for (size_t k = 0; k < run[i].size(); k++) {
         if (same_lay(c, run[i][k].l)) continue;
-        if (i < G && !fits(plan.gates[p.gates[i]], p, c)) continue;
-        if (i == G && !a0_compatible(c)) continue;
-        relax(at[i], {c, run[i][k].cost + exch_cost(), (int)k, true});
+        const double v = run[i][k].cost + exch_cost();
+        if (from < 0 || v < fc) { from = (int)k; fc = v; }
       }
+      if (from >= 0) relax(at[i], {c, fc, from, true});
+    }
     if (i == G) break;
     const Gate& g = plan.gates[p.gates[i]];
     const bool rel = relabel_gate(g, p);
+    run[i + 1].reserve(at[i].size());
     for (size_t k = 0; k < at[i].size(); k++) {
       const St& s = at[i][k];
       if (rel) {
-        relax(run[i + 1], {relabeled(s.l, tpos(p, g.t0), tpos(p, g.t1)), s.cost, (int)k, false});
+        run[i + 1].push_back({relabeled(s.l, tpos(p, g.t0), tpos(p, g.t1)), s.cost, (int)k, false});
         continue;
       }
       if (!fits(g, p, s.l)) continue;
-      relax(run[i + 1], {s.l, s.cost + gate_cost(g, p, s.l), (int)k, false});
+      run[i + 1].push_back({s.l, s.cost + gate_cost(g, p, s.l), (int)k, false});
     }
     if (run[i + 1].empty()) return false;
   }

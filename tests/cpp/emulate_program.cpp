@@ -5,6 +5,7 @@
 // ops, controls).  The tests compare it with direct gate-by-gate application,
 // so planner and program-generator bugs show up without a GPU.
 #include <complex>
+#include <cstdint>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -375,5 +376,38 @@ int64_t emu_lane_defer_count() { return g_lane_defer_count; }
 int emu_apply(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int prune, int fusion,
               double* re_im, int64_t* passes) {
   return emu_apply_nreg(n, ops, nops, mats, nmat, prune, fusion, re_im, passes, KET_FUSED_NREG);
+}
+
+// Plan an op list as a run on an n-qubit state would (automatic fusion) and
+// digest, with 64-bit FNV-1a, every register-tiled pass's load and store
+// layouts and program bytes in order; nothing is emulated, so n may be 30.
+// out[0] = the digest, out[1] = tiled passes, out[2] = program ops.
+int emu_plan_digest(int n, int precision, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int prune,
+                    int nreg, uint64_t* out) {
+  Plan plan;
+  std::string err;
+  int rc = lower_ops(n, ops, nops, mats, nmat, prune != 0, plan.gates, err);
+  if (rc) return rc;
+  fold_single_qubit(plan.gates, prune != 0);
+  plan_passes(n, precision, -1, prune != 0, plan);
+  uint64_t h = 0xcbf29ce484222325ull;
+  auto mix = [&h](const void* d, size_t b) {
+    const unsigned char* c = static_cast<const unsigned char*>(d);
+    for (size_t i = 0; i < b; i++) { h ^= c[i]; h *= 0x100000001b3ull; }
+  };
+  out[1] = out[2] = 0;
+  for (const Pass& p : plan.passes) {
+    if (!(p.fused && p.m == KET_T2_BITS && n >= KET_T2_BITS)) continue;
+    std::vector<FOp> prog;
+    uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
+    plan_program(plan, p, precision, prune != 0, nreg, prog, lp, sp);
+    mix(lp, sizeof lp);
+    mix(sp, sizeof sp);
+    if (!prog.empty()) mix(prog.data(), prog.size() * sizeof(FOp));
+    out[1]++;
+    out[2] += prog.size();
+  }
+  out[0] = h;
+  return 0;
 }
 }

@@ -37,6 +37,9 @@ def lib():
     L.emu_sw_count.argtypes = []
     L.emu_lane_defer_count.restype = C.c_int64
     L.emu_lane_defer_count.argtypes = []
+    L.emu_plan_digest.restype = C.c_int
+    L.emu_plan_digest.argtypes = [C.c_int, C.c_int, C.POINTER(ket_op), C.c_size_t, C.POINTER(C.c_double), C.c_size_t,
+                                  C.c_int, C.c_int, C.POINTER(C.c_uint64)]
     _lib = L
     return L
 
@@ -69,3 +72,16 @@ def emu_apply(n, ops, init_state, prune=True, fusion=-1, nreg=5, deferred=True):
     rc = lib().emu_apply_nreg(n, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, 1 if prune else 0, fusion,
                               st.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)), passes, nreg)
     return rc, st, list(passes)
+
+
+def plan_digest(n, ops, precision, prune=True, nreg=4):
+    """(FNV-1a digest of every tiled pass's layouts and program bytes, tiled
+    passes, program ops) for ops planned as a run on an n-qubit state would."""
+    from ket_b200.circuit import ops_to_abi
+    arr, m, k = ops_to_abi(ops)
+    mv = np.ascontiguousarray(m).view(np.float64)
+    out = (C.c_uint64 * 3)()
+    rc = lib().emu_plan_digest(n, precision, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size,
+                               1 if prune else 0, nreg, out)
+    assert rc == 0, rc
+    return out[0], out[1], out[2]

@@ -156,3 +156,37 @@ def test_relabelling_programs_keep_loads_before_stores(nreg):
     for p, q in ((6, 13), (9, 15), (7, 12)):
         want = np.swapaxes(want, n - 1 - p, n - 1 - q)
     assert np.array_equal(got, want.reshape(-1))
+
+
+# Digests of the programs the planner makes for fixed circuits.  A change to
+# the planner that is meant to leave its output alone (a faster search, a
+# refactor) must leave these alone; one that changes the programs on purpose
+# updates them, after the emulated and GPU parity tests pass.  They also pin
+# that planning is deterministic: every byte of every op is defined.
+PINNED_DIGESTS = [
+    # (circuit, n, precision, prune, register bits) -> (digest, tiled passes, program ops)
+    (("brickwork_qft", 30, 40, 42), "c128", True, 4, (0xeeddb0f01fc22c8b, 106, 1819)),
+    (("random", 14, 200, 2), "c128", True, 4, (0xdca14723c9e04af2, None, None)),
+    (("random", 14, 200, 2), "c64", False, 5, (0xca49d847b18b1794, None, None)),
+    (("brickwork_qft", 24, 12, 7), "c64", True, 4, (0xb1d93486d5347078, None, None)),
+]
+
+
+@pytest.mark.parametrize("circ,prec,prune,nreg,want", PINNED_DIGESTS)
+def test_pinned_program_digests(circ, prec, prune, nreg, want):
+    import ket_b200 as K
+    from ket_b200 import _lib, workloads as W
+    from ket_b200.circuit import flatten_ops
+    from emulator import plan_digest
+    if circ[0] == "brickwork_qft":
+        c, _ = W.brickwork_qft(circ[1], circ[2], circ[3])
+    else:
+        c = K.Circuit(circ[1])
+        for name, qs, ps in random_gates(circ[1], circ[2], circ[3]):
+            c = c.unitary(ps, *qs) if name == "unitary" else getattr(c, name)(*ps, *qs)
+    precision = _lib.KET_C128 if prec == "c128" else _lib.KET_C64
+    got = plan_digest(circ[1], flatten_ops(c.ops), precision, prune=prune, nreg=nreg)
+    assert got[0] == want[0], hex(got[0])
+    for g, w in zip(got[1:], want[1:]):
+        if w is not None:
+            assert g == w
