@@ -53,8 +53,6 @@ int tpos(const Pass& p, int q) {
   return -1;
 }
 
-bool needs_two_regs(const Gate&) { return false; }
-
 thread_local int g_anc_tb = -1;  // tile bit of the adjoint ancilla in the pass being lowered
 thread_local bool g_relabel = false;  // uncontrolled swaps of two tile bits become relabellings (FO_RELAY)
 
@@ -78,10 +76,9 @@ bool fits(const Gate& g, const Pass& p, const Lay& l) {
 }
 
 // For each tile bit, the index of the first gate from `from` on whose
-// target it is (kNever when none) and whether that gate needs two registers.
+// target it is (kNever when none).
 struct FirstUse {
   int next[NB];
-  int nreg[NB];
 };
 const int kNever = 1 << 30;
 
@@ -92,14 +89,14 @@ void first_use_step(const Plan& plan, const Pass& p, size_t i, FirstUse& f) {
   if (relabel_gate(g, p)) return;  // needs no role
   const int ts[2] = {tpos(p, g.t0), g.type == G_SWAP || g.type == G_MAT2 ? tpos(p, g.t1) : -1};
   for (int t : ts)
-    if (t >= 0) { f.next[t] = (int)i; f.nreg[t] = needs_two_regs(g) ? 1 : 0; }
+    if (t >= 0) f.next[t] = (int)i;
 }
 
 // First uses for every start index 0..G, by one backward sweep.
 std::vector<FirstUse> first_uses(const Plan& plan, const Pass& p) {
   const size_t G = p.gates.size();
   std::vector<FirstUse> f(G + 1);
-  for (int b = 0; b < NB; b++) { f[G].next[b] = kNever; f[G].nreg[b] = 0; }
+  for (int b = 0; b < NB; b++) f[G].next[b] = kNever;
   for (size_t i = G; i-- > 0;) {
     f[i] = f[i + 1];
     first_use_step(plan, p, i, f[i]);
@@ -110,7 +107,6 @@ std::vector<FirstUse> first_uses(const Plan& plan, const Pass& p) {
 // Choose a layout for the gates from index `from` on, given their first uses.
 Lay choose_with(const Plan& plan, const Pass& p, size_t from, bool a0, int precision, const FirstUse& fu) {
   const int* next = fu.next;
-  const int* nreg = fu.nreg;
   struct Bits {  // a short list of tile bits
     int v[NB];
     int n = 0;
@@ -123,15 +119,14 @@ Lay choose_with(const Plan& plan, const Pass& p, size_t from, bool a0, int preci
     const Gate& g = plan.gates[p.gates[from]];
     if (g.type == G_GRADM) must.add(tpos(p, g.t0));
   }
-  // tile bits by first use (soonest first; a use needing two registers first
-  // among equals; the lower bit first among the rest): a stable insertion sort
+  // tile bits by first use (soonest first, the lower bit first among
+  // equals): a stable insertion sort
   int order[NB];
   for (int b = 0; b < NB; b++) {
     int j = b;
     for (; j > 0; j--) {
       const int y = order[j - 1];
-      const bool before = next[b] != next[y] ? next[b] < next[y] : nreg[b] > nreg[y];
-      if (!before) break;
+      if (next[b] >= next[y]) break;
       order[j] = y;
     }
     order[j] = b;
@@ -147,8 +142,6 @@ Lay choose_with(const Plan& plan, const Pass& p, size_t from, bool a0, int preci
     for (int b : order) if (!used[b]) { warps.add(b); used[b] = true; }
   } else {
     for (int k = 0; k < must.n; k++) if (!used[must.v[k]] && regs.n < NRg()) take_reg(must.v[k]);
-    // prefer registers for bits whose first use needs two registers
-    for (int b : order) if (!used[b] && regs.n < NRg() && nreg[b]) take_reg(b);
     for (int b : order) if (!used[b] && regs.n < NRg()) take_reg(b);
     for (int b : order) if (!used[b] && lanes.n < 5) { lanes.add(b); used[b] = true; }
     for (int b = 0; b < NB; b++) if (!used[b]) { warps.add(b); used[b] = true; }
@@ -180,7 +173,7 @@ Lay choose_with(const Plan& plan, const Pass& p, size_t from, bool a0, int preci
 
 Lay choose(const Plan& plan, const Pass& p, size_t from, bool a0, int precision) {
   FirstUse f;
-  for (int b = 0; b < NB; b++) { f.next[b] = kNever; f.nreg[b] = 0; }
+  for (int b = 0; b < NB; b++) f.next[b] = kNever;
   for (size_t i = p.gates.size(); i-- > from;) first_use_step(plan, p, i, f);
   return choose_with(plan, p, from, a0, precision, f);
 }
