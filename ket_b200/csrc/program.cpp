@@ -864,6 +864,23 @@ bool plan_layouts(const Plan& plan, const Pass& p, int precision, std::vector<La
   return true;
 }
 
+// Switches for experiments, read once per process: the greedy layout rule
+// instead of the cost-model planner (everywhere, or for adjoint passes),
+// swaps as data moves instead of relabellings, and no deferred register
+// swaps or lane X gates.
+struct Switches {
+  bool greedy = getenv("KET_GREEDY_LAYOUT") != nullptr;
+  bool adjoint_greedy = getenv("KET_ADJOINT_GREEDY") != nullptr;
+  bool no_relabel = getenv("KET_NO_RELABEL") != nullptr;
+  bool no_defer = getenv("KET_NO_DEFER") != nullptr;
+  bool no_lane_defer = getenv("KET_NO_LANE_DEFER") != nullptr;
+};
+
+const Switches& switches() {
+  static const Switches s;
+  return s;
+}
+
 }  // namespace
 
 void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, int nreg, std::vector<FOp>& prog,
@@ -875,8 +892,9 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
   // adjoint passes too (their probes fit only where the ancilla and a 2x2
   // probe's target sit in registers, which the candidates respect); their
   // swaps stay data moves
-  const bool dp = !getenv("KET_GREEDY_LAYOUT") && (g_anc_tb < 0 || !getenv("KET_ADJOINT_GREEDY"));
-  g_relabel = dp && g_anc_tb < 0 && !getenv("KET_NO_RELABEL");
+  const Switches& sw = switches();
+  const bool dp = !sw.greedy && (g_anc_tb < 0 || !sw.adjoint_greedy);
+  g_relabel = dp && g_anc_tb < 0 && !sw.no_relabel;
   if (dp && plan_layouts(plan, p, precision, lay)) {
     // lay[i]: the layout gate i runs in; lay[G]: the store layout
     Lay cur = lay[0];
@@ -919,8 +937,8 @@ void plan_program(const Plan& plan, const Pass& p, int precision, bool prune, in
       merge_phase_polys(prog);
       merge_phase_fans(prog);
     }
-    if (!getenv("KET_NO_DEFER")) defer_swaps(prog);
-    if (!getenv("KET_NO_LANE_DEFER")) defer_lane_x(prog);
+    if (!sw.no_defer) defer_swaps(prog);
+    if (!sw.no_lane_defer) defer_lane_x(prog);
     for (FOp& o : prog) assign_opcode(o);
     g_relabel = false;
     return;
