@@ -410,4 +410,52 @@ int emu_plan_digest(int n, int precision, const ket_op* ops, size_t nops, const 
   out[0] = h;
   return 0;
 }
+
+// The same digest for an adjoint-style reverse plan on n + 1 qubits: the
+// lowered gates in reverse order, the ancilla on qubit n, and after every
+// one-qubit matrix gate a 2x2 probe (G_GRADM) on its target, after every
+// one-qubit diagonal a diagonal probe (G_GRADD); probe passes keep their
+// order, pruning is off, as in the adjoint sweep.
+int emu_adjoint_plan_digest(int n, const ket_op* ops, size_t nops, const double* mats, size_t nmat, int nreg,
+                            uint64_t* out) {
+  Plan fwd;
+  std::string err;
+  int rc = lower_ops(n, ops, nops, mats, nmat, false, fwd.gates, err);
+  if (rc) return rc;
+  Plan plan;
+  plan.anc = n;
+  int slot = 0;
+  for (size_t k = fwd.gates.size(); k-- > 0;) {
+    const Gate& g = fwd.gates[k];
+    plan.gates.push_back(g);
+    if (g.type != G_MAT1 && g.type != G_DIAG1) continue;
+    Gate pr;
+    pr.type = g.type == G_MAT1 ? G_GRADM : G_GRADD;
+    pr.t0 = g.t0;
+    pr.cmask = g.cmask;
+    pr.slot = slot++;
+    for (int q = 0; q < 4; q++) pr.m[q] = g.m[q];
+    plan.gates.push_back(pr);
+  }
+  plan_passes(n + 1, KET_C128, -1, false, plan);
+  uint64_t h = 0xcbf29ce484222325ull;
+  auto mix = [&h](const void* d, size_t b) {
+    const unsigned char* c = static_cast<const unsigned char*>(d);
+    for (size_t i = 0; i < b; i++) { h ^= c[i]; h *= 0x100000001b3ull; }
+  };
+  out[1] = out[2] = 0;
+  for (const Pass& p : plan.passes) {
+    if (!(p.fused && p.m == KET_T2_BITS)) continue;
+    std::vector<FOp> prog;
+    uint8_t lp[KET_T2_BITS], sp[KET_T2_BITS];
+    plan_program(plan, p, KET_C128, false, nreg, prog, lp, sp);
+    mix(lp, sizeof lp);
+    mix(sp, sizeof sp);
+    if (!prog.empty()) mix(prog.data(), prog.size() * sizeof(FOp));
+    out[1]++;
+    out[2] += prog.size();
+  }
+  out[0] = h;
+  return 0;
+}
 }

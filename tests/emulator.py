@@ -37,6 +37,9 @@ def lib():
     L.emu_sw_count.argtypes = []
     L.emu_lane_defer_count.restype = C.c_int64
     L.emu_lane_defer_count.argtypes = []
+    L.emu_adjoint_plan_digest.restype = C.c_int
+    L.emu_adjoint_plan_digest.argtypes = [C.c_int, C.POINTER(ket_op), C.c_size_t, C.POINTER(C.c_double), C.c_size_t,
+                                          C.c_int, C.POINTER(C.c_uint64)]
     L.emu_plan_digest.restype = C.c_int
     L.emu_plan_digest.argtypes = [C.c_int, C.c_int, C.POINTER(ket_op), C.c_size_t, C.POINTER(C.c_double), C.c_size_t,
                                   C.c_int, C.c_int, C.POINTER(C.c_uint64)]
@@ -83,5 +86,17 @@ def plan_digest(n, ops, precision, prune=True, nreg=4):
     out = (C.c_uint64 * 3)()
     rc = lib().emu_plan_digest(n, precision, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size,
                                1 if prune else 0, nreg, out)
+    assert rc == 0, rc
+    return out[0], out[1], out[2]
+
+
+def adjoint_plan_digest(n, ops, nreg=4):
+    """plan_digest for an adjoint-style reverse plan of ops on n + 1 qubits
+    (ancilla n, a probe after every one-qubit matrix or diagonal gate)."""
+    from ket_b200.circuit import ops_to_abi
+    arr, m, k = ops_to_abi(ops)
+    mv = np.ascontiguousarray(m).view(np.float64)
+    out = (C.c_uint64 * 3)()
+    rc = lib().emu_adjoint_plan_digest(n, arr, k, mv.ctypes.data_as(C.POINTER(C.c_double)), m.size, nreg, out)
     assert rc == 0, rc
     return out[0], out[1], out[2]

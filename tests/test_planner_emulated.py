@@ -190,3 +190,28 @@ def test_pinned_program_digests(circ, prec, prune, nreg, want):
     for g, w in zip(got[1:], want[1:]):
         if w is not None:
             assert g == w
+
+
+# The same for adjoint-style reverse plans (the ancilla on qubit n, probes
+# after the one-qubit matrix and diagonal gates): the probe passes' programs.
+PINNED_ADJOINT_DIGESTS = [
+    (("tfim_vqe", 24), (0x84d88aee9de27529, 30, 1068)),
+    (("random", 15, 250, 11), (0x77d05877904d3a2b, 11, 459)),
+]
+
+
+@pytest.mark.parametrize("circ,want", PINNED_ADJOINT_DIGESTS)
+def test_pinned_adjoint_program_digests(circ, want):
+    import ket_b200 as K
+    from ket_b200 import workloads as W
+    from ket_b200.circuit import flatten_ops
+    from emulator import adjoint_plan_digest
+    if circ[0] == "tfim_vqe":
+        ans, _, params = W.tfim_vqe(circ[1], 8, 1)
+        c = ans(params[0])
+    else:
+        c = K.Circuit(circ[1])
+        for name, qs, ps in random_gates(circ[1], circ[2], circ[3]):
+            c = c.unitary(ps, *qs) if name == "unitary" else getattr(c, name)(*ps, *qs)
+    got = adjoint_plan_digest(circ[1], flatten_ops(c.ops))
+    assert got == want, (hex(got[0]), got[1:])
